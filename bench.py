@@ -1,0 +1,395 @@
+"""Throughput benchmark of the force path: body-steps/s of a N = 2^20 Plummer sphere
+(quadrupole linear BVH, leaf 16, theta 0.5, softening 0.005, dt 5e-4), one instance per GPU.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = Solver::step (accelerations by Morton sort + LBVH build + bottom-up moments +
+warp traversal, then kick-drift) on the whole body set. Prints ONE JSON line on rank 0.
+
+  value   device-resident steps, CUDA events on the solver's stream; L2 (126 MB) flushed by a
+          256 MB write before every timed step (outside the events)
+  e2e     the same steps through the C ABI with host buffers: copy bodies in (nb_set_bodies),
+          step, copy bodies out (nb_get_bodies), wall clock per step
+  roofline dominant kernel = the traversal (FP32 pipe + MUFU bound, no tensor-core work):
+          achieved = counted interactions x flop weights / traversal event time; a second entry
+          gives the sort's algorithmic HBM bytes against the measured copy bandwidth
+  cpu_baseline  the oracle (CPU restatement of the reference's TBB path) on a bounded sample:
+          full tree build over all N bodies plus the traversal of a seeded target subsample,
+          extrapolated to all N targets, OpenMP over all host cores
+
+With --impl reference the same metric is measured for the reference's algorithm on the host
+cores (the oracle port: the reference itself cannot be built on this image).
+Under torchrun (N > 1) every rank runs its own instance (weak scaling, no data-path collective);
+timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "n-body_b200"))
+
+N_BODIES = 1 << 20
+SOFTENING = 0.005
+THETA = 0.5
+LEAF = 16
+ORDER = 2
+DT = 5e-4
+SEED = 43
+METRIC = "body-steps/s at N=1M Plummer theta=0.5, force RMS<=1e-3"
+# Flop weights per interaction, counted from n-body_b200/csrc/traverse.cu (FMA = 2 flops):
+# pair term 20 (usual direct-sum convention; 12 FP32 instructions + 1 rsqrt), quadrupole node 56.
+PAIR_FLOPS = 20
+QUAD_NODE_FLOPS = 56
+MONO_NODE_FLOPS = 20
+FP32_FLOP_PER_CLK_PER_SM = 256  # 128 FP32 lanes x FMA
+NUM_SMS = 148
+CPU_SAMPLE_TARGETS = 32768
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=N_BODIES)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join("/tmp", f"nb_clocks_{os.getpid()}_{device}.csv")
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = np.array([float(r[1]) for r in rows if r[1].replace(".", "").isdigit()])
+        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        loaded = sm[sm >= 0.5 * sm.max()] if len(sm) else sm
+        return {"sm_mhz": float(np.median(loaded)) if len(loaded) else None, "sm_max_mhz": smax,
+                "reasons": reasons, "samples": int(len(sm))}
+
+
+def flush_l2(buf):
+    buf.zero_()
+
+
+def accuracy(nb, solver, pm, eps, torch, device):
+    """Relative RMS force error vs an FP64 direct sum on a seeded 8192-target subsample, plus the
+    reference's own graders: RMSGrader = sqrt(max relerr^2) * 100 (RMSGrader.h:17-37) and
+    ConstitutionalGrader = max 100 |dF| / min(|F|, F_rms) (ConstitutionalGrader.h:40-64)."""
+    n = len(pm)
+    rng = np.random.default_rng(12345)
+    idx = np.sort(rng.choice(n, min(8192, n), replace=False))
+    acc = solver.update_accelerations()
+    dpm = torch.from_numpy(pm).to(device)
+    dt = torch.from_numpy(pm[idx].copy()).to(device)
+    out = torch.zeros((len(idx), 3), dtype=torch.float64, device=device)
+    solver.direct_device(n, dpm.data_ptr(), len(idx), dt.data_ptr(), out.data_ptr(), 64)
+    solver.synchronize()
+    ref = out.cpu().numpy()
+    got = acc[idx, :3].astype(np.float64)
+    diff = np.linalg.norm(got - ref, axis=1)
+    mag = np.linalg.norm(ref, axis=1)
+    rel = diff / mag
+    m = pm[idx, 3].astype(np.float64)
+    f_rms = np.sqrt(np.mean((mag * m) ** 2))
+    return {
+        "force_rms_rel": float(np.sqrt(np.mean(rel ** 2))),
+        "force_max_rel": float(rel.max()),
+        "rms_grader_pct": float(np.sqrt((rel ** 2).max()) * 100.0),
+        "constitutional_pct": float(np.max(100.0 * diff * m / np.minimum(mag * m, f_rms))),
+        "sample_targets": int(len(idx)),
+        "reference": "FP64 direct sum on GPU",
+    }
+
+
+def cpu_baseline(pm, eps, steps=1):
+    """The oracle (CPU restatement) on a bounded sample of the workload."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle as O
+
+    O.lib()
+    n = len(pm)
+    threads = O.max_threads()
+    rng = np.random.default_rng(777)
+    s = min(CPU_SAMPLE_TARGETS, n)
+    idx = np.sort(rng.choice(n, s, replace=False))
+    tiny = pm[idx[:1]].copy()
+    t0 = time.perf_counter()
+    O.bh_targets(pm, tiny, eps=eps, theta=THETA, leaf=LEAF, order=ORDER)
+    t_build = time.perf_counter() - t0
+    t_total = 0.0
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        O.bh_targets(pm, pm[idx], eps=eps, theta=THETA, leaf=LEAF, order=ORDER)
+        t_total += time.perf_counter() - t0
+    t_sample = t_total / steps
+    per_target = max(t_sample - t_build, 1e-12) / s
+    step_time = t_build + per_target * n
+    return {
+        "value": n / step_time,
+        "unit": "body-steps/s",
+        "cores": threads,
+        "kind": "port",
+        "sample": f"tree build over all {n} bodies + traversal of {s} seeded targets "
+                  f"({t_sample:.2f} s per sample), extrapolated to {n} targets "
+                  f"(est. {step_time:.1f} s per step)",
+    }
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(REPO, "n-body_b200"))
+    from nbody_b200 import scenarios
+
+    pm, _ = scenarios.plummer(args.n, seed=SEED)
+    eps = scenarios.softening_to_epsilon(SOFTENING)
+    if args.warmup > 0:
+        cpu_baseline(pm[: min(len(pm), 65536)], eps, steps=1)
+    vals = []
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(pm, eps, steps=1))
+    value = float(np.median([v["value"] for v in vals]))
+    base = dict(vals[-1])
+    base["value"] = value
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "body-steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * args.n / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(args), "cpu_baseline": base,
+        "e2e": {"value": value, "unit": "body-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args):
+    return {"workload": f"plummer-{args.n}-quadrupole-linear-bvh", "n_bodies": args.n, "theta": THETA,
+            "leaf_size": LEAF, "order": ORDER, "softening": SOFTENING, "epsilon_added_to_r2": SOFTENING ** 2,
+            "dt": DT, "seed": SEED, "l2": "flushed (256 MB write) before every timed step",
+            "parallelism": "one instance per GPU"}
+
+
+def run_ours(args):
+    import torch
+
+    world, rank, local = dist_env()
+    device = local
+    torch.cuda.set_device(device)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    import nbody_b200 as nb
+    from nbody_b200 import scenarios
+
+    pm, vel = scenarios.plummer(args.n, seed=SEED + rank)
+    eps = scenarios.softening_to_epsilon(SOFTENING)
+    # A dedicated (non-default) stream shared by the solver, the L2 flush and the timing events.
+    stream = torch.cuda.Stream(device)
+    with torch.cuda.stream(stream):
+        line = _run_ours_on_stream(args, torch, nb, pm, vel, eps, stream, world, rank, device)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def _run_ours_on_stream(args, torch, nb, pm, vel, eps, stream, world, rank, device):
+    solver = nb.QuadrupoleLinearBVHSolver(bodies=pm, rule=nb.Gravity(1.0, eps), velocities=vel, theta=THETA,
+                                          max_leaf_size=LEAF, time_step=DT, device=device)
+    solver.set_stream(stream.cuda_stream)
+    acc_info = accuracy(nb, solver, pm, eps, torch, torch.device("cuda", device))
+    counts = solver.counts()
+    solver.set_bodies(pm, vel)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+
+    for _ in range(args.warmup):
+        flush_l2(flush)
+        solver.step(1)
+    torch.cuda.synchronize(device)
+    p0, v0 = solver.bodies()
+    solver.enable_timing(True)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(device)
+    with Clocks(device) as clk:
+        for k in range(args.steps):
+            flush_l2(flush)
+            starts[k].record(stream)
+            solver.step(1)
+            ends[k].record(stream)
+        torch.cuda.synchronize(device)
+    if world > 1:
+        torch.distributed.barrier()
+    step_ms = float(sum(s.elapsed_time(e) for s, e in zip(starts, ends)))
+    phases = solver.phase_times()
+    solver.enable_timing(False)
+    p1, v1 = solver.bodies()
+    mom0 = (p0[:, 3:4].astype(np.float64) * v0[:, :3]).sum(0)
+    mom1 = (p1[:, 3:4].astype(np.float64) * v1[:, :3]).sum(0)
+
+    # e2e through the C ABI with pinned host buffers
+    h_pm = torch.from_numpy(p1.copy()).pin_memory()
+    h_vel = torch.from_numpy(v1.copy()).pin_memory()
+    out_pm = torch.empty_like(h_pm).pin_memory()
+    out_vel = torch.empty_like(h_vel).pin_memory()
+    lib = nb.lib()
+    torch.cuda.synchronize(device)
+    if world > 1:
+        torch.distributed.barrier()
+    e2e_s = 0.0
+    for _ in range(args.e2e_steps):
+        t0 = time.perf_counter()
+        solver._check(lib.nb_set_bodies(solver.handle, args.n, h_pm.data_ptr(), h_vel.data_ptr()))
+        solver._check(lib.nb_step(solver.handle, 1))
+        solver._check(lib.nb_get_bodies(solver.handle, out_pm.data_ptr(), out_vel.data_ptr()))
+        e2e_s += time.perf_counter() - t0
+        h_pm.copy_(out_pm)
+        h_vel.copy_(out_vel)
+
+    t_max = step_ms
+    e2e_max = e2e_s
+    if world > 1:
+        t = torch.tensor([step_ms, e2e_s], dtype=torch.float64, device=device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        t_max, e2e_max = float(t[0]), float(t[1])
+    value = args.n * world * args.steps / (t_max / 1000.0)
+    e2e_value = args.n * world * args.e2e_steps / e2e_max
+
+    # roofline of the dominant kernel (traversal), per launch
+    passes = max(int(phases["passes"]), 1)
+    trav_ms = phases["traverse_ms"] / passes
+    flops = counts["particle_particle"] * PAIR_FLOPS + counts["node_particle"] * QUAD_NODE_FLOPS
+    clk = clk.summary()
+    sm_mhz = clk.get("sm_mhz") or 1965.0
+    peak = NUM_SMS * FP32_FLOP_PER_CLK_PER_SM * sm_mhz * 1e6 / 1e12
+    achieved = flops / (trav_ms / 1000.0) / 1e12
+    traffic = read_traffic()
+    sort_ms = phases["sort_ms"] / passes
+    sort_bytes = 8 * 24 * args.n
+    hbm_peak = measured_hbm()
+    line = {
+        "metric": METRIC, "value": value, "unit": "body-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Plummer sphere)",
+        "config": workload_config(args),
+        "e2e": {"value": e2e_value, "unit": "body-steps/s", "h2d_bytes_per_step": 32 * args.n,
+                "d2h_bytes_per_step": 32 * args.n, "steps": args.e2e_steps,
+                "path": "nb_set_bodies (pinned host) + nb_step + nb_get_bodies, wall clock"},
+        "roofline": {"bound": "fp32", "kernel": "bh_kernel<2> (traversal)", "achieved": achieved, "peak": peak,
+                     "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": f"148 SMs x 256 FP32 flop/clk x {sm_mhz:.0f} MHz SM clock measured under "
+                                    "load (no FP32 peak in MEASURED_PEAKS.json; tensor cores do not apply)",
+                     "flops_per_launch": flops, "ms_per_launch": trav_ms,
+                     "interactions": {"pp": counts["particle_particle"], "np": counts["node_particle"]}},
+        "roofline_hbm": {"bound": "hbm", "kernel": "onesweep radix sort (8 passes)",
+                         "achieved": sort_bytes / (sort_ms / 1000.0) / 1e9 if sort_ms > 0 else None,
+                         "peak": hbm_peak, "unit": "GB/s",
+                         "frac": (sort_bytes / (sort_ms / 1000.0) / 1e9) / hbm_peak if sort_ms > 0 and hbm_peak
+                         else None, "bytes_per_sort": sort_bytes, "ms_per_sort": sort_ms,
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"},
+        "phases_ms_per_step": {k: phases[k] / passes for k in
+                               ("bbox_ms", "morton_ms", "sort_ms", "gather_ms", "build_ms", "traverse_ms",
+                                "integrate_ms")},
+        "gpu_launches": int(phases["launches"]),
+        "accuracy": acc_info,
+        "momentum_drift": float(np.linalg.norm(mom1 - mom0)),
+        "clocks": clk,
+    }
+    solver.close()
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(pm, eps)
+    return line
+
+
+def measured_hbm():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(path))["hbm_gbs"])
+    except Exception:
+        return 6650.0
+
+
+def read_traffic():
+    """DRAM bytes per traversal launch from the committed ncu summary, if one exists."""
+    path = os.path.join(REPO, "profiles", "traffic.txt")
+    try:
+        for line in open(path):
+            if line.startswith("bh_kernel_traffic_bytes_per_launch"):
+                return float(line.split("=")[1])
+    except Exception:
+        pass
+    return None
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

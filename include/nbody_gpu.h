@@ -1,0 +1,162 @@
+/*
+ * nbody_gpu.h - C ABI of the B200 (sm_100a) force-evaluation path of the n-body simulator.
+ *
+ * One opaque context stands in for one reference solver instance (Solver<Rule>,
+ * src/NBody/Simulation/Solver.h:26-187) together with its rule (Gravity, src/NBody/Physics/Rules/Gravity.h)
+ * and its tree (LinearBVH, src/NBody/Simulation/Solvers/Trees/LinearBVH.h). The context owns the
+ * bodies' device-resident state; host buffers are copied in and out at the calls that take them.
+ *
+ * Conventions
+ *   - Every function returns an int status: NB_OK (0) or a negative NB_ERR_* code; the message of
+ *     the last failure is available from nb_last_error(). (The reference reports errors through
+ *     assert and spdlog only, MultiSolver.h:86, 104-105.)
+ *   - Bodies cross the boundary as 4 floats each: positions+masses as (x, y, z, m), velocities
+ *     as (vx, vy, vz, unused), accelerations as (ax, ay, az, 0), always in the caller's order.
+ *     The reference keeps Position/Velocity/Acceleration as glm::vec3 and Mass as float
+ *     components in an EnTT registry (src/NBody/Simulation/Simulation.h:45); a caller gathers
+ *     those views into these arrays.
+ *   - "_device" variants take device pointers (16-byte aligned) on the context's device.
+ *   - Work is ordered on the context's CUDA stream (nb_set_stream to share the caller's stream).
+ *     Calls that return host data synchronise that stream.
+ *   - A context is not re-entrant: one thread at a time per context. Different contexts are
+ *     independent.
+ */
+#ifndef NBODY_GPU_H
+#define NBODY_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NB_OK 0
+#define NB_ERR_INVALID_ARGUMENT (-1)
+#define NB_ERR_CUDA (-2)
+#define NB_ERR_OUT_OF_MEMORY (-3)
+#define NB_ERR_NO_BODIES (-4)
+#define NB_ERR_DEVICE_TIMEOUT (-5)
+#define NB_ERR_UNSUPPORTED (-6)
+#define NB_ERR_DEVICE_CHECK (-7)
+
+/* Solver selection: the reference's Solver::id() strings (Solver.h:89-91). */
+typedef enum nb_solver {
+    /* ActiveTreeSolver<LinearBVH<S>, DiagonalOverCenterDistance, Gravity>
+     * (src/NBody/Simulation/Solvers/ActiveTreeSolver.h:16-82, LinearBVHSolver.h:18-53):
+     * order 1 = LinearBVHSolver ("linear-bvh"), order 2 = QuadrupoleLinearBVHSolver ("linear-bvh-4p"). */
+    NB_SOLVER_LINEAR_BVH = 0,
+    /* NaiveSolver (src/NBody/Simulation/Solvers/NaiveSolver.h:12-53, "naive"): FP32 direct sum. */
+    NB_SOLVER_NAIVE = 1
+} nb_solver;
+
+typedef struct nb_config {
+    int32_t solver;        /* nb_solver */
+    int32_t order;         /* multipole order of the node summaries: 1 (centre of mass) or 2 (quadrupole) */
+    float G;               /* Gravity::g()        (Gravity.h:195, 407) */
+    float epsilon;         /* Gravity::epsilon(): added to r^2 (Gravity.h:207) */
+    float theta;           /* ActiveTreeSolver::theta() (ActiveTreeSolver.h:78-80) */
+    int32_t max_leaf_size; /* LinearBVH::maxLeafSize() (LinearBVH.h:135-137) */
+    float time_step;       /* Solver::timeStep() (Solver.h:101) */
+    int32_t device;        /* CUDA device ordinal */
+} nb_config;
+
+/* Interaction counts of the last force pass, SimpleTrackingRule's convention
+ * (src/NBody/Physics/Rules/SimpleTrackingRule.h:29-51): one per Gravity call. */
+typedef struct nb_counts {
+    uint64_t particle_particle;
+    uint64_t particle_node;
+    uint64_t node_particle;
+    uint64_t node_node;
+} nb_counts;
+
+/* Device time per phase, summed over the force passes since timing was enabled (CUDA events on
+ * the context's stream). Kernel launches of each phase are counted in `launches`. */
+typedef struct nb_phase_times {
+    double bbox_ms, morton_ms, sort_ms, gather_ms, build_ms, traverse_ms, integrate_ms;
+    int64_t passes;
+    int64_t launches;
+} nb_phase_times;
+
+typedef struct nb_ctx nb_ctx;
+
+/* Reference defaults: Gravity(G = 1, epsilon = 1e-5) (Gravity.h:195), theta 0.3
+ * (ActiveTreeSolver.h:21), maxLeafSize 64 (LinearBVH.h:88), dt 0.001 (Solver.h:34), order 1. */
+void nb_config_default(nb_config *cfg);
+
+/* Construct a solver (Solver(Simulation&, Rule&), Solver.h:51). Fails with NB_ERR_CUDA when no
+ * usable sm_100 device is present: there is no CPU fallback. */
+int nb_create(const nb_config *cfg, nb_ctx **out);
+int nb_destroy(nb_ctx *ctx);
+const char *nb_last_error(const nb_ctx *ctx);
+
+/* Solver::id() / Solver::name() of the configured solver (Solver.h:89-91, LinearBVHSolver.h:28-44). */
+const char *nb_solver_id(const nb_ctx *ctx);
+const char *nb_solver_name(const nb_ctx *ctx);
+
+/* Change theta, leaf size, G, epsilon, dt or the solver between steps
+ * (ActiveTreeSolver::theta(), LinearBVH::maxLeafSize(), Gravity::g()/epsilon(), Solver::timeStep()). */
+int nb_set_config(nb_ctx *ctx, const nb_config *cfg);
+int nb_get_config(const nb_ctx *ctx, nb_config *cfg);
+
+/* Order the context's work on a caller-owned cudaStream_t (NULL: the context's own stream). */
+int nb_set_stream(nb_ctx *ctx, void *cuda_stream);
+void *nb_get_stream(const nb_ctx *ctx);
+
+/* Replace the body set (the Simulation's Position/Mass/Velocity components). velocity may be NULL
+ * (zero velocities). n may be 0. */
+int nb_set_bodies(nb_ctx *ctx, int64_t n, const float *pos_mass, const float *velocity);
+int nb_set_bodies_device(nb_ctx *ctx, int64_t n, const void *d_pos_mass, const void *d_velocity);
+int64_t nb_body_count(const nb_ctx *ctx);
+
+/* Read the current bodies back in the caller's order. Either pointer may be NULL. */
+int nb_get_bodies(nb_ctx *ctx, float *pos_mass, float *velocity);
+int nb_get_bodies_device(nb_ctx *ctx, void *d_pos_mass, void *d_velocity);
+
+/* Solver::updateAccelerations() (Solver.h:115; ActiveTreeSolver.h:33-72; NaiveSolver.h:22-52):
+ * compute every body's acceleration from the current positions. acc_out (n x 4 floats, caller's
+ * order) may be NULL to leave the result on the device. */
+int nb_update_accelerations(nb_ctx *ctx, float *acc_out);
+int nb_get_accelerations(nb_ctx *ctx, float *acc_out);
+int nb_get_accelerations_device(nb_ctx *ctx, void *d_acc_out);
+
+/* Solver::step() repeated `steps` times (Solver.h:103-139): accelerations, then v += a dt,
+ * then x += v dt. Device-resident between steps; asynchronous on the context's stream. */
+int nb_step(nb_ctx *ctx, int32_t steps);
+
+/* Wait for the context's work; reports device-side check failures (e.g. a bounded wait that
+ * expired) as NB_ERR_DEVICE_TIMEOUT / NB_ERR_DEVICE_CHECK. */
+int nb_synchronize(nb_ctx *ctx);
+
+/* SimpleTrackingRule counts of the last force pass (synchronises). */
+int nb_get_counts(nb_ctx *ctx, nb_counts *out);
+
+/* Per-phase device timing (CUDA events), off by default. */
+int nb_enable_timing(nb_ctx *ctx, int enable);
+int nb_get_phase_times(nb_ctx *ctx, nb_phase_times *out);
+
+/* Parity taps on the last tree built (synchronise). Any output pointer may be NULL.
+ *   num_nodes     node count of the linear BVH (preorder)
+ *   record_floats floats per node record (12 for order 1, 16 for order 2); see nb_tree_record
+ *   sorted_codes  n Morton codes in sorted order (MortonSort.h:46-73)
+ *   sorted_ids    n caller indices of the sorted bodies (the Morton sort's permutation)
+ *   records       num_nodes * record_floats floats
+ *   bbox          6 floats: global box min xyz, max xyz (SummaryType.h:73-81) */
+int nb_get_tree(nb_ctx *ctx, int64_t *num_nodes, int32_t *record_floats, uint64_t *sorted_codes,
+                uint32_t *sorted_ids, float *records, float *bbox);
+
+/* Direct sum on device pointers: accelerations of nt targets (4 floats each) from n bodies.
+ * precision 32: FP32, acc 4 floats per target (NaiveSolver arithmetic).
+ * precision 64: FP64 accumulation, acc 3 doubles per target (accuracy reference). */
+int nb_direct_device(nb_ctx *ctx, int64_t n, const void *d_bodies, int64_t nt, const void *d_targets,
+                     void *d_acc, int32_t precision);
+
+/* Page-locked host buffers for fast copies in and out (cudaMallocHost / cudaFreeHost). */
+void *nb_host_alloc(size_t bytes);
+void nb_host_free(void *p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NBODY_GPU_H */

@@ -1,0 +1,623 @@
+// C ABI of the force path (declared in include/nbody_gpu.h): context, device memory and the
+// per-step pipeline.
+//
+// One force pass (Solver::updateAccelerations, ActiveTreeSolver.h:33-72) on the device:
+//   bbox reduce (skipped when the previous drift already reduced it)
+//   -> Morton codes + digit histograms -> one-sweep radix sort (8 passes)
+//   -> gather positions/velocities/ids into Morton order
+//   -> Karras build + collapse + bottom-up summaries + preorder records
+//   -> lock-step warp traversal
+// and Solver::step adds the kick-drift kernel (which also reduces the next bounding box).
+// No phase has a host fallback: without a usable device nb_create fails.
+#include <algorithm>
+#include <array>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/nbody_gpu.h"
+#include "nb_internal.cuh"
+
+using namespace nbg;
+
+namespace {
+
+template<typename T>
+cudaError_t dev_alloc(T **p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc((void **) p, count * sizeof(T));
+}
+
+template<typename T>
+void dev_free(T *&p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+enum Phase { kBBox = 0, kMorton, kSort, kGather, kBuild, kTraverse, kIntegrate, kEnd, kNumMarks };
+
+}  // namespace
+
+struct nb_ctx {
+    nb_config cfg{};
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string error;
+
+    int64_t n = 0, cap = 0;
+    float4 *pos = nullptr, *vel = nullptr, *acc = nullptr, *pos2 = nullptr, *vel2 = nullptr;
+    uint32_t *id = nullptr, *id2 = nullptr;
+    uint64_t *keys = nullptr;
+    uint32_t *vals = nullptr;
+    SortWorkspace sw;
+    TreeWorkspace tw;
+    float4 *nodes = nullptr;
+    int64_t node_cap = 0;
+    BBoxAccum *bbox = nullptr;
+    unsigned long long *counts = nullptr;
+    uint32_t *err = nullptr;
+    double *acc64 = nullptr;
+    int64_t acc64_cap = 0;
+
+    bool bbox_valid = false;  // bbox already holds the box of the current positions
+    bool have_tree = false;
+    bool have_acc = false;
+    bool acc_is_bh = false;
+
+    bool timing = false;
+    std::vector<cudaEvent_t> event_pool;
+    std::vector<std::array<cudaEvent_t, kNumMarks>> pending;  // marks of passes not yet read
+    nb_phase_times times{};
+    std::string id_str, name_str;
+};
+
+namespace {
+
+int fail(nb_ctx *c, int code, const std::string &msg) {
+    if (c) c->error = msg;
+    return code;
+}
+
+int check_cuda(nb_ctx *c, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return NB_OK;
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    return fail(c, e == cudaErrorMemoryAllocation ? NB_ERR_OUT_OF_MEMORY : NB_ERR_CUDA, m);
+}
+
+#define NB_TRY(expr, what)                                  \
+    do {                                                    \
+        int _rc = check_cuda(ctx, (expr), what);            \
+        if (_rc != NB_OK) return _rc;                       \
+    } while (0)
+
+int rec_floats(int order) { return 4 * (order == 1 ? NodeLayout<1>::REC : NodeLayout<2>::REC); }
+
+void refresh_names(nb_ctx *ctx) {
+    if (ctx->cfg.solver == NB_SOLVER_NAIVE) {
+        ctx->id_str = "naive";
+        ctx->name_str = "Naive";
+    } else if (ctx->cfg.order == 1) {
+        ctx->id_str = "linear-bvh";
+        ctx->name_str = "Linear-BVH";
+    } else {
+        ctx->id_str = "linear-bvh-4p";
+        ctx->name_str = "Linear BVH (Quadrupole)";
+    }
+}
+
+int validate(nb_ctx *ctx, const nb_config *cfg) {
+    if (!cfg) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "config is NULL");
+    if (cfg->solver != NB_SOLVER_LINEAR_BVH && cfg->solver != NB_SOLVER_NAIVE)
+        return fail(ctx, NB_ERR_INVALID_ARGUMENT, "unknown solver");
+    if (cfg->order < 1 || cfg->order > kMaxOrder)
+        return fail(ctx, NB_ERR_UNSUPPORTED, "order must be 1 (centre of mass) or 2 (quadrupole)");
+    if (cfg->max_leaf_size < 1) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "max_leaf_size must be >= 1");
+    if (!(cfg->theta >= 0.f)) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "theta must be >= 0");
+    if (!(cfg->epsilon >= 0.f)) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "epsilon must be >= 0");
+    return NB_OK;
+}
+
+void free_buffers(nb_ctx *ctx) {
+    dev_free(ctx->pos); dev_free(ctx->vel); dev_free(ctx->acc); dev_free(ctx->pos2); dev_free(ctx->vel2);
+    dev_free(ctx->id); dev_free(ctx->id2); dev_free(ctx->keys); dev_free(ctx->vals);
+    dev_free(ctx->sw.keys_alt); dev_free(ctx->sw.vals_alt); dev_free(ctx->sw.lookback);
+    dev_free(ctx->tw.range); dev_free(ctx->tw.left); dev_free(ctx->tw.right); dev_free(ctx->tw.parent);
+    dev_free(ctx->tw.splittable); dev_free(ctx->tw.visit); dev_free(ctx->tw.sbmin); dev_free(ctx->tw.sbmax);
+    dev_free(ctx->tw.scom); dev_free(ctx->tw.sq0); dev_free(ctx->tw.sq1); dev_free(ctx->tw.cnt);
+    dev_free(ctx->nodes);
+    ctx->cap = 0;
+    ctx->node_cap = 0;
+}
+
+int ensure_capacity(nb_ctx *ctx, int64_t n) {
+    if (n <= ctx->cap) return NB_OK;
+    free_buffers(ctx);
+    const int64_t c = std::max<int64_t>(n, 1);
+    const size_t slots = (size_t) (2 * c);
+    NB_TRY(dev_alloc(&ctx->pos, c), "alloc positions");
+    NB_TRY(dev_alloc(&ctx->vel, c), "alloc velocities");
+    NB_TRY(dev_alloc(&ctx->acc, c), "alloc accelerations");
+    NB_TRY(dev_alloc(&ctx->pos2, c), "alloc positions");
+    NB_TRY(dev_alloc(&ctx->vel2, c), "alloc velocities");
+    NB_TRY(dev_alloc(&ctx->id, c), "alloc ids");
+    NB_TRY(dev_alloc(&ctx->id2, c), "alloc ids");
+    NB_TRY(dev_alloc(&ctx->keys, c), "alloc codes");
+    NB_TRY(dev_alloc(&ctx->vals, c), "alloc sort values");
+    NB_TRY(dev_alloc(&ctx->sw.keys_alt, c), "alloc codes");
+    NB_TRY(dev_alloc(&ctx->sw.vals_alt, c), "alloc sort values");
+    NB_TRY(dev_alloc(&ctx->sw.lookback, sort_lookback_words(c)), "alloc sort look-back");
+    ctx->sw.capacity = c;
+    NB_TRY(dev_alloc(&ctx->tw.range, c), "alloc tree ranges");
+    NB_TRY(dev_alloc(&ctx->tw.left, c), "alloc tree");
+    NB_TRY(dev_alloc(&ctx->tw.right, c), "alloc tree");
+    NB_TRY(dev_alloc(&ctx->tw.parent, c), "alloc tree");
+    NB_TRY(dev_alloc(&ctx->tw.splittable, c), "alloc tree");
+    NB_TRY(dev_alloc(&ctx->tw.visit, c), "alloc tree");
+    NB_TRY(dev_alloc(&ctx->tw.sbmin, slots), "alloc summaries");
+    NB_TRY(dev_alloc(&ctx->tw.sbmax, slots), "alloc summaries");
+    NB_TRY(dev_alloc(&ctx->tw.scom, slots), "alloc summaries");
+    NB_TRY(dev_alloc(&ctx->tw.sq0, slots), "alloc summaries");
+    NB_TRY(dev_alloc(&ctx->tw.sq1, slots), "alloc summaries");
+    NB_TRY(dev_alloc(&ctx->tw.cnt, slots), "alloc summaries");
+    ctx->tw.capacity = c;
+    ctx->node_cap = 2 * c;
+    NB_TRY(dev_alloc(&ctx->nodes, (size_t) ctx->node_cap * NodeLayout<2>::REC), "alloc tree nodes");
+    ctx->cap = c;
+    return NB_OK;
+}
+
+cudaEvent_t take_event(nb_ctx *ctx) {
+    if (!ctx->event_pool.empty()) {
+        cudaEvent_t e = ctx->event_pool.back();
+        ctx->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+struct Marks {
+    nb_ctx *ctx;
+    std::array<cudaEvent_t, kNumMarks> ev{};
+    bool on;
+    explicit Marks(nb_ctx *c) : ctx(c), on(c->timing) {
+        if (on)
+            for (auto &e: ev) e = take_event(c);
+    }
+    void mark(int phase) {
+        if (on) cudaEventRecord(ev[phase], ctx->stream);
+    }
+    void commit() {
+        if (on) ctx->pending.push_back(ev);
+    }
+};
+
+// Reads finished passes' events into the phase totals (after a synchronise).
+void collect_times(nb_ctx *ctx) {
+    for (auto &ev: ctx->pending) {
+        float ms[kNumMarks - 1];
+        for (int p = 0; p < kNumMarks - 1; ++p) {
+            ms[p] = 0.f;
+            cudaEventElapsedTime(&ms[p], ev[p], ev[p + 1]);
+        }
+        ctx->times.bbox_ms += ms[kBBox];
+        ctx->times.morton_ms += ms[kMorton];
+        ctx->times.sort_ms += ms[kSort];
+        ctx->times.gather_ms += ms[kGather];
+        ctx->times.build_ms += ms[kBuild];
+        ctx->times.traverse_ms += ms[kTraverse];
+        ctx->times.integrate_ms += ms[kIntegrate];
+        ctx->times.passes += 1;
+        for (auto e: ev) ctx->event_pool.push_back(e);
+    }
+    ctx->pending.clear();
+}
+
+// Kernel launches of one force pass + drift (for the launch count the bench reports).
+int64_t launches_per_pass(const nb_ctx *ctx, bool with_bbox, bool with_drift) {
+    if (ctx->cfg.solver == NB_SOLVER_NAIVE) return 1 + (with_drift ? 1 : 0);
+    // morton(1) + scan(1) + 8 sort passes + gather(1) + karras(1) + summarize(1) + emit(1)
+    // + root-leaf(1) + traverse(1)
+    int64_t k = 1 + 1 + 8 + 1 + 1 + 1 + 1 + 1 + 1;
+    if (ctx->n <= 1) k -= 3;  // no Karras internal nodes
+    return k + (with_bbox ? 1 : 0) + (with_drift ? 1 : 0);
+}
+
+// One force pass over the current state. Leaves accelerations in ctx->acc (current order).
+int force_pass(nb_ctx *ctx, Marks &mk) {
+    const int64_t n = ctx->n;
+    cudaStream_t s = ctx->stream;
+    cudaMemsetAsync(ctx->counts, 0, 4 * sizeof(unsigned long long), s);
+    const bool need_bbox = !ctx->bbox_valid;
+    mk.mark(kBBox);
+    if (ctx->cfg.solver == NB_SOLVER_NAIVE) {
+        mk.mark(kMorton); mk.mark(kSort); mk.mark(kGather); mk.mark(kBuild); mk.mark(kTraverse);
+        launch_direct_f32(ctx->pos, n, ctx->pos, n, ctx->cfg.G, ctx->cfg.epsilon, ctx->acc, s);
+        ctx->have_tree = false;
+        ctx->acc_is_bh = false;
+        if (ctx->timing) ctx->times.launches += 1;
+        return check_cuda(ctx, cudaGetLastError(), "naive direct sum");
+    }
+    if (need_bbox) {
+        launch_bbox_reset(ctx->bbox, s);
+        launch_bbox_reduce(ctx->pos, n, ctx->bbox, s);
+    }
+    mk.mark(kMorton);
+    launch_morton_hist(ctx->pos, n, ctx->bbox, ctx->keys, ctx->sw.hist, s);
+    mk.mark(kSort);
+    launch_radix_sort(ctx->keys, ctx->vals, n, ctx->sw, ctx->err, s);
+    mk.mark(kGather);
+    launch_gather_state(ctx->vals, n, ctx->pos, ctx->vel, ctx->id, ctx->pos2, ctx->vel2, ctx->id2, s);
+    std::swap(ctx->pos, ctx->pos2);
+    std::swap(ctx->vel, ctx->vel2);
+    std::swap(ctx->id, ctx->id2);
+    mk.mark(kBuild);
+    launch_build_tree(ctx->keys, ctx->pos, n, ctx->cfg.max_leaf_size, ctx->cfg.order, ctx->cfg.theta, ctx->tw,
+                      ctx->nodes, ctx->node_cap, ctx->err, s);
+    mk.mark(kTraverse);
+    launch_bh_traverse(ctx->cfg.order, ctx->nodes, ctx->tw.num_nodes, ctx->pos, n, ctx->pos, n, ctx->cfg.G,
+                       ctx->cfg.epsilon, ctx->acc, ctx->counts, s);
+    ctx->have_tree = true;
+    ctx->acc_is_bh = true;
+    if (ctx->timing) ctx->times.launches += launches_per_pass(ctx, need_bbox, false);
+    return check_cuda(ctx, cudaGetLastError(), "force pass");
+}
+
+int device_status(nb_ctx *ctx) {
+    uint32_t e = 0;
+    NB_TRY(cudaMemcpyAsync(&e, ctx->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream), "read status");
+    NB_TRY(cudaStreamSynchronize(ctx->stream), "synchronize");
+    if (ctx->timing) collect_times(ctx);
+    if (e & kErrLookbackTimeout)
+        return fail(ctx, NB_ERR_DEVICE_TIMEOUT, "radix sort look-back wait exceeded its limit");
+    if (e & kErrNodeOverflow) return fail(ctx, NB_ERR_DEVICE_CHECK, "tree node buffer overflow");
+    if (e & kErrTreeDepth) return fail(ctx, NB_ERR_DEVICE_CHECK, "tree walk exceeded the maximum depth");
+    return NB_OK;
+}
+
+int begin(nb_ctx *ctx) {
+    if (!ctx) return NB_ERR_INVALID_ARGUMENT;
+    return check_cuda(ctx, cudaSetDevice(ctx->cfg.device), "cudaSetDevice");
+}
+
+}  // namespace
+
+extern "C" {
+
+void nb_config_default(nb_config *cfg) {
+    if (!cfg) return;
+    cfg->solver = NB_SOLVER_LINEAR_BVH;
+    cfg->order = 1;
+    cfg->G = 1.0f;
+    cfg->epsilon = 0.00001f;
+    cfg->theta = 0.3f;
+    cfg->max_leaf_size = 64;
+    cfg->time_step = 0.001f;
+    cfg->device = 0;
+}
+
+int nb_create(const nb_config *cfg, nb_ctx **out) {
+    if (!out) return NB_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    nb_ctx *ctx = new nb_ctx();
+    int rc = validate(ctx, cfg);
+    if (rc != NB_OK) { delete ctx; return rc; }
+    ctx->cfg = *cfg;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count <= cfg->device || cfg->device < 0) {
+        cudaGetLastError();
+        delete ctx;
+        return NB_ERR_CUDA;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess || prop.major < 10) {
+        delete ctx;
+        return NB_ERR_UNSUPPORTED;
+    }
+    if (cudaSetDevice(cfg->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return NB_ERR_CUDA;
+    }
+    ctx->stream = ctx->own_stream;
+    if (dev_alloc(&ctx->bbox, 1) != cudaSuccess || dev_alloc(&ctx->counts, 4) != cudaSuccess ||
+        dev_alloc(&ctx->err, 1) != cudaSuccess || dev_alloc(&ctx->sw.hist, 8 * 256) != cudaSuccess ||
+        dev_alloc(&ctx->sw.offsets, 8 * 256 + 8) != cudaSuccess || dev_alloc(&ctx->sw.tile_counter, 8) != cudaSuccess ||
+        dev_alloc(&ctx->tw.num_nodes, 1) != cudaSuccess) {
+        nb_destroy(ctx);
+        return NB_ERR_OUT_OF_MEMORY;
+    }
+    cudaMemsetAsync(ctx->err, 0, sizeof(uint32_t), ctx->stream);
+    cudaMemsetAsync(ctx->counts, 0, 4 * sizeof(unsigned long long), ctx->stream);
+    cudaMemsetAsync(ctx->tw.num_nodes, 0, sizeof(int), ctx->stream);
+    refresh_names(ctx);
+    *out = ctx;
+    return NB_OK;
+}
+
+int nb_destroy(nb_ctx *ctx) {
+    if (!ctx) return NB_OK;
+    cudaSetDevice(ctx->cfg.device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    free_buffers(ctx);
+    dev_free(ctx->bbox); dev_free(ctx->counts); dev_free(ctx->err); dev_free(ctx->sw.hist);
+    dev_free(ctx->sw.offsets); dev_free(ctx->sw.tile_counter); dev_free(ctx->tw.num_nodes); dev_free(ctx->acc64);
+    for (auto &ev: ctx->pending) ctx->event_pool.insert(ctx->event_pool.end(), ev.begin(), ev.end());
+    for (auto e: ctx->event_pool) cudaEventDestroy(e);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return NB_OK;
+}
+
+const char *nb_last_error(const nb_ctx *ctx) { return ctx ? ctx->error.c_str() : "no context"; }
+
+const char *nb_solver_id(const nb_ctx *ctx) { return ctx ? ctx->id_str.c_str() : ""; }
+
+const char *nb_solver_name(const nb_ctx *ctx) { return ctx ? ctx->name_str.c_str() : ""; }
+
+int nb_set_config(nb_ctx *ctx, const nb_config *cfg) {
+    if (!ctx) return NB_ERR_INVALID_ARGUMENT;
+    int rc = validate(ctx, cfg);
+    if (rc != NB_OK) return rc;
+    if (cfg->device != ctx->cfg.device) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "the device cannot change");
+    ctx->cfg = *cfg;
+    ctx->have_tree = false;
+    refresh_names(ctx);
+    return NB_OK;
+}
+
+int nb_get_config(const nb_ctx *ctx, nb_config *cfg) {
+    if (!ctx || !cfg) return NB_ERR_INVALID_ARGUMENT;
+    *cfg = ctx->cfg;
+    return NB_OK;
+}
+
+int nb_set_stream(nb_ctx *ctx, void *cuda_stream) {
+    if (!ctx) return NB_ERR_INVALID_ARGUMENT;
+    ctx->stream = cuda_stream ? (cudaStream_t) cuda_stream : ctx->own_stream;
+    return NB_OK;
+}
+
+void *nb_get_stream(const nb_ctx *ctx) { return ctx ? (void *) ctx->stream : nullptr; }
+
+int64_t nb_body_count(const nb_ctx *ctx) { return ctx ? ctx->n : -1; }
+
+static int set_bodies_impl(nb_ctx *ctx, int64_t n, const void *pm, const void *vel, cudaMemcpyKind kind) {
+    int rc = begin(ctx);
+    if (rc != NB_OK) return rc;
+    if (n < 0 || n > kMaxBodies) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "body count out of range");
+    if (n > 0 && !pm) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "positions are NULL");
+    rc = ensure_capacity(ctx, n);
+    if (rc != NB_OK) return rc;
+    ctx->n = n;
+    const size_t bytes = (size_t) n * sizeof(float4);
+    if (n > 0) {
+        NB_TRY(cudaMemcpyAsync(ctx->pos, pm, bytes, kind, ctx->stream), "copy positions");
+        if (vel) NB_TRY(cudaMemcpyAsync(ctx->vel, vel, bytes, kind, ctx->stream), "copy velocities");
+        else NB_TRY(cudaMemsetAsync(ctx->vel, 0, bytes, ctx->stream), "zero velocities");
+        NB_TRY(cudaMemsetAsync(ctx->acc, 0, bytes, ctx->stream), "zero accelerations");
+        launch_iota(ctx->id, n, ctx->stream);
+    }
+    ctx->bbox_valid = false;
+    ctx->have_tree = false;
+    ctx->have_acc = false;
+    return check_cuda(ctx, cudaGetLastError(), "set bodies");
+}
+
+int nb_set_bodies(nb_ctx *ctx, int64_t n, const float *pos_mass, const float *velocity) {
+    int rc = set_bodies_impl(ctx, n, pos_mass, velocity, cudaMemcpyHostToDevice);
+    if (rc != NB_OK) return rc;
+    // The caller may reuse its host buffers as soon as this returns.
+    return check_cuda(ctx, cudaStreamSynchronize(ctx->stream), "set bodies");
+}
+
+int nb_set_bodies_device(nb_ctx *ctx, int64_t n, const void *d_pos_mass, const void *d_velocity) {
+    return set_bodies_impl(ctx, n, d_pos_mass, d_velocity, cudaMemcpyDeviceToDevice);
+}
+
+static int get_state_impl(nb_ctx *ctx, void *pm, void *vel, cudaMemcpyKind kind, bool host) {
+    int rc = begin(ctx);
+    if (rc != NB_OK) return rc;
+    const int64_t n = ctx->n;
+    const size_t bytes = (size_t) n * sizeof(float4);
+    if (n > 0) {
+        // pos2/vel2 are free between passes; use them to restore the caller's order.
+        if (pm) {
+            launch_scatter_by_id(ctx->id, n, ctx->pos, ctx->pos2, ctx->stream);
+            NB_TRY(cudaMemcpyAsync(pm, ctx->pos2, bytes, kind, ctx->stream), "copy positions out");
+        }
+        if (vel) {
+            launch_scatter_by_id(ctx->id, n, ctx->vel, ctx->vel2, ctx->stream);
+            NB_TRY(cudaMemcpyAsync(vel, ctx->vel2, bytes, kind, ctx->stream), "copy velocities out");
+        }
+    }
+    rc = check_cuda(ctx, cudaGetLastError(), "get bodies");
+    if (rc != NB_OK) return rc;
+    return host ? device_status(ctx) : NB_OK;
+}
+
+int nb_get_bodies(nb_ctx *ctx, float *pos_mass, float *velocity) {
+    return get_state_impl(ctx, pos_mass, velocity, cudaMemcpyDeviceToHost, true);
+}
+
+int nb_get_bodies_device(nb_ctx *ctx, void *d_pos_mass, void *d_velocity) {
+    return get_state_impl(ctx, d_pos_mass, d_velocity, cudaMemcpyDeviceToDevice, false);
+}
+
+static int copy_acc_out(nb_ctx *ctx, void *out, cudaMemcpyKind kind, bool host) {
+    const int64_t n = ctx->n;
+    if (!ctx->have_acc) return fail(ctx, NB_ERR_NO_BODIES, "no accelerations computed yet");
+    if (n > 0) {
+        launch_scatter_by_id(ctx->id, n, ctx->acc, ctx->pos2, ctx->stream);
+        NB_TRY(cudaMemcpyAsync(out, ctx->pos2, (size_t) n * sizeof(float4), kind, ctx->stream), "copy accelerations");
+    }
+    int rc = check_cuda(ctx, cudaGetLastError(), "accelerations out");
+    if (rc != NB_OK) return rc;
+    return host ? device_status(ctx) : NB_OK;
+}
+
+int nb_update_accelerations(nb_ctx *ctx, float *acc_out) {
+    int rc = begin(ctx);
+    if (rc != NB_OK) return rc;
+    Marks mk(ctx);
+    if (ctx->n > 0) {
+        rc = force_pass(ctx, mk);
+        if (rc != NB_OK) return rc;
+    }
+    mk.mark(kIntegrate);
+    mk.mark(kEnd);
+    mk.commit();
+    ctx->have_acc = true;
+    if (acc_out) return copy_acc_out(ctx, acc_out, cudaMemcpyDeviceToHost, true);
+    return NB_OK;
+}
+
+int nb_get_accelerations(nb_ctx *ctx, float *acc_out) {
+    int rc = begin(ctx);
+    if (rc != NB_OK) return rc;
+    if (!acc_out) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "output is NULL");
+    return copy_acc_out(ctx, acc_out, cudaMemcpyDeviceToHost, true);
+}
+
+int nb_get_accelerations_device(nb_ctx *ctx, void *d_acc_out) {
+    int rc = begin(ctx);
+    if (rc != NB_OK) return rc;
+    if (!d_acc_out) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "output is NULL");
+    return copy_acc_out(ctx, d_acc_out, cudaMemcpyDeviceToDevice, false);
+}
+
+int nb_step(nb_ctx *ctx, int32_t steps) {
+    int rc = begin(ctx);
+    if (rc != NB_OK) return rc;
+    if (steps < 0) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "negative step count");
+    for (int32_t k = 0; k < steps; ++k) {
+        Marks mk(ctx);
+        if (ctx->n > 0) {
+            rc = force_pass(ctx, mk);
+            if (rc != NB_OK) return rc;
+            mk.mark(kIntegrate);
+            const bool reduce_box = ctx->cfg.solver != NB_SOLVER_NAIVE;
+            if (reduce_box) launch_bbox_reset(ctx->bbox, ctx->stream);
+            launch_kick_drift(ctx->pos, ctx->vel, ctx->acc, ctx->n, ctx->cfg.time_step,
+                              reduce_box ? ctx->bbox : nullptr, ctx->stream);
+            ctx->bbox_valid = reduce_box;
+            if (ctx->timing) ctx->times.launches += 1;
+            rc = check_cuda(ctx, cudaGetLastError(), "kick-drift");
+            if (rc != NB_OK) return rc;
+        } else {
+            mk.mark(kMorton); mk.mark(kSort); mk.mark(kGather); mk.mark(kBuild); mk.mark(kTraverse);
+            mk.mark(kIntegrate);
+        }
+        mk.mark(kEnd);
+        mk.commit();
+        ctx->have_acc = true;
+    }
+    return NB_OK;
+}
+
+int nb_synchronize(nb_ctx *ctx) {
+    int rc = begin(ctx);
+    if (rc != NB_OK) return rc;
+    return device_status(ctx);
+}
+
+int nb_get_counts(nb_ctx *ctx, nb_counts *out) {
+    int rc = begin(ctx);
+    if (rc != NB_OK) return rc;
+    if (!out) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "output is NULL");
+    unsigned long long c[4] = {0, 0, 0, 0};
+    NB_TRY(cudaMemcpyAsync(c, ctx->counts, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream), "read counts");
+    rc = device_status(ctx);
+    if (rc != NB_OK) return rc;
+    if (ctx->acc_is_bh) {
+        out->particle_particle = c[0];
+        out->node_particle = c[1];
+    } else {
+        out->particle_particle = (uint64_t) ctx->n * (uint64_t) ctx->n;
+        out->node_particle = 0;
+    }
+    out->particle_node = 0;
+    out->node_node = 0;
+    return NB_OK;
+}
+
+int nb_enable_timing(nb_ctx *ctx, int enable) {
+    int rc = begin(ctx);
+    if (rc != NB_OK) return rc;
+    rc = device_status(ctx);
+    ctx->timing = enable != 0;
+    ctx->times = nb_phase_times{};
+    return rc;
+}
+
+int nb_get_phase_times(nb_ctx *ctx, nb_phase_times *out) {
+    int rc = begin(ctx);
+    if (rc != NB_OK) return rc;
+    if (!out) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "output is NULL");
+    rc = device_status(ctx);
+    *out = ctx->times;
+    return rc;
+}
+
+int nb_get_tree(nb_ctx *ctx, int64_t *num_nodes, int32_t *record_floats, uint64_t *sorted_codes, uint32_t *sorted_ids,
+                float *records, float *bbox) {
+    int rc = begin(ctx);
+    if (rc != NB_OK) return rc;
+    if (!ctx->have_tree) return fail(ctx, NB_ERR_NO_BODIES, "no tree has been built");
+    int nn = 0;
+    NB_TRY(cudaMemcpyAsync(&nn, ctx->tw.num_nodes, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream), "read tree");
+    uint32_t box[6];
+    NB_TRY(cudaMemcpyAsync(box, ctx->bbox, sizeof(box), cudaMemcpyDeviceToHost, ctx->stream), "read bbox");
+    rc = device_status(ctx);
+    if (rc != NB_OK) return rc;
+    const int rf = rec_floats(ctx->cfg.order);
+    if (num_nodes) *num_nodes = nn;
+    if (record_floats) *record_floats = rf;
+    if (bbox) {
+        for (int k = 0; k < 3; ++k) {
+            bbox[k] = ordered_to_float(box[k]);
+            bbox[3 + k] = ordered_to_float(~box[3 + k]);
+        }
+    }
+    const int64_t n = ctx->n;
+    if (sorted_codes && n > 0)
+        NB_TRY(cudaMemcpyAsync(sorted_codes, ctx->keys, (size_t) n * 8, cudaMemcpyDeviceToHost, ctx->stream), "codes");
+    if (sorted_ids && n > 0)
+        NB_TRY(cudaMemcpyAsync(sorted_ids, ctx->id, (size_t) n * 4, cudaMemcpyDeviceToHost, ctx->stream), "ids");
+    if (records && nn > 0)
+        NB_TRY(cudaMemcpyAsync(records, ctx->nodes, (size_t) nn * rf * sizeof(float), cudaMemcpyDeviceToHost,
+                               ctx->stream), "records");
+    return device_status(ctx);
+}
+
+int nb_direct_device(nb_ctx *ctx, int64_t n, const void *d_bodies, int64_t nt, const void *d_targets, void *d_acc,
+                     int32_t precision) {
+    int rc = begin(ctx);
+    if (rc != NB_OK) return rc;
+    if (n < 0 || nt < 0 || (n > 0 && !d_bodies) || (nt > 0 && (!d_targets || !d_acc)))
+        return fail(ctx, NB_ERR_INVALID_ARGUMENT, "bad direct-sum arguments");
+    if (precision == 32)
+        launch_direct_f32((const float4 *) d_bodies, n, (const float4 *) d_targets, nt, ctx->cfg.G, ctx->cfg.epsilon,
+                          (float4 *) d_acc, ctx->stream);
+    else if (precision == 64)
+        launch_direct_f64((const float4 *) d_bodies, n, (const float4 *) d_targets, nt, (double) ctx->cfg.G,
+                          (double) ctx->cfg.epsilon, (double *) d_acc, ctx->stream);
+    else
+        return fail(ctx, NB_ERR_INVALID_ARGUMENT, "precision must be 32 or 64");
+    return check_cuda(ctx, cudaGetLastError(), "direct sum");
+}
+
+void *nb_host_alloc(size_t bytes) {
+    void *p = nullptr;
+    if (cudaMallocHost(&p, bytes ? bytes : 1) != cudaSuccess) return nullptr;
+    return p;
+}
+
+void nb_host_free(void *p) {
+    if (p) cudaFreeHost(p);
+}
+
+}  // extern "C"

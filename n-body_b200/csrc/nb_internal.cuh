@@ -1,0 +1,146 @@
+// Internal declarations shared by the sm_100a kernels of the force path.
+//
+// Device data layout (all in HBM, structure of arrays, 16-byte aligned):
+//   bodies      float4 (x, y, z, m)     one per body, in Morton order after each sort
+//   velocities  float4 (vx, vy, vz, 0)
+//   ids         uint32                  input index of the body held in each slot
+//   codes       uint64                  Morton codes, sorted together with a uint32 slot index
+//   nodes       float4[REC] per node    preorder linear BVH, see NodeLayout below
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace nbg {
+
+// ---- bit-exact float helpers (no FMA contraction, IEEE round-to-nearest) ----
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+// glm::min / glm::max semantics: min(x, y) = (y < x) ? y : x, max(x, y) = (x < y) ? y : x
+__device__ __forceinline__ float gmin(float x, float y) { return (y < x) ? y : x; }
+__device__ __forceinline__ float gmax(float x, float y) { return (x < y) ? y : x; }
+
+// Order-preserving map float -> uint32 (for atomicMin/atomicMax on floats).
+__host__ __device__ __forceinline__ uint32_t float_to_ordered(float f) {
+#ifdef __CUDA_ARCH__
+    uint32_t u = __float_as_uint(f);
+#else
+    uint32_t u;
+    __builtin_memcpy(&u, &f, 4);
+#endif
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__host__ __device__ __forceinline__ float ordered_to_float(uint32_t o) {
+    uint32_t u = (o & 0x80000000u) ? (o & 0x7fffffffu) : ~o;
+#ifdef __CUDA_ARCH__
+    return __uint_as_float(u);
+#else
+    float f;
+    __builtin_memcpy(&f, &u, 4);
+    return f;
+#endif
+}
+
+// Global bounding box accumulator: 6 ordered uints, all reduced with atomicMin.
+// [0..2] = ordered(min.xyz), [3..5] = ~ordered(max.xyz). Reset by filling with 0xFF bytes.
+struct BBoxAccum {
+    uint32_t v[6];
+};
+
+// ---- node records (preorder linear BVH) ----
+// rec[0] = (centre.xyz, mac_threshold)   centre = (max + min) / 2 of the node's bounding box;
+//          a target at squared distance d2 from the centre takes the node's approximation iff
+//          d2 >= mac_threshold (bit-identical to diag^2 / d2 < theta^2 of the reference MAC)
+// rec[1] = (centre_of_mass.xyz, mass)
+// order 1: rec[2] = (link0, link1, 0, 0)                        REC = 3
+// order 2: rec[2] = (Qxx, Qxy, Qxz, Qyy), rec[3] = (Qyz, Qzz, link0, link1)   REC = 4
+// link for an internal node: (index after its subtree, -1); for a leaf: (first body, end body).
+template<int ORDER>
+struct NodeLayout;
+template<>
+struct NodeLayout<1> {
+    static constexpr int REC = 3;
+};
+template<>
+struct NodeLayout<2> {
+    static constexpr int REC = 4;
+};
+
+constexpr int kMaxOrder = 2;
+// Deepest possible binary radix tree over 64-bit codes with 32-bit index tie-breaks.
+constexpr int kMaxTreeDepth = 128;
+
+// ---- device-side error reporting ----
+enum DeviceError : uint32_t {
+    kErrNone = 0,
+    kErrLookbackTimeout = 1u << 0,   // onesweep look-back wait exceeded its limit
+    kErrTreeDepth = 1u << 1,         // a walk up the tree exceeded the maximum depth
+    kErrNodeOverflow = 1u << 2,      // more tree nodes than the node buffer holds
+};
+
+// ---- launchers (stream-ordered; defined in the .cu files) ----
+
+// bbox_morton.cu
+void launch_bbox_reset(BBoxAccum *acc, cudaStream_t s);
+void launch_bbox_reduce(const float4 *pos, int64_t n, BBoxAccum *acc, cudaStream_t s);
+void launch_morton_hist(const float4 *pos, int64_t n, const BBoxAccum *acc, uint64_t *codes, uint32_t *hist,
+                        cudaStream_t s);
+
+// radix_sort.cu
+struct SortWorkspace {
+    uint64_t *keys_alt = nullptr;
+    uint32_t *vals_alt = nullptr;
+    uint32_t *hist = nullptr;      // 8 x 256 digit counts, filled by launch_morton_hist
+    uint32_t *offsets = nullptr;   // 8 x 256 exclusive prefixes + 8 trivial-pass flags
+    uint32_t *lookback = nullptr;  // 8 x tiles x 256
+    uint32_t *tile_counter = nullptr;  // 8
+    int64_t capacity = 0;
+};
+int64_t sort_tiles(int64_t n);
+size_t sort_lookback_words(int64_t n);
+// Sorts (keys, iota) by key; the sorted keys and slot indices end in keys/vals (ping-pong inside).
+void launch_radix_sort(uint64_t *keys, uint32_t *vals, int64_t n, SortWorkspace &ws, uint32_t *err,
+                       cudaStream_t s);
+
+// lbvh_build.cu
+struct TreeWorkspace {
+    int2 *range = nullptr;          // n-1 internal Karras nodes: first, last
+    int *left = nullptr, *right = nullptr;  // child encoding: internal i >= 0, Karras leaf j as ~j
+    int *parent = nullptr;          // parent of internal node
+    uint8_t *splittable = nullptr;  // n-1
+    int *visit = nullptr;           // n-1 arrival counters
+    float4 *sbmin = nullptr, *sbmax = nullptr, *scom = nullptr;  // 2n-1 summary slots
+    float4 *sq0 = nullptr, *sq1 = nullptr;                        // quadrupole slots (order >= 2)
+    int *cnt = nullptr;             // subtree node count per slot
+    int *num_nodes = nullptr;       // device scalar: final node count
+    int64_t capacity = 0;
+};
+void launch_build_tree(const uint64_t *sorted_codes, const float4 *bodies, int64_t n, int leaf, int order, float theta,
+                       TreeWorkspace &tw, float4 *nodes, int64_t node_capacity, uint32_t *err, cudaStream_t s);
+
+// traverse.cu
+void launch_bh_traverse(int order, const float4 *nodes, const int *num_nodes, const float4 *bodies, int64_t n_bodies,
+                        const float4 *targets, int64_t n_targets, float G, float eps, float4 *acc,
+                        unsigned long long *counts, cudaStream_t s);
+
+// direct_sum.cu
+void launch_direct_f32(const float4 *bodies, int64_t n, const float4 *targets, int64_t nt, float G, float eps,
+                       float4 *acc, cudaStream_t s);
+void launch_direct_f64(const float4 *bodies, int64_t n, const float4 *targets, int64_t nt, double G, double eps,
+                       double *acc3, cudaStream_t s);
+
+// integrate.cu
+void launch_gather_state(const uint32_t *perm, int64_t n, const float4 *pos, const float4 *vel, const uint32_t *id,
+                         float4 *pos_out, float4 *vel_out, uint32_t *id_out, cudaStream_t s);
+void launch_scatter_by_id(const uint32_t *id, int64_t n, const float4 *src, float4 *dst, cudaStream_t s);
+void launch_kick_drift(float4 *pos, float4 *vel, const float4 *acc, int64_t n, float dt, BBoxAccum *next_bbox,
+                       cudaStream_t s);
+void launch_iota(uint32_t *id, int64_t n, cudaStream_t s);
+
+// Largest number of bodies one context accepts (30-bit counts in the sort's look-back words,
+// 31-bit body indices in the tree).
+constexpr int64_t kMaxBodies = (int64_t(1) << 30) - 1;
+
+}  // namespace nbg

@@ -1,0 +1,118 @@
+"""Seeded synthetic scenarios (host-side input data, not part of the force path).
+
+The reference measures on AGORA/MUGS snapshots that are not available here; these generators
+produce inputs with the configured shapes instead. All return float32 arrays of shape (n, 4):
+bodies as (x, y, z, m) and velocities as (vx, vy, vz, 0). G = 1 throughout.
+
+  uniform_ball   positions uniform in the unit ball (rejection from [-1, 1]^3), masses uniform
+                 in [0.5, 1.5] / n, zero velocities
+  plummer        Plummer sphere (scale radius a, total mass M): radii from the inverse cumulative
+                 mass r = a (X^(-2/3) - 1)^(-1/2), truncated at r_max; isotropic speeds from the
+                 distribution function by von Neumann rejection (Aarseth, Henon & Wielen 1974)
+  hernquist      Hernquist sphere: r = a sqrt(X) / (1 - sqrt(X)), truncated at r_max; isotropic
+                 speeds by rejection from the Hernquist (1990) ergodic distribution function
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _rng(seed: int) -> np.random.Generator:
+    return np.random.Generator(np.random.MT19937(seed))
+
+
+def _isotropic(rng: np.random.Generator, n: int) -> np.ndarray:
+    cos_t = rng.uniform(-1.0, 1.0, n)
+    phi = rng.uniform(0.0, 2.0 * np.pi, n)
+    sin_t = np.sqrt(1.0 - cos_t * cos_t)
+    return np.stack([sin_t * np.cos(phi), sin_t * np.sin(phi), cos_t], axis=1)
+
+
+def _pack(pos: np.ndarray, mass: np.ndarray, vel: np.ndarray):
+    n = len(pos)
+    bodies = np.zeros((n, 4), np.float32)
+    bodies[:, :3] = pos
+    bodies[:, 3] = mass
+    velocities = np.zeros((n, 4), np.float32)
+    velocities[:, :3] = vel
+    return bodies, velocities
+
+
+def uniform_ball(n: int, seed: int = 42):
+    rng = _rng(seed)
+    pts = np.zeros((0, 3))
+    while len(pts) < n:
+        c = rng.uniform(-1.0, 1.0, (max(2 * (n - len(pts)), 16), 3))
+        pts = np.concatenate([pts, c[(c * c).sum(1) < 1.0]])
+    mass = rng.uniform(0.5, 1.5, n) / n
+    return _pack(pts[:n], mass, np.zeros((n, 3)))
+
+
+def plummer(n: int, seed: int = 43, a: float = 1.0, M: float = 1.0, r_max: float = 100.0):
+    rng = _rng(seed)
+    r = np.zeros(0)
+    while len(r) < n:
+        X = rng.uniform(0.0, 1.0, n - len(r))
+        X = X[(X > 0.0)]
+        rr = a / np.sqrt(X ** (-2.0 / 3.0) - 1.0)
+        r = np.concatenate([r, rr[rr <= r_max * a]])
+    r = r[:n]
+    pos = r[:, None] * _isotropic(rng, n)
+    # speed fraction q = v / v_esc with density g(q) = q^2 (1 - q^2)^(7/2) (max < 0.1)
+    q = np.zeros(0)
+    while len(q) < n:
+        qq = rng.uniform(0.0, 1.0, 2 * (n - len(q)) + 16)
+        yy = rng.uniform(0.0, 0.1, len(qq))
+        q = np.concatenate([q, qq[yy < qq * qq * (1.0 - qq * qq) ** 3.5]])
+    q = q[:n]
+    v_esc = np.sqrt(2.0 * M / a) * (1.0 + (r / a) ** 2) ** -0.25
+    vel = (q * v_esc)[:, None] * _isotropic(rng, n)
+    pos -= pos.mean(0)
+    vel -= vel.mean(0)
+    return _pack(pos, np.full(n, M / n), vel)
+
+
+def _hernquist_df(E: np.ndarray) -> np.ndarray:
+    """Hernquist (1990) ergodic DF for G = M = a = 1, q = sqrt(-E) in (0, 1), up to a constant."""
+    q = np.sqrt(np.clip(-E, 0.0, 1.0 - 1e-12))
+    qq = q * q
+    return (3.0 * np.arcsin(q) + q * np.sqrt(1.0 - qq) * (1.0 - 2.0 * qq) * (8.0 * qq * qq - 8.0 * qq - 3.0)) \
+        / (1.0 - qq) ** 2.5
+
+
+def hernquist(n: int, seed: int = 44, a: float = 1.0, M: float = 1.0, r_max: float = 100.0):
+    rng = _rng(seed)
+    r = np.zeros(0)
+    while len(r) < n:
+        X = rng.uniform(0.0, 1.0, n - len(r))
+        s = np.sqrt(X)
+        rr = a * s / np.maximum(1.0 - s, 1e-300)
+        r = np.concatenate([r, rr[rr <= r_max * a]])
+    r = r[:n]
+    pos = r[:, None] * _isotropic(rng, n)
+    # speeds by rejection from p(v) ~ v^2 f(psi - v^2/2), psi = 1 / (1 + r) in units G = M = a = 1
+    psi = (M / a) / (1.0 + r / a)
+    v_esc = np.sqrt(2.0 * psi)
+    speed = np.zeros(n)
+    todo = np.arange(n)
+    while len(todo):
+        u = rng.uniform(0.0, 1.0, len(todo))
+        v = u * v_esc[todo]
+        E = 0.5 * v * v - psi[todo]
+        p = (u * u) * _hernquist_df(E / (M / a))
+        # bound: the density in u peaks below u^2 f(-psi) at u = 0 .. 1; use f(-psi) as envelope
+        env = _hernquist_df(-psi[todo] / (M / a))
+        y = rng.uniform(0.0, 1.0, len(todo)) * env
+        ok = y < p
+        speed[todo[ok]] = v[ok]
+        todo = todo[~ok]
+    vel = speed[:, None] * _isotropic(rng, n)
+    pos -= pos.mean(0)
+    vel -= vel.mean(0)
+    return _pack(pos, np.full(n, M / n), vel)
+
+
+def softening_to_epsilon(softening_length: float) -> float:
+    """A configured softening length e enters the reference's Gravity as epsilon = e^2, since
+    Gravity adds epsilon to r^2 (Gravity.h:207)."""
+    return float(np.float32(softening_length) * np.float32(softening_length))
