@@ -262,9 +262,10 @@ def test_device_direct_sum_f64(nb, oracle):
     with make_solver(nb, pm[:1], eps=1e-4) as s:
         s.direct_device(len(pm), dpm.data_ptr(), len(idx), dt.data_ptr(), out.data_ptr(), 64)
         s.synchronize()
-    ref = oracle.direct_f64(pm, idx=idx, eps=1e-4)
+    # the device kernel widens the float epsilon of the rule; give the oracle the same value
+    ref = oracle.direct_f64(pm, idx=idx, eps=float(np.float32(1e-4)))
     got = out.cpu().numpy()
-    assert np.abs(got - ref).max() <= 1e-10 * np.abs(ref).max()
+    assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max()
 
 
 def test_repeatable(nb):
