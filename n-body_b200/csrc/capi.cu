@@ -53,8 +53,8 @@ struct nb_ctx {
     uint32_t *vals = nullptr;
     SortWorkspace sw;
     TreeWorkspace tw;
-    float4 *nodes = nullptr;
-    int64_t node_cap = 0;
+    NodeArrays nodes;
+    TraverseWorkspace trav;
     BBoxAccum *bbox = nullptr;
     unsigned long long *counts = nullptr;
     uint32_t *err = nullptr;
@@ -92,7 +92,9 @@ int check_cuda(nb_ctx *c, cudaError_t e, const char *what) {
         if (_rc != NB_OK) return _rc;                       \
     } while (0)
 
-int rec_floats(int order) { return 4 * (order == 1 ? NodeLayout<1>::REC : NodeLayout<2>::REC); }
+// Exported record: mac (4 floats), link (2 ints + 2 zero), payload (4 floats per PAY entry).
+int pay_float4s(int order) { return order == 1 ? NodeLayout<1>::PAY : NodeLayout<2>::PAY; }
+int rec_floats(int order) { return 8 + 4 * pay_float4s(order); }
 
 void refresh_names(nb_ctx *ctx) {
     if (ctx->cfg.solver == NB_SOLVER_NAIVE) {
@@ -126,9 +128,9 @@ void free_buffers(nb_ctx *ctx) {
     dev_free(ctx->tw.range); dev_free(ctx->tw.left); dev_free(ctx->tw.right); dev_free(ctx->tw.parent);
     dev_free(ctx->tw.splittable); dev_free(ctx->tw.visit); dev_free(ctx->tw.sbmin); dev_free(ctx->tw.sbmax);
     dev_free(ctx->tw.scom); dev_free(ctx->tw.sq0); dev_free(ctx->tw.sq1); dev_free(ctx->tw.cnt);
-    dev_free(ctx->nodes);
+    dev_free(ctx->nodes.mac); dev_free(ctx->nodes.link); dev_free(ctx->nodes.pay);
+    ctx->nodes.capacity = 0;
     ctx->cap = 0;
-    ctx->node_cap = 0;
 }
 
 int ensure_capacity(nb_ctx *ctx, int64_t n) {
@@ -162,8 +164,11 @@ int ensure_capacity(nb_ctx *ctx, int64_t n) {
     NB_TRY(dev_alloc(&ctx->tw.sq1, slots), "alloc summaries");
     NB_TRY(dev_alloc(&ctx->tw.cnt, slots), "alloc summaries");
     ctx->tw.capacity = c;
-    ctx->node_cap = 2 * c;
-    NB_TRY(dev_alloc(&ctx->nodes, (size_t) ctx->node_cap * NodeLayout<2>::REC), "alloc tree nodes");
+    const int64_t node_cap = 2 * c;
+    NB_TRY(dev_alloc(&ctx->nodes.mac, (size_t) node_cap), "alloc tree nodes");
+    NB_TRY(dev_alloc(&ctx->nodes.link, (size_t) node_cap), "alloc tree nodes");
+    NB_TRY(dev_alloc(&ctx->nodes.pay, (size_t) node_cap * NodeLayout<2>::PAY), "alloc tree nodes");
+    ctx->nodes.capacity = node_cap;
     ctx->cap = c;
     return NB_OK;
 }
@@ -256,10 +261,10 @@ int force_pass(nb_ctx *ctx, Marks &mk) {
     std::swap(ctx->id, ctx->id2);
     mk.mark(kBuild);
     launch_build_tree(ctx->keys, ctx->pos, n, ctx->cfg.max_leaf_size, ctx->cfg.order, ctx->cfg.theta, ctx->tw,
-                      ctx->nodes, ctx->node_cap, ctx->err, s);
+                      ctx->nodes, ctx->err, s);
     mk.mark(kTraverse);
     launch_bh_traverse(ctx->cfg.order, ctx->nodes, ctx->tw.num_nodes, ctx->pos, n, ctx->pos, n, ctx->cfg.G,
-                       ctx->cfg.epsilon, ctx->acc, ctx->counts, s);
+                       ctx->cfg.epsilon, ctx->acc, ctx->counts, ctx->trav, ctx->err, s);
     ctx->have_tree = true;
     ctx->acc_is_bh = true;
     if (ctx->timing) ctx->times.launches += launches_per_pass(ctx, need_bbox, false);
@@ -275,6 +280,8 @@ int device_status(nb_ctx *ctx) {
         return fail(ctx, NB_ERR_DEVICE_TIMEOUT, "radix sort look-back wait exceeded its limit");
     if (e & kErrNodeOverflow) return fail(ctx, NB_ERR_DEVICE_CHECK, "tree node buffer overflow");
     if (e & kErrTreeDepth) return fail(ctx, NB_ERR_DEVICE_CHECK, "tree walk exceeded the maximum depth");
+    if (e & kErrStackOverflow) return fail(ctx, NB_ERR_DEVICE_CHECK, "traversal stack overflow");
+    if (e & kErrTraverseLimit) return fail(ctx, NB_ERR_DEVICE_CHECK, "traversal met an invalid tree link");
     return NB_OK;
 }
 
@@ -330,6 +337,12 @@ int nb_create(const nb_config *cfg, nb_ctx **out) {
         nb_destroy(ctx);
         return NB_ERR_OUT_OF_MEMORY;
     }
+    ctx->trav.warps = traverse_resident_warps(cfg->device);
+    if (dev_alloc(&ctx->trav.stack, (size_t) ctx->trav.warps * kTraverseStack) != cudaSuccess ||
+        dev_alloc(&ctx->trav.group_counter, 1) != cudaSuccess) {
+        nb_destroy(ctx);
+        return NB_ERR_OUT_OF_MEMORY;
+    }
     cudaMemsetAsync(ctx->err, 0, sizeof(uint32_t), ctx->stream);
     cudaMemsetAsync(ctx->counts, 0, 4 * sizeof(unsigned long long), ctx->stream);
     cudaMemsetAsync(ctx->tw.num_nodes, 0, sizeof(int), ctx->stream);
@@ -345,6 +358,7 @@ int nb_destroy(nb_ctx *ctx) {
     free_buffers(ctx);
     dev_free(ctx->bbox); dev_free(ctx->counts); dev_free(ctx->err); dev_free(ctx->sw.hist);
     dev_free(ctx->sw.offsets); dev_free(ctx->sw.tile_counter); dev_free(ctx->tw.num_nodes); dev_free(ctx->acc64);
+    dev_free(ctx->trav.stack); dev_free(ctx->trav.group_counter);
     for (auto &ev: ctx->pending) ctx->event_pool.insert(ctx->event_pool.end(), ev.begin(), ev.end());
     for (auto e: ctx->event_pool) cudaEventDestroy(e);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -587,9 +601,27 @@ int nb_get_tree(nb_ctx *ctx, int64_t *num_nodes, int32_t *record_floats, uint64_
         NB_TRY(cudaMemcpyAsync(sorted_codes, ctx->keys, (size_t) n * 8, cudaMemcpyDeviceToHost, ctx->stream), "codes");
     if (sorted_ids && n > 0)
         NB_TRY(cudaMemcpyAsync(sorted_ids, ctx->id, (size_t) n * 4, cudaMemcpyDeviceToHost, ctx->stream), "ids");
-    if (records && nn > 0)
-        NB_TRY(cudaMemcpyAsync(records, ctx->nodes, (size_t) nn * rf * sizeof(float), cudaMemcpyDeviceToHost,
+    if (records && nn > 0) {
+        const int pf = pay_float4s(ctx->cfg.order);
+        std::vector<float4> mac((size_t) nn), pay((size_t) nn * pf);
+        std::vector<int2> link((size_t) nn);
+        NB_TRY(cudaMemcpyAsync(mac.data(), ctx->nodes.mac, (size_t) nn * sizeof(float4), cudaMemcpyDeviceToHost,
                                ctx->stream), "records");
+        NB_TRY(cudaMemcpyAsync(link.data(), ctx->nodes.link, (size_t) nn * sizeof(int2), cudaMemcpyDeviceToHost,
+                               ctx->stream), "records");
+        NB_TRY(cudaMemcpyAsync(pay.data(), ctx->nodes.pay, (size_t) nn * pf * sizeof(float4), cudaMemcpyDeviceToHost,
+                               ctx->stream), "records");
+        rc = device_status(ctx);
+        if (rc != NB_OK) return rc;
+        for (int64_t k = 0; k < nn; ++k) {
+            float *r = records + k * rf;
+            std::memcpy(r, &mac[k], 16);
+            std::memcpy(r + 4, &link[k], 8);
+            r[6] = 0.f;
+            r[7] = 0.f;
+            std::memcpy(r + 8, &pay[k * pf], (size_t) pf * 16);
+        }
+    }
     return device_status(ctx);
 }
 

@@ -22,7 +22,9 @@
 //                     are single IEEE operations in the reference's order, so summaries are
 //                     bit-identical to the CPU restatement.
 //   emit_kernel       preorder index of every final node (walk to the root adding left-sibling
-//                     subtree sizes) and the packed 48/64-byte node record the traversal reads.
+//                     subtree sizes) and the node arrays the traversal reads: MAC data (centre and
+//                     exact MAC threshold), links (right child / leaf body range) and payload
+//                     (centre of mass, mass, quadrupole).
 #include <cfloat>
 
 #include "nb_internal.cuh"
@@ -242,32 +244,31 @@ __device__ float mac_threshold(float a, float t) {
 }
 
 template<int ORDER>
-__device__ void write_record(float4 *__restrict__ nodes, int64_t cap, int pre, const Summ<ORDER> &s, float t,
-                             int link0, int link1, uint32_t *err) {
-    if (pre < 0 || pre >= cap) {
+__device__ void write_record(const NodeArrays &nodes, int pre, const Summ<ORDER> &s, float t, int link0, int link1,
+                             uint32_t *err) {
+    if (pre < 0 || pre >= nodes.capacity) {
         atomicOr(err, (uint32_t) kErrNodeOverflow);
         return;
     }
-    constexpr int REC = NodeLayout<ORDER>::REC;
-    float4 *r = nodes + (int64_t) pre * REC;
+    constexpr int PAY = NodeLayout<ORDER>::PAY;
     float cx = fdiv(fadd(s.bmax[0], s.bmin[0]), 2.0f);
     float cy = fdiv(fadd(s.bmax[1], s.bmin[1]), 2.0f);
     float cz = fdiv(fadd(s.bmax[2], s.bmin[2]), 2.0f);
     float dx = fsub(s.bmax[0], s.bmin[0]), dy = fsub(s.bmax[1], s.bmin[1]), dz = fsub(s.bmax[2], s.bmin[2]);
     float diag2 = fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz));
-    r[0] = make_float4(cx, cy, cz, mac_threshold(diag2, t));
-    r[1] = make_float4(s.com[0], s.com[1], s.com[2], s.M);
-    if constexpr (ORDER == 1) {
-        r[2] = make_float4(__int_as_float(link0), __int_as_float(link1), 0.f, 0.f);
-    } else {
-        r[2] = make_float4(s.q[0], s.q[1], s.q[2], s.q[3]);
-        r[3] = make_float4(s.q[4], s.q[5], __int_as_float(link0), __int_as_float(link1));
+    nodes.mac[pre] = make_float4(cx, cy, cz, mac_threshold(diag2, t));
+    nodes.link[pre] = make_int2(link0, link1);
+    float4 *p = nodes.pay + (int64_t) pre * PAY;
+    p[0] = make_float4(s.com[0], s.com[1], s.com[2], s.M);
+    if constexpr (ORDER >= 2) {
+        p[1] = make_float4(s.q[0], s.q[1], s.q[2], s.q[3]);
+        p[2] = make_float4(s.q[4], s.q[5], 0.f, 0.f);
     }
 }
 
 template<int ORDER>
-__global__ void __launch_bounds__(kThreads) emit_kernel(int n, TreeWorkspace tw, float t, float4 *__restrict__ nodes,
-                                                        int64_t cap, uint32_t *err) {
+__global__ void __launch_bounds__(kThreads) emit_kernel(int n, TreeWorkspace tw, float t, NodeArrays nodes,
+                                                        uint32_t *err) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1 || !tw.splittable[i]) return;
     int pre = 0;
@@ -282,37 +283,35 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(int n, TreeWorkspace tw,
         if (tw.right[p] == u) pre += tw.cnt[slot_of(tw.left[p], n)];
         u = p;
     }
-    const int cnt_i = tw.cnt[i];
-    write_record<ORDER>(nodes, cap, pre, load_slot<ORDER>(tw, i), t, pre + cnt_i, -1, err);
     const int lc = tw.left[i], rc = tw.right[i];
     const int lslot = slot_of(lc, n);
+    const int right_pre = pre + 1 + tw.cnt[lslot];
+    write_record<ORDER>(nodes, pre, load_slot<ORDER>(tw, i), t, right_pre, -1, err);
     if (is_final_leaf(tw.splittable, lc)) {
         int2 r = lc < 0 ? make_int2(~lc, ~lc) : tw.range[lc];
-        write_record<ORDER>(nodes, cap, pre + 1, load_slot<ORDER>(tw, lslot), t, r.x, r.y + 1, err);
+        write_record<ORDER>(nodes, pre + 1, load_slot<ORDER>(tw, lslot), t, r.x, r.y + 1, err);
     }
     if (is_final_leaf(tw.splittable, rc)) {
         int2 r = rc < 0 ? make_int2(~rc, ~rc) : tw.range[rc];
-        write_record<ORDER>(nodes, cap, pre + 1 + tw.cnt[lslot], load_slot<ORDER>(tw, slot_of(rc, n)), t, r.x,
-                            r.y + 1, err);
+        write_record<ORDER>(nodes, right_pre, load_slot<ORDER>(tw, slot_of(rc, n)), t, r.x, r.y + 1, err);
     }
-    if (i == 0) *tw.num_nodes = cnt_i;
+    if (i == 0) *tw.num_nodes = tw.cnt[i];
 }
 
 // The whole tree is one leaf when n == 1, or when the root is not splittable (n <= maxLeafSize
 // or every code equal).
 template<int ORDER>
 __global__ void root_leaf_kernel(const float4 *__restrict__ bodies, int n, TreeWorkspace tw, float t,
-                                 float4 *__restrict__ nodes, int64_t cap, uint32_t *err) {
+                                 NodeArrays nodes, uint32_t *err) {
     if (n > 1 && tw.splittable[0]) return;
-    write_record<ORDER>(nodes, cap, 0, leaf_summary<ORDER>(bodies, 0, n - 1), t, 0, n, err);
+    write_record<ORDER>(nodes, 0, leaf_summary<ORDER>(bodies, 0, n - 1), t, 0, n, err);
     *tw.num_nodes = 1;
 }
 
 }  // namespace
 
 void launch_build_tree(const uint64_t *sorted_codes, const float4 *bodies, int64_t n64, int leaf, int order,
-                       float theta, TreeWorkspace &tw, float4 *nodes, int64_t node_capacity, uint32_t *err,
-                       cudaStream_t s) {
+                       float theta, TreeWorkspace &tw, const NodeArrays &nodes, uint32_t *err, cudaStream_t s) {
     const int n = (int) n64;
     if (n <= 0) {
         cudaMemsetAsync(tw.num_nodes, 0, sizeof(int), s);
@@ -329,15 +328,15 @@ void launch_build_tree(const uint64_t *sorted_codes, const float4 *bodies, int64
     if (order == 1) {
         if (internal > 0) {
             summarize_kernel<1><<<blocks, kThreads, 0, s>>>(bodies, n, tw, err);
-            emit_kernel<1><<<blocks, kThreads, 0, s>>>(n, tw, t, nodes, node_capacity, err);
+            emit_kernel<1><<<blocks, kThreads, 0, s>>>(n, tw, t, nodes, err);
         }
-        root_leaf_kernel<1><<<1, 1, 0, s>>>(bodies, n, tw, t, nodes, node_capacity, err);
+        root_leaf_kernel<1><<<1, 1, 0, s>>>(bodies, n, tw, t, nodes, err);
     } else {
         if (internal > 0) {
             summarize_kernel<2><<<blocks, kThreads, 0, s>>>(bodies, n, tw, err);
-            emit_kernel<2><<<blocks, kThreads, 0, s>>>(n, tw, t, nodes, node_capacity, err);
+            emit_kernel<2><<<blocks, kThreads, 0, s>>>(n, tw, t, nodes, err);
         }
-        root_leaf_kernel<2><<<1, 1, 0, s>>>(bodies, n, tw, t, nodes, node_capacity, err);
+        root_leaf_kernel<2><<<1, 1, 0, s>>>(bodies, n, tw, t, nodes, err);
     }
 }
 

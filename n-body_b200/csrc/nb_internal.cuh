@@ -49,23 +49,29 @@ struct BBoxAccum {
     uint32_t v[6];
 };
 
-// ---- node records (preorder linear BVH) ----
-// rec[0] = (centre.xyz, mac_threshold)   centre = (max + min) / 2 of the node's bounding box;
-//          a target at squared distance d2 from the centre takes the node's approximation iff
-//          d2 >= mac_threshold (bit-identical to diag^2 / d2 < theta^2 of the reference MAC)
-// rec[1] = (centre_of_mass.xyz, mass)
-// order 1: rec[2] = (link0, link1, 0, 0)                        REC = 3
-// order 2: rec[2] = (Qxx, Qxy, Qxz, Qyy), rec[3] = (Qyz, Qzz, link0, link1)   REC = 4
-// link for an internal node: (index after its subtree, -1); for a leaf: (first body, end body).
+// ---- node records (preorder linear BVH), three arrays indexed by preorder position ----
+// mac[c]  = (centre.xyz, mac_threshold): centre = (max + min) / 2 of the node's bounding box;
+//           a target at squared distance d2 from the centre takes the node's approximation iff
+//           d2 >= mac_threshold (bit-identical to diag^2 / d2 < theta^2 of the reference MAC)
+// link[c] = internal node: (preorder index of the right child, -1); the left child is c + 1
+//           leaf:          (first body, end body) of its range in Morton order
+// pay[c * PAY + k]: k = 0: (centre_of_mass.xyz, mass); order 2 adds k = 1: (Qxx, Qxy, Qxz, Qyy),
+//           k = 2: (Qyz, Qzz, 0, 0) - moments about the centre of mass, not traceless.
 template<int ORDER>
 struct NodeLayout;
 template<>
 struct NodeLayout<1> {
-    static constexpr int REC = 3;
+    static constexpr int PAY = 1;
 };
 template<>
 struct NodeLayout<2> {
-    static constexpr int REC = 4;
+    static constexpr int PAY = 3;
+};
+struct NodeArrays {
+    float4 *mac = nullptr;
+    int2 *link = nullptr;
+    float4 *pay = nullptr;
+    int64_t capacity = 0;
 };
 
 constexpr int kMaxOrder = 2;
@@ -78,6 +84,8 @@ enum DeviceError : uint32_t {
     kErrLookbackTimeout = 1u << 0,   // onesweep look-back wait exceeded its limit
     kErrTreeDepth = 1u << 1,         // a walk up the tree exceeded the maximum depth
     kErrNodeOverflow = 1u << 2,      // more tree nodes than the node buffer holds
+    kErrStackOverflow = 1u << 3,     // traversal stack full (a push was dropped)
+    kErrTraverseLimit = 1u << 4,     // traversal met an invalid link or exceeded its round limit
 };
 
 // ---- launchers (stream-ordered; defined in the .cu files) ----
@@ -118,12 +126,20 @@ struct TreeWorkspace {
     int64_t capacity = 0;
 };
 void launch_build_tree(const uint64_t *sorted_codes, const float4 *bodies, int64_t n, int leaf, int order, float theta,
-                       TreeWorkspace &tw, float4 *nodes, int64_t node_capacity, uint32_t *err, cudaStream_t s);
+                       TreeWorkspace &tw, const NodeArrays &nodes, uint32_t *err, cudaStream_t s);
 
 // traverse.cu
-void launch_bh_traverse(int order, const float4 *nodes, const int *num_nodes, const float4 *bodies, int64_t n_bodies,
+struct TraverseWorkspace {
+    int2 *stack = nullptr;            // per resident warp: kTraverseStack entries of (node, target mask)
+    unsigned *group_counter = nullptr;
+    int64_t warps = 0;                // resident warps the stack memory was sized for
+};
+constexpr int kTraverseStack = 4608;
+// Resident warps of the persistent traversal grid on `device` (for sizing TraverseWorkspace).
+int64_t traverse_resident_warps(int device);
+void launch_bh_traverse(int order, const NodeArrays &nodes, const int *num_nodes, const float4 *bodies, int64_t n_bodies,
                         const float4 *targets, int64_t n_targets, float G, float eps, float4 *acc,
-                        unsigned long long *counts, cudaStream_t s);
+                        unsigned long long *counts, TraverseWorkspace &ws, uint32_t *err, cudaStream_t s);
 
 // direct_sum.cu
 void launch_direct_f32(const float4 *bodies, int64_t n, const float4 *targets, int64_t nt, float G, float eps,

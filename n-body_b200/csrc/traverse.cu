@@ -1,26 +1,39 @@
-// Barnes-Hut traversal of the preorder linear BVH: one warp walks the tree for 32 Morton-adjacent
-// targets in lock step, without a stack.
+// Barnes-Hut traversal of the preorder linear BVH for groups of 32 Morton-adjacent targets, one
+// warp per group, in a persistent grid.
 //
 // Semantics are those of Descent::activeTree (src/NBody/Simulation/Solvers/Descent/activeTree.h:24-79)
 // under DiagonalOverCenterDistance (DiagonalOverCenterDistance.h:18-22) with the Gravity rule
-// (src/NBody/Physics/Rules/Gravity.h:199-259), decided per target:
-//   - a node is approximated for a target iff diag^2 / |centre - p|^2 < theta^2; the node record
-//     carries the exact threshold on |centre - p|^2, and the squared distance is formed with the
-//     reference's IEEE operation order, so every target takes exactly the reference's decisions
-//     (and the interaction counts match the reference's SimpleTrackingRule counts exactly);
-//   - an opened leaf interacts pairwise with its bodies (including the target itself, which
-//     contributes zero);
-//   - otherwise the children are visited.
+// (src/NBody/Physics/Rules/Gravity.h:199-259), decided per target: a node is approximated for a
+// target iff diag^2 / |centre - p|^2 < theta^2 (the node carries the exact threshold on
+// |centre - p|^2, and squared distances are formed in the reference's IEEE operation order), an
+// opened leaf interacts pairwise with all its bodies, otherwise the children are visited. Every
+// target therefore takes exactly the reference's decisions, and the interaction counts equal the
+// reference's SimpleTrackingRule counts.
 //
-// Lock-step without a stack: nodes are stored in preorder with a "skip" index (first node after
-// the subtree). Each lane keeps the next preorder node it needs; the warp processes the smallest
-// such node (one redux.sync), so every lane sees its own visit sequence in order, node records
-// are broadcast loads shared by the whole warp, and leaf bodies are loaded once per warp.
+// Work organisation (per warp, 32 targets, 32-bit target masks):
+//   1. Chunked traversal: up to 32 (node, mask) entries are popped from the warp's stack, one per
+//      lane. Each lane classifies its node against the bounding box of the group's targets:
+//        accept-all  if even the box point nearest the centre passes the MAC,
+//        open-all    if even the farthest box corner fails it,
+//        mixed       otherwise.
+//      Rounding is monotone, so the rounded squared distance of every target lies between the
+//      nearest and farthest values computed with the same operation sequence: the group decision
+//      is exact for every target, not a heuristic.
+//   2. Mixed nodes are batched and resolved lane-parallel: each lane takes one node and tests the
+//      32 targets (broadcast from shared memory), producing accept and open masks.
+//   3. Accepted (node, mask) entries and opened (leaf, mask) entries go to short shared-memory
+//      lists that are evaluated densely: every lane reads the same node or body (broadcast load)
+//      and computes the term for its own target where its mask bit is set. Opened internal nodes
+//      push both children.
+// The expensive terms thus run without traversal bookkeeping between them, and the per-node
+// traversal cost is spread over 32 nodes per instruction.
 //
-// Arithmetic: FP32, one MUFU rsqrt per interaction, G applied once per target. The pair term is
-// 12 FP32 instructions (20 flops by the usual direct-sum convention); the quadrupole node term
-// (non-traceless moments about the centre of mass, as in Gravity.h:239-259 with D<3> contracted
-// analytically: (D3:Q)_i = g3 R_i (R.Q.R) + g2 (2 (Q R)_i + R_i tr Q)) is 56 flops.
+// Arithmetic: FP32, one MUFU rsqrt per interaction, G applied once per target. Pair term:
+// 20 flops by the usual direct-sum convention (12 FP32 instructions + rsqrt). Quadrupole node
+// term (non-traceless moments about the centre of mass, Gravity.h:239-259, with D<3> contracted
+// analytically: (D3:Q)_i = g3 R_i (R.Q.R) + g2 (2 (Q R)_i + R_i tr Q)): 56 flops.
+#include <algorithm>
+#include <cfloat>
 #include <climits>
 
 #include "nb_internal.cuh"
@@ -30,11 +43,37 @@ namespace nbg {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kList = 64;          // capacity of each per-warp list; rounds append at most 32
+constexpr unsigned kFull = 0xffffffffu;
+
+enum : int { kNone = 0, kAcceptAll = 1, kOpenAll = 2, kMixed = 3 };
+
+struct WarpLists {
+    float4 tpos[32];
+    int approx_node[kList];
+    uint32_t approx_mask[kList];
+    int pp_begin[kList], pp_end[kList];
+    uint32_t pp_mask[kList];
+    int mixed_node[kList];
+    uint32_t mixed_mask[kList];
+};
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Squared distance in the reference's IEEE order: (dx*dx + dy*dy) + dz*dz, d = p - c.
+__device__ __forceinline__ float ref_dist2(float px, float py, float pz, float4 c) {
+    const float dx = fsub(px, c.x), dy = fsub(py, c.y), dz = fsub(pz, c.z);
+    return fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz));
+}
 
 template<bool EPS0>
-__device__ __forceinline__ void pair_term(float px, float py, float pz, float4 b, float eps, float &ax, float &ay,
-                                          float &az) {
-    const float rx = px - b.x, ry = py - b.y, rz = pz - b.z;
+__device__ __forceinline__ void pair_term(float4 p, float4 b, float eps, float &ax, float &ay, float &az) {
+    const float rx = p.x - b.x, ry = p.y - b.y, rz = p.z - b.z;
     const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps)));
     if (EPS0 && r2 == 0.f) return;  // equal positions contribute nothing (Gravity.h:203)
     const float inv = rsqrtf(r2);
@@ -45,9 +84,9 @@ __device__ __forceinline__ void pair_term(float px, float py, float pz, float4 b
 }
 
 template<bool EPS0>
-__device__ __forceinline__ void quad_term(float px, float py, float pz, float4 com, const float q[6], float eps,
-                                          float &ax, float &ay, float &az) {
-    const float rx = px - com.x, ry = py - com.y, rz = pz - com.z;
+__device__ __forceinline__ void quad_term(float4 p, float4 com, float4 q0, float4 q1, float eps, float &ax,
+                                          float &ay, float &az) {
+    const float rx = p.x - com.x, ry = p.y - com.y, rz = p.z - com.z;
     const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps)));
     if (EPS0 && r2 == 0.f) return;
     const float inv = rsqrtf(r2);
@@ -55,11 +94,11 @@ __device__ __forceinline__ void quad_term(float px, float py, float pz, float4 c
     const float inv3 = inv2 * inv;
     const float inv5 = inv3 * inv2;
     const float inv7 = inv5 * inv2;
-    const float qx = fmaf(q[0], rx, fmaf(q[1], ry, q[2] * rz));
-    const float qy = fmaf(q[1], rx, fmaf(q[3], ry, q[4] * rz));
-    const float qz = fmaf(q[2], rx, fmaf(q[4], ry, q[5] * rz));
+    const float qx = fmaf(q0.x, rx, fmaf(q0.y, ry, q0.z * rz));
+    const float qy = fmaf(q0.y, rx, fmaf(q0.w, ry, q1.x * rz));
+    const float qz = fmaf(q0.z, rx, fmaf(q1.x, ry, q1.y * rz));
     const float rqr = fmaf(rx, qx, fmaf(ry, qy, rz * qz));
-    const float tr = q[0] + q[3] + q[5];
+    const float tr = q0.x + q0.w + q1.y;
     const float sr = fmaf(-7.5f * inv7, rqr, fmaf(1.5f * inv5, tr, -com.w * inv3));
     const float sq = 3.0f * inv5;
     ax = fmaf(rx, sr, fmaf(qx, sq, ax));
@@ -67,73 +106,256 @@ __device__ __forceinline__ void quad_term(float px, float py, float pz, float4 c
     az = fmaf(rz, sr, fmaf(qz, sq, az));
 }
 
+// Warp-wide ordered append: returns this lane's slot (valid where pred) and advances count.
+__device__ __forceinline__ int warp_append(bool pred, int &count, uint32_t lt) {
+    const uint32_t b = __ballot_sync(kFull, pred);
+    const int pos = count + __popc(b & lt);
+    count += __popc(b);
+    return pos;
+}
+
 template<int ORDER, bool EPS0>
-__global__ void __launch_bounds__(kThreads) bh_kernel(const float4 *__restrict__ nodes,
-                                                      const int *__restrict__ num_nodes_p,
+__device__ __forceinline__ void flush_approx(WarpLists &L, int &napprox, const float4 *__restrict__ pay, float4 p,
+                                             float eps, int lane, float &ax, float &ay, float &az, unsigned &cnp) {
+    constexpr int PAY = NodeLayout<ORDER>::PAY;
+    int j = 0;
+    for (; j + 1 < napprox; j += 2) {
+        const int c0 = L.approx_node[j], c1 = L.approx_node[j + 1];
+        const bool b0 = (L.approx_mask[j] >> lane) & 1u, b1 = (L.approx_mask[j + 1] >> lane) & 1u;
+        const float4 *p0 = pay + (int64_t) c0 * PAY, *p1 = pay + (int64_t) c1 * PAY;
+        const float4 m0 = __ldg(p0), m1 = __ldg(p1);
+        if constexpr (ORDER == 1) {
+            if (b0) pair_term<EPS0>(p, m0, eps, ax, ay, az);
+            if (b1) pair_term<EPS0>(p, m1, eps, ax, ay, az);
+        } else {
+            const float4 q00 = __ldg(p0 + 1), q01 = __ldg(p0 + 2), q10 = __ldg(p1 + 1), q11 = __ldg(p1 + 2);
+            if (b0) quad_term<EPS0>(p, m0, q00, q01, eps, ax, ay, az);
+            if (b1) quad_term<EPS0>(p, m1, q10, q11, eps, ax, ay, az);
+        }
+        cnp += (unsigned) b0 + (unsigned) b1;
+    }
+    if (j < napprox) {
+        const int c0 = L.approx_node[j];
+        const bool b0 = (L.approx_mask[j] >> lane) & 1u;
+        const float4 *p0 = pay + (int64_t) c0 * PAY;
+        const float4 m0 = __ldg(p0);
+        if constexpr (ORDER == 1) {
+            if (b0) pair_term<EPS0>(p, m0, eps, ax, ay, az);
+        } else {
+            const float4 q00 = __ldg(p0 + 1), q01 = __ldg(p0 + 2);
+            if (b0) quad_term<EPS0>(p, m0, q00, q01, eps, ax, ay, az);
+        }
+        cnp += (unsigned) b0;
+    }
+    napprox = 0;
+    __syncwarp();
+}
+
+template<bool EPS0>
+__device__ __forceinline__ void flush_pp(WarpLists &L, int &npp, const float4 *__restrict__ bodies, float4 p,
+                                         float eps, int lane, float &ax, float &ay, float &az, unsigned &cpp) {
+    for (int j = 0; j < npp; ++j) {
+        const int b = L.pp_begin[j], e = L.pp_end[j];
+        const bool on = (L.pp_mask[j] >> lane) & 1u;
+        int k = b;
+        for (; k + 3 < e; k += 4) {
+            const float4 s0 = __ldg(bodies + k), s1 = __ldg(bodies + k + 1);
+            const float4 s2 = __ldg(bodies + k + 2), s3 = __ldg(bodies + k + 3);
+            if (on) {
+                pair_term<EPS0>(p, s0, eps, ax, ay, az);
+                pair_term<EPS0>(p, s1, eps, ax, ay, az);
+                pair_term<EPS0>(p, s2, eps, ax, ay, az);
+                pair_term<EPS0>(p, s3, eps, ax, ay, az);
+            }
+        }
+        for (; k < e; ++k) {
+            const float4 s0 = __ldg(bodies + k);
+            if (on) pair_term<EPS0>(p, s0, eps, ax, ay, az);
+        }
+        if (on) cpp += (unsigned) (e - b);
+    }
+    npp = 0;
+    __syncwarp();
+}
+
+template<int ORDER, bool EPS0>
+__global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const int *__restrict__ num_nodes_p,
                                                       const float4 *__restrict__ bodies, int n_bodies,
-                                                      const float4 *__restrict__ targets, int64_t n_targets, float G,
+                                                      const float4 *__restrict__ targets, int n_targets, float G,
                                                       float eps, float4 *__restrict__ acc,
-                                                      unsigned long long *__restrict__ counts) {
-    constexpr int REC = NodeLayout<ORDER>::REC;
-    const int lane = threadIdx.x & 31;
-    const int64_t i = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x);
-    if ((i - lane) >= n_targets) return;  // whole warp out of range
+                                                      unsigned long long *__restrict__ counts,
+                                                      int2 *__restrict__ stack_base, unsigned *__restrict__ group_counter,
+                                                      uint32_t *__restrict__ err) {
+    __shared__ WarpLists lists[kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    WarpLists &L = lists[warp];
+    int2 *stack = stack_base + ((int64_t) blockIdx.x * kWarps + warp) * kTraverseStack;
+    const float4 *__restrict__ mac = nodes.mac;
+    const int2 *__restrict__ link = nodes.link;
+    const float4 *__restrict__ pay = nodes.pay;
     const int num_nodes = *num_nodes_p;
-    const bool valid = i < n_targets;
-    const float4 p = valid ? targets[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-    float ax = 0.f, ay = 0.f, az = 0.f;
-    unsigned npp = 0, nnp = 0;
-    int next = valid ? 0 : INT_MAX;
+    const int num_groups = (n_targets + 31) / 32;
+    const uint32_t lt = lanemask_lt();
+    // A valid tree needs fewer chunk rounds than it has nodes for one group; the cap only bounds
+    // the work on a corrupted tree.
+    const int64_t round_limit = 4 * (int64_t) num_nodes + 64;
+    unsigned cpp = 0, cnp = 0;
 
     while (true) {
-        const int c = __reduce_min_sync(0xffffffffu, next);
-        if (c >= num_nodes) break;
-        const float4 *r = nodes + (int64_t) c * REC;
-        const float4 mac = __ldg(r);
-        const float4 com = __ldg(r + 1);
-        float q[6];
-        int link0, link1;
-        if constexpr (ORDER == 1) {
-            const float4 l = __ldg(r + 2);
-            link0 = __float_as_int(l.x);
-            link1 = __float_as_int(l.y);
-        } else {
-            const float4 q0 = __ldg(r + 2), q1 = __ldg(r + 3);
-            q[0] = q0.x; q[1] = q0.y; q[2] = q0.z; q[3] = q0.w; q[4] = q1.x; q[5] = q1.y;
-            link0 = __float_as_int(q1.z);
-            link1 = __float_as_int(q1.w);
-        }
-        const bool leaf = link1 >= 0;
-        if (leaf) {  // defensive clamp: a leaf never reaches outside the body array
-            link0 = max(link0, 0);
-            link1 = min(link1, n_bodies);
-        }
-        bool open = false;
-        if (next == c) {
-            const float dx = fsub(p.x, mac.x), dy = fsub(p.y, mac.y), dz = fsub(p.z, mac.z);
-            const float d2 = fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz));
-            if (d2 >= mac.w) {
-                if constexpr (ORDER == 1) pair_term<EPS0>(p.x, p.y, p.z, com, eps, ax, ay, az);
-                else quad_term<EPS0>(p.x, p.y, p.z, com, q, eps, ax, ay, az);
-                ++nnp;
-                next = leaf ? c + 1 : max(link0, c + 1);  // the cursor only moves forward
-            } else {
-                next = c + 1;
-                open = leaf;
+        int g = 0;
+        if (lane == 0) g = (int) atomicAdd(group_counter, 1u);
+        g = __shfl_sync(kFull, g, 0);
+        if (g >= num_groups) break;
+        const int i = g * 32 + lane;
+        const bool valid = i < n_targets;
+        const float4 p = valid ? targets[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const uint32_t full = __ballot_sync(kFull, valid);
+        float lo[3] = {valid ? p.x : FLT_MAX, valid ? p.y : FLT_MAX, valid ? p.z : FLT_MAX};
+        float hi[3] = {valid ? p.x : -FLT_MAX, valid ? p.y : -FLT_MAX, valid ? p.z : -FLT_MAX};
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                lo[k] = fminf(lo[k], __shfl_xor_sync(kFull, lo[k], o));
+                hi[k] = fmaxf(hi[k], __shfl_xor_sync(kFull, hi[k], o));
             }
         }
-        if (leaf && __any_sync(0xffffffffu, open)) {
-            for (int j = link0; j < link1; ++j) {
-                const float4 b = __ldg(bodies + j);
-                if (open) pair_term<EPS0>(p.x, p.y, p.z, b, eps, ax, ay, az);
-            }
-            if (open) npp += (unsigned) (link1 - link0);
+        L.tpos[lane] = p;
+        int top = 0, napprox = 0, npp = 0, nmixed = 0;
+        if (num_nodes > 0) {
+            if (lane == 0) stack[0] = make_int2(0, (int) full);
+            top = 1;
         }
+        __syncwarp();
+        float ax = 0.f, ay = 0.f, az = 0.f;
+        int64_t rounds = 0;
+
+        while (top > 0 || nmixed > 0) {
+            if (++rounds > round_limit) {
+                if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
+                break;
+            }
+            if (top > 0) {
+                // ---- 1. pop up to 32 entries and classify them lane-parallel ----
+                const int k = min(32, top);
+                const int base = top - k;
+                top = base;
+                int c = 0, l0 = 0, l1 = -1, cls = kNone;
+                uint32_t m = 0;
+                if (lane < k) {
+                    const int2 e = stack[base + lane];
+                    c = e.x;
+                    m = (uint32_t) e.y;
+                    const float4 mc = __ldg(mac + c);
+                    const int2 lk = __ldg(link + c);
+                    l0 = lk.x;
+                    l1 = lk.y;
+                    // nearest box point and farthest box corner, per axis, with the reference's rounding
+                    const float nx = fsub(fminf(fmaxf(mc.x, lo[0]), hi[0]), mc.x);
+                    const float ny = fsub(fminf(fmaxf(mc.y, lo[1]), hi[1]), mc.y);
+                    const float nz = fsub(fminf(fmaxf(mc.z, lo[2]), hi[2]), mc.z);
+                    const float fx = fmaxf(fabsf(fsub(lo[0], mc.x)), fabsf(fsub(hi[0], mc.x)));
+                    const float fy = fmaxf(fabsf(fsub(lo[1], mc.y)), fabsf(fsub(hi[1], mc.y)));
+                    const float fz = fmaxf(fabsf(fsub(lo[2], mc.z)), fabsf(fsub(hi[2], mc.z)));
+                    const float dmin2 = fadd(fadd(fmul(nx, nx), fmul(ny, ny)), fmul(nz, nz));
+                    const float dmax2 = fadd(fadd(fmul(fx, fx), fmul(fy, fy)), fmul(fz, fz));
+                    if (!(mc.w == mc.w)) cls = kOpenAll;  // NaN threshold: never approximated
+                    else if (dmin2 >= mc.w) cls = kAcceptAll;
+                    else if (dmax2 < mc.w) cls = kOpenAll;
+                    else cls = kMixed;
+                }
+                __syncwarp();  // popped entries are read before children overwrite them
+                const bool is_acc = cls == kAcceptAll;
+                const bool is_leaf_open = cls == kOpenAll && l1 >= 0;
+                const bool is_int_open = cls == kOpenAll && l1 < 0 && l0 > c + 1 && l0 < num_nodes;
+                if (cls == kOpenAll && l1 < 0 && !is_int_open) atomicOr(err, (uint32_t) kErrTraverseLimit);
+                const bool is_mix = cls == kMixed;
+                int pos = warp_append(is_acc, napprox, lt);
+                if (is_acc) { L.approx_node[pos] = c; L.approx_mask[pos] = m; }
+                pos = warp_append(is_leaf_open, npp, lt);
+                if (is_leaf_open) {
+                    L.pp_begin[pos] = max(l0, 0);
+                    L.pp_end[pos] = min(l1, n_bodies);
+                    L.pp_mask[pos] = m;
+                }
+                pos = warp_append(is_mix, nmixed, lt);
+                if (is_mix) { L.mixed_node[pos] = c; L.mixed_mask[pos] = m; }
+                const uint32_t bi = __ballot_sync(kFull, is_int_open);
+                if (is_int_open) {
+                    const int sp = top + 2 * __popc(bi & lt);
+                    if (sp + 1 < kTraverseStack) {
+                        stack[sp] = make_int2(l0, (int) m);     // right child
+                        stack[sp + 1] = make_int2(c + 1, (int) m);  // left child, popped first
+                    } else {
+                        atomicOr(err, (uint32_t) kErrStackOverflow);
+                    }
+                }
+                top = min(top + 2 * __popc(bi), kTraverseStack);
+                __syncwarp();
+                // each round appends at most 32 entries per list: evaluate before the next one
+                if (napprox > kList - 32) flush_approx<ORDER, EPS0>(L, napprox, pay, p, eps, lane, ax, ay, az, cnp);
+                if (npp > kList - 32) flush_pp<EPS0>(L, npp, bodies, p, eps, lane, ax, ay, az, cpp);
+            }
+            if (nmixed >= 32 || (top == 0 && nmixed > 0)) {
+                // ---- 2. resolve up to 32 mixed nodes: per-target MAC, lane-parallel over nodes ----
+                const int k = min(32, nmixed);
+                const int base = nmixed - k;
+                nmixed = base;
+                int c = 0, l0 = 0, l1 = -1;
+                uint32_t A = 0, O = 0;
+                if (lane < k) {
+                    c = L.mixed_node[base + lane];
+                    const uint32_t m = L.mixed_mask[base + lane];
+                    const float4 mc = __ldg(mac + c);
+                    const int2 lk = __ldg(link + c);
+                    l0 = lk.x;
+                    l1 = lk.y;
+                    uint32_t bits = 0;
+#pragma unroll 8
+                    for (int t = 0; t < 32; ++t) {
+                        const float4 tp = L.tpos[t];
+                        bits |= (ref_dist2(tp.x, tp.y, tp.z, mc) >= mc.w) ? (1u << t) : 0u;
+                    }
+                    A = bits & m;
+                    O = m & ~A;
+                }
+                __syncwarp();
+                const bool is_acc = A != 0;
+                const bool is_leaf_open = O != 0 && l1 >= 0;
+                const bool is_int_open = O != 0 && l1 < 0 && l0 > c + 1 && l0 < num_nodes;
+                if (O != 0 && l1 < 0 && !is_int_open) atomicOr(err, (uint32_t) kErrTraverseLimit);
+                int pos = warp_append(is_acc, napprox, lt);
+                if (is_acc) { L.approx_node[pos] = c; L.approx_mask[pos] = A; }
+                pos = warp_append(is_leaf_open, npp, lt);
+                if (is_leaf_open) {
+                    L.pp_begin[pos] = max(l0, 0);
+                    L.pp_end[pos] = min(l1, n_bodies);
+                    L.pp_mask[pos] = O;
+                }
+                const uint32_t bi = __ballot_sync(kFull, is_int_open);
+                if (is_int_open) {
+                    const int sp = top + 2 * __popc(bi & lt);
+                    if (sp + 1 < kTraverseStack) {
+                        stack[sp] = make_int2(l0, (int) O);
+                        stack[sp + 1] = make_int2(c + 1, (int) O);
+                    } else {
+                        atomicOr(err, (uint32_t) kErrStackOverflow);
+                    }
+                }
+                top = min(top + 2 * __popc(bi), kTraverseStack);
+                __syncwarp();
+                if (napprox > kList - 32) flush_approx<ORDER, EPS0>(L, napprox, pay, p, eps, lane, ax, ay, az, cnp);
+                if (npp > kList - 32) flush_pp<EPS0>(L, npp, bodies, p, eps, lane, ax, ay, az, cpp);
+            }
+        }
+        flush_approx<ORDER, EPS0>(L, napprox, pay, p, eps, lane, ax, ay, az, cnp);
+        flush_pp<EPS0>(L, npp, bodies, p, eps, lane, ax, ay, az, cpp);
+        if (valid) acc[i] = make_float4(G * ax, G * ay, G * az, 0.f);
+        __syncwarp();
     }
-    if (valid) acc[i] = make_float4(G * ax, G * ay, G * az, 0.f);
     if (counts) {
-        const unsigned spp = __reduce_add_sync(0xffffffffu, npp);
-        const unsigned snp = __reduce_add_sync(0xffffffffu, nnp);
+        const unsigned spp = __reduce_add_sync(kFull, cpp);
+        const unsigned snp = __reduce_add_sync(kFull, cnp);
         if (lane == 0) {
             atomicAdd(counts + 0, (unsigned long long) spp);
             atomicAdd(counts + 1, (unsigned long long) snp);
@@ -141,28 +363,65 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(const float4 *__restrict__
     }
 }
 
-template<int ORDER>
-void launch_order(const float4 *nodes, const int *num_nodes, const float4 *bodies, int n_bodies,
-                  const float4 *targets, int64_t nt, float G, float eps, float4 *acc, unsigned long long *counts,
-                  cudaStream_t s) {
-    const int64_t blocks = (nt + kThreads - 1) / kThreads;
-    if (eps == 0.f)
-        bh_kernel<ORDER, true><<<(unsigned) blocks, kThreads, 0, s>>>(nodes, num_nodes, bodies, n_bodies, targets, nt,
-                                                                       G, eps, acc, counts);
-    else
-        bh_kernel<ORDER, false><<<(unsigned) blocks, kThreads, 0, s>>>(nodes, num_nodes, bodies, n_bodies, targets, nt,
-                                                                        G, eps, acc, counts);
+// Occupancy and SM count are fixed per device and kernel: queried once (B200 parts are identical).
+template<int ORDER, bool EPS0>
+int blocks_per_sm() {
+    static int cached = 0;
+    if (cached == 0) {
+        int b = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, bh_kernel<ORDER, EPS0>, kThreads, 0);
+        cached = b > 0 ? b : 1;
+    }
+    return cached;
+}
+
+int sm_count(int device) {
+    static int cached[64] = {0};
+    if (device < 0 || device >= 64) device = 0;
+    if (cached[device] == 0) {
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        cached[device] = sms > 0 ? sms : 1;
+    }
+    return cached[device];
+}
+
+template<int ORDER, bool EPS0>
+void launch_variant(const NodeArrays &nodes, const int *num_nodes, const float4 *bodies, int n_bodies,
+                    const float4 *targets, int nt, float G, float eps, float4 *acc, unsigned long long *counts,
+                    TraverseWorkspace &ws, uint32_t *err, cudaStream_t s) {
+    int device = 0;
+    cudaGetDevice(&device);
+    int64_t blocks = (int64_t) sm_count(device) * blocks_per_sm<ORDER, EPS0>();
+    blocks = std::min<int64_t>(blocks, ws.warps / kWarps);
+    const int64_t groups = (nt + 31) / 32;
+    blocks = std::min<int64_t>(blocks, (groups + kWarps - 1) / kWarps);
+    if (blocks < 1) blocks = 1;
+    cudaMemsetAsync(ws.group_counter, 0, sizeof(unsigned), s);
+    bh_kernel<ORDER, EPS0><<<(unsigned) blocks, kThreads, 0, s>>>(nodes, num_nodes, bodies, n_bodies, targets, nt, G,
+                                                                   eps, acc, counts, ws.stack, ws.group_counter, err);
 }
 
 }  // namespace
 
-void launch_bh_traverse(int order, const float4 *nodes, const int *num_nodes, const float4 *bodies, int64_t n_bodies,
+int64_t traverse_resident_warps(int device) {
+    int b = std::max(std::max(blocks_per_sm<1, false>(), blocks_per_sm<1, true>()),
+                     std::max(blocks_per_sm<2, false>(), blocks_per_sm<2, true>()));
+    return (int64_t) sm_count(device) * b * kWarps;
+}
+
+void launch_bh_traverse(int order, const NodeArrays &nodes, const int *num_nodes, const float4 *bodies, int64_t n_bodies,
                         const float4 *targets, int64_t n_targets, float G, float eps, float4 *acc,
-                        unsigned long long *counts, cudaStream_t s) {
+                        unsigned long long *counts, TraverseWorkspace &ws, uint32_t *err, cudaStream_t s) {
     if (n_targets <= 0) return;
-    const int nb = (int) n_bodies;
-    if (order == 1) launch_order<1>(nodes, num_nodes, bodies, nb, targets, n_targets, G, eps, acc, counts, s);
-    else launch_order<2>(nodes, num_nodes, bodies, nb, targets, n_targets, G, eps, acc, counts, s);
+    const int nb = (int) n_bodies, nt = (int) n_targets;
+    if (order == 1) {
+        if (eps == 0.f) launch_variant<1, true>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s);
+        else launch_variant<1, false>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s);
+    } else {
+        if (eps == 0.f) launch_variant<2, true>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s);
+        else launch_variant<2, false>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s);
+    }
 }
 
 }  // namespace nbg

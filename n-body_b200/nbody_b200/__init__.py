@@ -348,21 +348,17 @@ class NaiveSolver(Solver):
 
 
 def decode_records(records: np.ndarray, order: int) -> dict:
-    """Split packed node records (see nb_internal.cuh NodeLayout) into named fields."""
-    r = np.asarray(records, np.float32)
-    link = r[:, -2:] if order == 1 else r[:, 14:16]
-    if order == 1:
-        link = r[:, 8:10]
+    """Split exported node records into named fields. Per node: MAC centre and threshold (4 floats),
+    link (2 int32: internal = right child's preorder index and -1, leaf = body range), 2 pad floats,
+    then the payload: centre of mass and mass, and for order 2 the packed quadrupole."""
+    r = np.ascontiguousarray(records, np.float32)
     out = {
         "center": r[:, 0:3],
         "mac_threshold": r[:, 3],
-        "com": r[:, 4:7],
-        "mass": r[:, 7],
-        "link": np.ascontiguousarray(link).view(np.int32),
+        "link": np.ascontiguousarray(r[:, 4:6]).view(np.int32),
+        "com": r[:, 8:11],
+        "mass": r[:, 11],
     }
     if order == 2:
-        out["quadrupole"] = np.concatenate([r[:, 8:12], r[:, 12:14]], axis=1)
+        out["quadrupole"] = np.ascontiguousarray(r[:, 12:18])
     return out
-
-
-from . import scenarios  # noqa: E402  (host-side scenario generators)

@@ -34,15 +34,6 @@ def oracle_tree(oracle, pm, leaf, order):
     return box, codes, perm, sc, tree, bb, cm, mo
 
 
-def subtree_sizes(tree):
-    b, e, l, r = tree
-    size = np.ones(len(b), np.int64)
-    for k in range(len(b) - 1, -1, -1):
-        if l[k] >= 0:
-            size[k] = 1 + size[l[k]] + size[r[k]]
-    return size
-
-
 def check_tree(nb, oracle, s, pm, leaf, order, theta):
     t = s.tree()
     box, codes, perm, sc, tree, bb, cm, mo = oracle_tree(oracle, pm, leaf, order)
@@ -57,8 +48,9 @@ def check_tree(nb, oracle, s, pm, leaf, order, theta):
     assert np.array_equal(link[:, 1] >= 0, leaf_mask)
     assert np.array_equal(link[leaf_mask, 0], b[leaf_mask])
     assert np.array_equal(link[leaf_mask, 1], e[leaf_mask])
-    skip = np.arange(len(b)) + subtree_sizes(tree)
-    assert np.array_equal(link[~leaf_mask, 0], skip[~leaf_mask])
+    # internal nodes link their right child (the left child is the next node in preorder)
+    assert np.array_equal(link[~leaf_mask, 0], r[~leaf_mask])
+    assert np.all(l[~leaf_mask] == np.arange(len(b))[~leaf_mask] + 1)
     # summaries, bit-exact
     assert np.array_equal(rec["com"], cm[:, :3])
     assert np.array_equal(rec["mass"], cm[:, 3])
