@@ -362,3 +362,6 @@ def decode_records(records: np.ndarray, order: int) -> dict:
     if order == 2:
         out["quadrupole"] = np.ascontiguousarray(r[:, 12:18])
     return out
+
+
+from . import scenarios  # noqa: E402  (host-side scenario generators)
