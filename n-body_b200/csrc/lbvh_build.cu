@@ -262,7 +262,8 @@ __device__ void write_record(const NodeArrays &nodes, int pre, const Summ<ORDER>
     p[0] = make_float4(s.com[0], s.com[1], s.com[2], s.M);
     if constexpr (ORDER >= 2) {
         p[1] = make_float4(s.q[0], s.q[1], s.q[2], s.q[3]);
-        p[2] = make_float4(s.q[4], s.q[5], 0.f, 0.f);
+        // third slot: 1.5 * trace(Q), the traversal's quadrupole term uses it per interaction
+        p[2] = make_float4(s.q[4], s.q[5], fmul(1.5f, fadd(fadd(s.q[0], s.q[3]), s.q[5])), 0.f);
     }
 }
 

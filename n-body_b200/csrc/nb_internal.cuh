@@ -56,7 +56,7 @@ struct BBoxAccum {
 // link[c] = internal node: (preorder index of the right child, -1); the left child is c + 1
 //           leaf:          (first body, end body) of its range in Morton order
 // pay[c * PAY + k]: k = 0: (centre_of_mass.xyz, mass); order 2 adds k = 1: (Qxx, Qxy, Qxz, Qyy),
-//           k = 2: (Qyz, Qzz, 0, 0) - moments about the centre of mass, not traceless.
+//           k = 2: (Qyz, Qzz, 1.5 * trace(Q), 0) - moments about the centre of mass, not traceless.
 template<int ORDER>
 struct NodeLayout;
 template<>

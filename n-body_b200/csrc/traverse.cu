@@ -21,10 +21,10 @@
 //      is exact for every target, not a heuristic.
 //   2. Mixed nodes are batched and resolved lane-parallel: each lane takes one node and tests the
 //      32 targets (broadcast from shared memory), producing accept and open masks.
-//   3. Accepted (node, mask) entries and opened (leaf, mask) entries go to short shared-memory
-//      lists that are evaluated densely: every lane reads the same node or body (broadcast load)
-//      and computes the term for its own target where its mask bit is set. Opened internal nodes
-//      push both children.
+//   3. Nodes accepted by every target go to a shared list evaluated by all lanes with broadcast
+//      loads; nodes accepted by some targets only go to per-target private lists in shared memory,
+//      evaluated target-major (each lane walks its own list). Opened leaves go to a (leaf, mask)
+//      list evaluated with broadcast body loads. Opened internal nodes push both children.
 // The expensive terms thus run without traversal bookkeeping between them, and the per-node
 // traversal cost is spread over 32 nodes per instruction.
 //
@@ -45,18 +45,19 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kList = 64;          // capacity of each per-warp list; rounds append at most 32
+constexpr int kPriv = 32;          // per-target private list of partially accepted nodes
 constexpr unsigned kFull = 0xffffffffu;
 
 enum : int { kNone = 0, kAcceptAll = 1, kOpenAll = 2, kMixed = 3 };
 
 struct WarpLists {
     float4 tpos[32];
-    int approx_node[kList];
-    uint32_t approx_mask[kList];
+    int approx_node[kList];       // nodes accepted by every target of the group
     int pp_begin[kList], pp_end[kList];
     uint32_t pp_mask[kList];
     int mixed_node[kList];
     uint32_t mixed_mask[kList];
+    int priv[kPriv][32];          // [slot][lane]: nodes accepted by some targets only
 };
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -98,8 +99,8 @@ __device__ __forceinline__ void quad_term(float4 p, float4 com, float4 q0, float
     const float qy = fmaf(q0.y, rx, fmaf(q0.w, ry, q1.x * rz));
     const float qz = fmaf(q0.z, rx, fmaf(q1.x, ry, q1.y * rz));
     const float rqr = fmaf(rx, qx, fmaf(ry, qy, rz * qz));
-    const float tr = q0.x + q0.w + q1.y;
-    const float sr = fmaf(-7.5f * inv7, rqr, fmaf(1.5f * inv5, tr, -com.w * inv3));
+    // q1.z holds 1.5 * (Qxx + Qyy + Qzz), precomputed per node
+    const float sr = fmaf(-7.5f * inv7, rqr, fmaf(inv5, q1.z, -com.w * inv3));
     const float sq = 3.0f * inv5;
     ax = fmaf(rx, sr, fmaf(qx, sq, ax));
     ay = fmaf(ry, sr, fmaf(qy, sq, ay));
@@ -115,39 +116,61 @@ __device__ __forceinline__ int warp_append(bool pred, int &count, uint32_t lt) {
 }
 
 template<int ORDER, bool EPS0>
-__device__ __forceinline__ void flush_approx(WarpLists &L, int &napprox, const float4 *__restrict__ pay, float4 p,
-                                             float eps, int lane, float &ax, float &ay, float &az, unsigned &cnp) {
+__device__ __forceinline__ void node_term(const float4 *__restrict__ pay, int c, float4 p, float eps, float &ax,
+                                          float &ay, float &az) {
     constexpr int PAY = NodeLayout<ORDER>::PAY;
+    const float4 *pc = pay + (int64_t) c * PAY;
+    if constexpr (ORDER == 1) {
+        pair_term<EPS0>(p, __ldg(pc), eps, ax, ay, az);
+    } else {
+        quad_term<EPS0>(p, __ldg(pc), __ldg(pc + 1), __ldg(pc + 2), eps, ax, ay, az);
+    }
+}
+
+// Nodes accepted by the whole group: every lane evaluates every entry (broadcast loads).
+template<int ORDER, bool EPS0>
+__device__ __forceinline__ void flush_approx(WarpLists &L, int &napprox, const float4 *__restrict__ pay, float4 p,
+                                             float eps, float &ax, float &ay, float &az, unsigned &cnp) {
     int j = 0;
     for (; j + 1 < napprox; j += 2) {
         const int c0 = L.approx_node[j], c1 = L.approx_node[j + 1];
-        const bool b0 = (L.approx_mask[j] >> lane) & 1u, b1 = (L.approx_mask[j + 1] >> lane) & 1u;
-        const float4 *p0 = pay + (int64_t) c0 * PAY, *p1 = pay + (int64_t) c1 * PAY;
-        const float4 m0 = __ldg(p0), m1 = __ldg(p1);
-        if constexpr (ORDER == 1) {
-            if (b0) pair_term<EPS0>(p, m0, eps, ax, ay, az);
-            if (b1) pair_term<EPS0>(p, m1, eps, ax, ay, az);
-        } else {
-            const float4 q00 = __ldg(p0 + 1), q01 = __ldg(p0 + 2), q10 = __ldg(p1 + 1), q11 = __ldg(p1 + 2);
-            if (b0) quad_term<EPS0>(p, m0, q00, q01, eps, ax, ay, az);
-            if (b1) quad_term<EPS0>(p, m1, q10, q11, eps, ax, ay, az);
-        }
-        cnp += (unsigned) b0 + (unsigned) b1;
+        node_term<ORDER, EPS0>(pay, c0, p, eps, ax, ay, az);
+        node_term<ORDER, EPS0>(pay, c1, p, eps, ax, ay, az);
     }
-    if (j < napprox) {
-        const int c0 = L.approx_node[j];
-        const bool b0 = (L.approx_mask[j] >> lane) & 1u;
-        const float4 *p0 = pay + (int64_t) c0 * PAY;
-        const float4 m0 = __ldg(p0);
-        if constexpr (ORDER == 1) {
-            if (b0) pair_term<EPS0>(p, m0, eps, ax, ay, az);
-        } else {
-            const float4 q00 = __ldg(p0 + 1), q01 = __ldg(p0 + 2);
-            if (b0) quad_term<EPS0>(p, m0, q00, q01, eps, ax, ay, az);
-        }
-        cnp += (unsigned) b0;
-    }
+    if (j < napprox) node_term<ORDER, EPS0>(pay, L.approx_node[j], p, eps, ax, ay, az);
+    cnp += (unsigned) napprox;
     napprox = 0;
+    __syncwarp();
+}
+
+// Nodes accepted by some targets only: each lane walks its own list (target-major).
+template<int ORDER, bool EPS0>
+__device__ __forceinline__ void flush_private(WarpLists &L, int &npriv, const float4 *__restrict__ pay, float4 p,
+                                              float eps, int lane, float &ax, float &ay, float &az, unsigned &cnp) {
+    const int most = __reduce_max_sync(kFull, npriv);
+    for (int k = 0; k < most; ++k) {
+        if (k < npriv) node_term<ORDER, EPS0>(pay, L.priv[k][lane], p, eps, ax, ay, az);
+    }
+    cnp += (unsigned) npriv;
+    npriv = 0;
+    __syncwarp();
+}
+
+// Partially accepted entries (node c_i with target mask A_i in lane i) go to the private lists
+// of the targets in A_i; a full list is evaluated before it would overflow.
+template<int ORDER, bool EPS0>
+__device__ __forceinline__ void append_private(WarpLists &L, int &npriv, bool partial, int c, uint32_t A,
+                                               const float4 *__restrict__ pay, float4 p, float eps, int lane,
+                                               float &ax, float &ay, float &az, unsigned &cnp) {
+    uint32_t pend = __ballot_sync(kFull, partial);
+    while (pend) {
+        const int src = __ffs(pend) - 1;
+        pend &= pend - 1;
+        const int node = __shfl_sync(kFull, c, src);
+        const uint32_t mask = __shfl_sync(kFull, A, src);
+        if (__any_sync(kFull, npriv == kPriv)) flush_private<ORDER, EPS0>(L, npriv, pay, p, eps, lane, ax, ay, az, cnp);
+        if ((mask >> lane) & 1u) L.priv[npriv++][lane] = node;
+    }
     __syncwarp();
 }
 
@@ -221,13 +244,14 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
             }
         }
         L.tpos[lane] = p;
-        int top = 0, napprox = 0, npp = 0, nmixed = 0;
+        int top = 0, napprox = 0, npp = 0, nmixed = 0, npriv = 0;
         if (num_nodes > 0) {
             if (lane == 0) stack[0] = make_int2(0, (int) full);
             top = 1;
         }
         __syncwarp();
         float ax = 0.f, ay = 0.f, az = 0.f;
+        unsigned gnp = 0, gpp = 0;  // this group's interaction counts (kept for valid targets only)
         int64_t rounds = 0;
 
         while (top > 0 || nmixed > 0) {
@@ -265,13 +289,15 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
                     else cls = kMixed;
                 }
                 __syncwarp();  // popped entries are read before children overwrite them
-                const bool is_acc = cls == kAcceptAll;
+                const bool is_acc = cls == kAcceptAll && m == full;
+                const bool is_acc_part = cls == kAcceptAll && m != full;
                 const bool is_leaf_open = cls == kOpenAll && l1 >= 0;
                 const bool is_int_open = cls == kOpenAll && l1 < 0 && l0 > c + 1 && l0 < num_nodes;
                 if (cls == kOpenAll && l1 < 0 && !is_int_open) atomicOr(err, (uint32_t) kErrTraverseLimit);
                 const bool is_mix = cls == kMixed;
                 int pos = warp_append(is_acc, napprox, lt);
-                if (is_acc) { L.approx_node[pos] = c; L.approx_mask[pos] = m; }
+                if (is_acc) L.approx_node[pos] = c;
+                append_private<ORDER, EPS0>(L, npriv, is_acc_part, c, m, pay, p, eps, lane, ax, ay, az, gnp);
                 pos = warp_append(is_leaf_open, npp, lt);
                 if (is_leaf_open) {
                     L.pp_begin[pos] = max(l0, 0);
@@ -293,8 +319,8 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
                 top = min(top + 2 * __popc(bi), kTraverseStack);
                 __syncwarp();
                 // each round appends at most 32 entries per list: evaluate before the next one
-                if (napprox > kList - 32) flush_approx<ORDER, EPS0>(L, napprox, pay, p, eps, lane, ax, ay, az, cnp);
-                if (npp > kList - 32) flush_pp<EPS0>(L, npp, bodies, p, eps, lane, ax, ay, az, cpp);
+                if (napprox > kList - 32) flush_approx<ORDER, EPS0>(L, napprox, pay, p, eps, ax, ay, az, gnp);
+                if (npp > kList - 32) flush_pp<EPS0>(L, npp, bodies, p, eps, lane, ax, ay, az, gpp);
             }
             if (nmixed >= 32 || (top == 0 && nmixed > 0)) {
                 // ---- 2. resolve up to 32 mixed nodes: per-target MAC, lane-parallel over nodes ----
@@ -320,12 +346,14 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
                     O = m & ~A;
                 }
                 __syncwarp();
-                const bool is_acc = A != 0;
+                const bool is_acc = A != 0 && A == full;
+                const bool is_acc_part = A != 0 && A != full;
                 const bool is_leaf_open = O != 0 && l1 >= 0;
                 const bool is_int_open = O != 0 && l1 < 0 && l0 > c + 1 && l0 < num_nodes;
                 if (O != 0 && l1 < 0 && !is_int_open) atomicOr(err, (uint32_t) kErrTraverseLimit);
                 int pos = warp_append(is_acc, napprox, lt);
-                if (is_acc) { L.approx_node[pos] = c; L.approx_mask[pos] = A; }
+                if (is_acc) L.approx_node[pos] = c;
+                append_private<ORDER, EPS0>(L, npriv, is_acc_part, c, A, pay, p, eps, lane, ax, ay, az, gnp);
                 pos = warp_append(is_leaf_open, npp, lt);
                 if (is_leaf_open) {
                     L.pp_begin[pos] = max(l0, 0);
@@ -344,13 +372,18 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
                 }
                 top = min(top + 2 * __popc(bi), kTraverseStack);
                 __syncwarp();
-                if (napprox > kList - 32) flush_approx<ORDER, EPS0>(L, napprox, pay, p, eps, lane, ax, ay, az, cnp);
-                if (npp > kList - 32) flush_pp<EPS0>(L, npp, bodies, p, eps, lane, ax, ay, az, cpp);
+                if (napprox > kList - 32) flush_approx<ORDER, EPS0>(L, napprox, pay, p, eps, ax, ay, az, gnp);
+                if (npp > kList - 32) flush_pp<EPS0>(L, npp, bodies, p, eps, lane, ax, ay, az, gpp);
             }
         }
-        flush_approx<ORDER, EPS0>(L, napprox, pay, p, eps, lane, ax, ay, az, cnp);
-        flush_pp<EPS0>(L, npp, bodies, p, eps, lane, ax, ay, az, cpp);
+        flush_approx<ORDER, EPS0>(L, napprox, pay, p, eps, ax, ay, az, gnp);
+        flush_private<ORDER, EPS0>(L, npriv, pay, p, eps, lane, ax, ay, az, gnp);
+        flush_pp<EPS0>(L, npp, bodies, p, eps, lane, ax, ay, az, gpp);
         if (valid) acc[i] = make_float4(G * ax, G * ay, G * az, 0.f);
+        if (valid) {
+            cnp += gnp;
+            cpp += gpp;
+        }
         __syncwarp();
     }
     if (counts) {
