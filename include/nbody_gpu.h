@@ -151,6 +151,19 @@ int nb_get_tree(nb_ctx *ctx, int64_t *num_nodes, int32_t *record_floats, uint64_
 int nb_direct_device(nb_ctx *ctx, int64_t n, const void *d_bodies, int64_t nt, const void *d_targets,
                      void *d_acc, int32_t precision);
 
+/* Morton-code sort that allocates no device memory (no counterpart in the reference: it serves
+ * callers that cannot call cudaMalloc, such as applications whose own pool owns all device memory
+ * or step loops that must not take cudaMalloc's implicit device synchronisation).
+ * Sorts n 64-bit codes (device pointer d_codes) into d_sorted_codes, with d_sorted_ids[k] = the
+ * input index of the k-th smallest code; equal codes keep their input order. All three are
+ * caller-owned device buffers. Scratch comes from one static device array of about 16 MiB that
+ * every GPU loading this library holds until exit: n must be at most 2^20 (larger n is rejected
+ * with NB_ERR_INVALID_ARGUMENT). The first call on a device looks up that array with the device
+ * current; make it before any stream capture. Calls share the array: calls that overlap on the
+ * GPU race. Runs on cuda_stream (NULL: the legacy default stream) and waits for it. */
+int nb_sort_codes_noalloc(const uint64_t *d_codes, uint64_t *d_sorted_codes, uint32_t *d_sorted_ids, int64_t n,
+                          void *cuda_stream);
+
 /* Page-locked host buffers for fast copies in and out (cudaMallocHost / cudaFreeHost). */
 void *nb_host_alloc(size_t bytes);
 void nb_host_free(void *p);

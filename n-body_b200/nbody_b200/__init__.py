@@ -114,6 +114,7 @@ SIGNATURES = {
     "nb_get_phase_times": (C.c_int, [_vp, C.POINTER(PhaseTimes)]),
     "nb_get_tree": (C.c_int, [_vp, C.POINTER(_i64), C.POINTER(_i32), _vp, _vp, _vp, _vp]),
     "nb_direct_device": (C.c_int, [_vp, _i64, _vp, _i64, _vp, _vp, _i32]),
+    "nb_sort_codes_noalloc": (C.c_int, [_vp, _vp, _vp, _i64, _vp]),
     "nb_host_alloc": (_vp, [C.c_size_t]),
     "nb_host_free": (None, [_vp]),
 }
