@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--n", type=int, default=N_BODIES)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["plummer-1m", "batched"], default="plummer-1m",
+                    help="plummer-1m: one N=2^20 instance (the headline); batched: 256 uneven instances")
+    ap.add_argument("--instances", type=int, default=256)
     return ap.parse_args()
 
 
@@ -383,10 +386,108 @@ def read_traffic():
     return None
 
 
+BATCH_SOFTENING = 0.01
+BATCH_DT = 5e-4
+
+
+def batched_instances(count, seed=44):
+    """256 Plummer spheres with N log-uniform in [1024, 200000] and theta uniform in [0.4, 0.7]."""
+    from nbody_b200 import scenarios
+
+    rng = np.random.default_rng(seed)
+    sizes = np.round(np.exp(rng.uniform(np.log(1024), np.log(200000), count))).astype(np.int64)
+    thetas = rng.uniform(0.4, 0.7, count).astype(np.float32)
+    bodies, vels = [], []
+    for k, n in enumerate(sizes):
+        pm, vel = scenarios.plummer(int(n), seed=seed * 1000 + k)
+        bodies.append(pm)
+        vels.append(vel)
+    return sizes, thetas, bodies, vels
+
+
+def run_batched(args):
+    """Batched workload: every instance advanced by one launch per phase (graph-captured steps),
+    against the same instances stepped one after another through the plain single-instance path."""
+    import torch
+
+    world, rank, local = dist_env()
+    device = local
+    torch.cuda.set_device(device)
+    import nbody_b200 as nb
+
+    sizes, thetas, bodies, vels = batched_instances(args.instances, seed=44 + rank)
+    eps = float(np.float32(BATCH_SOFTENING) * np.float32(BATCH_SOFTENING))
+    total = int(sizes.sum())
+    stream = torch.cuda.Stream(device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    with torch.cuda.stream(stream):
+        s = nb.QuadrupoleLinearBVHSolver(rule=nb.Gravity(1.0, eps), max_leaf_size=LEAF, time_step=BATCH_DT,
+                                         device=device)
+        s.set_stream(stream.cuda_stream)
+        s.set_instances(sizes, np.concatenate(bodies), np.concatenate(vels), thetas)
+        s.enable_graphs(True)
+        s.step(max(args.warmup, 3))
+        torch.cuda.synchronize(device)
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        flush.zero_()
+        t0.record(stream)
+        s.step(args.steps)
+        t1.record(stream)
+        torch.cuda.synchronize(device)
+        batch_ms = t0.elapsed_time(t1)
+        s.enable_timing(True)
+        s.step(2)
+        phases = s.phase_times()
+        s.close()
+        # the same instances, one after another, through the plain path (one context each)
+        ctxs = []
+        for k in range(len(sizes)):
+            c = nb.QuadrupoleLinearBVHSolver(bodies=bodies[k], velocities=vels[k], rule=nb.Gravity(1.0, eps),
+                                             theta=float(thetas[k]), max_leaf_size=LEAF, time_step=BATCH_DT,
+                                             device=device)
+            c.set_stream(stream.cuda_stream)
+            c.step(1)
+            ctxs.append(c)
+        seq_steps = max(1, min(args.steps, 5))
+        torch.cuda.synchronize(device)
+        flush.zero_()
+        t0.record(stream)
+        for _ in range(seq_steps):
+            for c in ctxs:
+                c.step(1)
+        t1.record(stream)
+        torch.cuda.synchronize(device)
+        seq_ms = t0.elapsed_time(t1)
+        for c in ctxs:
+            c.close()
+    value = total * args.steps / (batch_ms / 1000.0)
+    seq_value = total * seq_steps / (seq_ms / 1000.0)
+    line = {
+        "metric": "body-steps/s, 256 batched Plummer instances (N log-uniform 1024..200000, theta 0.4..0.7)",
+        "value": value, "unit": "body-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": batch_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded Plummer spheres)",
+        "config": {"workload": f"batched-{len(sizes)}-plummer-quadrupole", "instances": int(len(sizes)),
+                   "total_bodies": total, "n_min": int(sizes.min()), "n_max": int(sizes.max()),
+                   "softening": BATCH_SOFTENING, "leaf_size": LEAF, "order": ORDER, "dt": BATCH_DT,
+                   "graphs": "two steps per CUDA graph", "l2": "flushed (256 MB write) before the timed steps"},
+        "sequential_plain_path": {"value": seq_value, "unit": "body-steps/s", "steps": seq_steps,
+                                  "ratio_batched_over_sequential": value / seq_value},
+        "phases_ms_per_step": {k: phases[k] / max(phases["passes"], 1) for k in
+                               ("bbox_ms", "morton_ms", "sort_ms", "gather_ms", "build_ms", "traverse_ms",
+                                "integrate_ms")},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "batched":
+        run_batched(args)
     else:
         run_ours(args)
 

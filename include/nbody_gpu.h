@@ -145,6 +145,24 @@ int nb_get_phase_times(nb_ctx *ctx, nb_phase_times *out);
 int nb_get_tree(nb_ctx *ctx, int64_t *num_nodes, int32_t *record_floats, uint64_t *sorted_codes,
                 uint32_t *sorted_ids, float *records, float *bbox);
 
+/* Batched independent instances (one launch per phase over all of them). Replaces the body set
+ * with `count` instances laid out back to back: instance k holds sizes[k] bodies (at least one)
+ * starting after instance k-1 in pos_mass / velocity (4 floats per body; velocity may be NULL).
+ * thetas[k] is instance k's opening angle (NULL: the config's theta); G, epsilon, leaf size, order
+ * and dt are shared. Each instance is an independent simulation: its own bounding box, Morton
+ * codes and tree (ActiveTreeSolver.h:33-72 per instance), and its results are bit-identical to
+ * running it alone. nb_update_accelerations / nb_step / nb_get_bodies then act on the whole batch,
+ * in the concatenated caller order. At most 65535 instances. */
+int nb_set_instances(nb_ctx *ctx, int32_t count, const int64_t *sizes, const float *thetas, const float *pos_mass,
+                     const float *velocity);
+int32_t nb_instance_count(const nb_ctx *ctx);
+/* Preorder index of each instance's root in the last tree built (count entries; synchronises). */
+int nb_get_instance_roots(nb_ctx *ctx, int32_t *roots);
+
+/* Capture pairs of steps in a CUDA graph and replay it in nb_step (off by default; per-phase
+ * timing, when enabled, runs the steps uncaptured). */
+int nb_enable_graphs(nb_ctx *ctx, int enable);
+
 /* Direct sum on device pointers: accelerations of nt targets (4 floats each) from n bodies.
  * precision 32: FP32, acc 4 floats per target (NaiveSolver arithmetic).
  * precision 64: FP64 accumulation, acc 3 doubles per target (accuracy reference). */

@@ -1,0 +1,143 @@
+// Kernels of the batched pipeline: many independent instances (each its own Morton box, tree and
+// theta) laid out back to back in one body array and advanced by one launch per phase.
+//
+// Per force pass:
+//   seg_bbox_kernel      one block per instance: exact FP32 min/max of its positions
+//                        (outerBoundingBox, SummaryType.h:73-81, per instance)
+//   seg_morton_kernel    Morton code of every body in its instance's box (MortonSort.h:46-73) and
+//                        the eight digit histograms of all codes
+//   8 one-sweep passes   over all codes (radix_sort.cu), then 1-2 stable passes on the instance id
+//                        (inst_key_kernel builds the keys, compose_kernel maps the result back), so
+//                        bodies end grouped by instance, sorted by code within it, ties by position
+//   the Karras build     over the keys (instance, code, index): each instance's subtree is exactly
+//                        its standalone tree (lbvh_build.cu)
+//   the traversal        driven by a table of 32-target groups that never straddle instances
+// Since every instance sees exactly the operations of a standalone run, in the same order,
+// its codes, tree and accelerations are bit-identical to running it alone.
+#include <cfloat>
+
+#include "nb_internal.cuh"
+
+namespace nbg {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__global__ void __launch_bounds__(kThreads) seg_bbox_kernel(const float4 *__restrict__ pos,
+                                                            const int2 *__restrict__ inst_range,
+                                                            float *__restrict__ inst_box) {
+    const int k = blockIdx.x;
+    const int2 r = inst_range[k];
+    float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
+    float mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int i = r.x + threadIdx.x; i <= r.y; i += blockDim.x) {
+        const float4 p = __ldg(pos + i);
+        mn[0] = gmin(mn[0], p.x); mn[1] = gmin(mn[1], p.y); mn[2] = gmin(mn[2], p.z);
+        mx[0] = gmax(mx[0], p.x); mx[1] = gmax(mx[1], p.y); mx[2] = gmax(mx[2], p.z);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            mn[c] = gmin(mn[c], __shfl_xor_sync(0xffffffffu, mn[c], o));
+            mx[c] = gmax(mx[c], __shfl_xor_sync(0xffffffffu, mx[c], o));
+        }
+    }
+    __shared__ float smn[3][kThreads / 32], smx[3][kThreads / 32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) { smn[c][warp] = mn[c]; smx[c][warp] = mx[c]; }
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        const int c = threadIdx.x;
+        float a = smn[c][0], b = smx[c][0];
+        for (int w = 1; w < kThreads / 32; ++w) { a = gmin(a, smn[c][w]); b = gmax(b, smx[c][w]); }
+        inst_box[6 * k + c] = a;
+        inst_box[6 * k + 3 + c] = b;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) seg_morton_kernel(const float4 *__restrict__ pos, int64_t n,
+                                                              const int *__restrict__ inst_of,
+                                                              const float *__restrict__ inst_box,
+                                                              uint64_t *__restrict__ codes,
+                                                              uint32_t *__restrict__ hist) {
+    __shared__ uint32_t sh[8 * 256];
+    for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const int64_t stride = (int64_t) gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const float *b = inst_box + 6 * inst_of[i];
+        const float mn[3] = {b[0], b[1], b[2]};
+        const float dx = fsub(b[3], b[0]), dy = fsub(b[4], b[1]), dz = fsub(b[5], b[2]);
+        const float scale = gmax(gmax(dx, dy), dz);
+        const uint64_t code = morton_code(__ldg(pos + i), mn, scale);
+        codes[i] = code;
+#pragma unroll
+        for (int d = 0; d < 8; ++d) atomicAdd(&sh[d * 256 + (uint32_t) ((code >> (8 * d)) & 255u)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 8 * 256; i += blockDim.x) {
+        const uint32_t c = sh[i];
+        if (c) atomicAdd(&hist[i], c);
+    }
+}
+
+// Instance id of the body at each code-sorted position (positions never leave their instance's
+// segment, so inst_of indexed by the sort's slot value is that body's instance).
+__global__ void __launch_bounds__(kThreads) inst_key_kernel(const uint32_t *__restrict__ slot, int64_t n,
+                                                            const int *__restrict__ inst_of,
+                                                            uint64_t *__restrict__ ikeys) {
+    const int64_t k = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t s = slot[k];
+    ikeys[k] = (s < (uint64_t) n) ? (uint64_t) inst_of[s] : 0ull;
+}
+
+// perm[j] = slot[order[j]], codes_out[j] = codes[order[j]]: the instance-major permutation.
+__global__ void __launch_bounds__(kThreads) compose_kernel(const uint32_t *__restrict__ order, int64_t n,
+                                                           const uint32_t *__restrict__ slot,
+                                                           const uint64_t *__restrict__ codes,
+                                                           uint32_t *__restrict__ perm,
+                                                           uint64_t *__restrict__ codes_out) {
+    const int64_t j = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint32_t k = order[j];
+    if (k >= (uint64_t) n) return;
+    perm[j] = slot[k];
+    codes_out[j] = codes[k];
+}
+
+unsigned blocks_for(int64_t n) { return (unsigned) ((n + kThreads - 1) / kThreads); }
+
+}  // namespace
+
+void launch_seg_bbox(const float4 *pos, const int2 *inst_range, int num_inst, float *inst_box, cudaStream_t s) {
+    if (num_inst <= 0) return;
+    seg_bbox_kernel<<<num_inst, kThreads, 0, s>>>(pos, inst_range, inst_box);
+}
+
+void launch_seg_morton(const float4 *pos, int64_t n, const int *inst_of, const float *inst_box, uint64_t *codes,
+                       uint32_t *hist, cudaStream_t s) {
+    if (n <= 0) return;
+    cudaMemsetAsync(hist, 0, 8 * 256 * sizeof(uint32_t), s);
+    int64_t blocks = (n + kThreads * 4 - 1) / (kThreads * 4);
+    blocks = blocks < 1 ? 1 : (blocks > 148 * 8 ? 148 * 8 : blocks);
+    seg_morton_kernel<<<(unsigned) blocks, kThreads, 0, s>>>(pos, n, inst_of, inst_box, codes, hist);
+}
+
+void launch_inst_keys(const uint32_t *slot, int64_t n, const int *inst_of, uint64_t *ikeys, cudaStream_t s) {
+    if (n <= 0) return;
+    inst_key_kernel<<<blocks_for(n), kThreads, 0, s>>>(slot, n, inst_of, ikeys);
+}
+
+void launch_compose(const uint32_t *order, int64_t n, const uint32_t *slot, const uint64_t *codes, uint32_t *perm,
+                    uint64_t *codes_out, cudaStream_t s) {
+    if (n <= 0) return;
+    compose_kernel<<<blocks_for(n), kThreads, 0, s>>>(order, n, slot, codes, perm, codes_out);
+}
+
+}  // namespace nbg

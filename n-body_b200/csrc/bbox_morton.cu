@@ -23,22 +23,6 @@ namespace {
 
 constexpr int kThreads = 256;
 
-__device__ __forceinline__ uint64_t expand_bits21(uint64_t i) {
-    i &= 0x1fffff;
-    i = (i | i << 32) & 0x1f00000000ffffULL;
-    i = (i | i << 16) & 0x1f0000ff0000ffULL;
-    i = (i | i << 8) & 0x100f00f00f00f00fULL;
-    i = (i | i << 4) & 0x10c30c30c30c30c3ULL;
-    i = (i | i << 2) & 0x1249249249249249ULL;
-    return i;
-}
-
-__device__ __forceinline__ uint64_t axis_cell(float v) {
-    float c = gmin(gmax(fmul(v, 2097152.f), 0.f), 2097151.f);
-    // NaN (zero scale: all positions equal) maps to cell 0.
-    return (c == c) ? __float2ull_rz(c) : 0ull;
-}
-
 __global__ void __launch_bounds__(kThreads) bbox_reduce_kernel(const float4 *__restrict__ pos, int64_t n,
                                                                BBoxAccum *__restrict__ acc) {
     float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
@@ -90,11 +74,7 @@ __global__ void __launch_bounds__(kThreads) morton_hist_kernel(const float4 *__r
     __syncthreads();
     const int64_t stride = (int64_t) gridDim.x * blockDim.x;
     for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        float4 p = __ldg(pos + i);
-        uint64_t cx = axis_cell(fdiv(fsub(p.x, mn[0]), scale));
-        uint64_t cy = axis_cell(fdiv(fsub(p.y, mn[1]), scale));
-        uint64_t cz = axis_cell(fdiv(fsub(p.z, mn[2]), scale));
-        uint64_t code = expand_bits21(cx) * 4u + expand_bits21(cy) * 2u + expand_bits21(cz);
+        const uint64_t code = morton_code(__ldg(pos + i), mn, scale);
         codes[i] = code;
 #pragma unroll
         for (int d = 0; d < 8; ++d) atomicAdd(&sh[d * 256 + (uint32_t) ((code >> (8 * d)) & 255u)], 1u);

@@ -61,6 +61,24 @@ struct nb_ctx {
     double *acc64 = nullptr;
     int64_t acc64_cap = 0;
 
+    // batch of independent instances (0: one instance set by nb_set_bodies)
+    int32_t num_inst = 0;
+    std::vector<int64_t> inst_start, inst_size;
+    int *inst_of = nullptr, *inst_root = nullptr;
+    float *inst_theta2 = nullptr, *inst_box = nullptr;
+    int2 *inst_range = nullptr;
+    int4 *groups = nullptr;
+    int64_t ngroups = 0;
+    uint64_t *ikeys = nullptr, *ikeys2 = nullptr;
+    uint32_t *ivals = nullptr, *ivals2 = nullptr;
+    uint32_t *inst_offsets = nullptr, *inst_lookback = nullptr, *inst_tiles = nullptr;
+    int inst_passes = 0;
+    const uint64_t *sorted_codes = nullptr;  // buffer holding the last pass's sorted codes
+
+    // CUDA graph of two consecutive steps (bodies ping-pong between two buffers each step)
+    bool use_graphs = false;
+    cudaGraphExec_t graph2 = nullptr;
+
     bool bbox_valid = false;  // bbox already holds the box of the current positions
     bool have_tree = false;
     bool have_acc = false;
@@ -119,6 +137,22 @@ int validate(nb_ctx *ctx, const nb_config *cfg) {
     if (!(cfg->theta >= 0.f)) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "theta must be >= 0");
     if (!(cfg->epsilon >= 0.f)) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "epsilon must be >= 0");
     return NB_OK;
+}
+
+void free_batch(nb_ctx *ctx) {
+    dev_free(ctx->inst_of); dev_free(ctx->inst_root); dev_free(ctx->inst_theta2); dev_free(ctx->inst_box);
+    dev_free(ctx->inst_range); dev_free(ctx->groups); dev_free(ctx->ikeys); dev_free(ctx->ikeys2);
+    dev_free(ctx->ivals); dev_free(ctx->ivals2); dev_free(ctx->inst_offsets); dev_free(ctx->inst_lookback);
+    dev_free(ctx->inst_tiles);
+    ctx->num_inst = 0;
+    ctx->ngroups = 0;
+    ctx->inst_start.clear();
+    ctx->inst_size.clear();
+}
+
+void drop_graph(nb_ctx *ctx) {
+    if (ctx->graph2) cudaGraphExecDestroy(ctx->graph2);
+    ctx->graph2 = nullptr;
 }
 
 void free_buffers(nb_ctx *ctx) {
@@ -231,6 +265,55 @@ int64_t launches_per_pass(const nb_ctx *ctx, bool with_bbox, bool with_drift) {
     return k + (with_bbox ? 1 : 0) + (with_drift ? 1 : 0);
 }
 
+// Force pass over a batch of instances: per-instance boxes and codes, a global code sort followed
+// by a stable sort on the instance id, one build over (instance, code, index) keys, and one
+// traversal over a group table whose 32-target groups never straddle instances.
+int force_pass_batch(nb_ctx *ctx, Marks &mk) {
+    const int64_t n = ctx->n;
+    cudaStream_t s = ctx->stream;
+    launch_seg_bbox(ctx->pos, ctx->inst_range, ctx->num_inst, ctx->inst_box, s);
+    mk.mark(kMorton);
+    launch_seg_morton(ctx->pos, n, ctx->inst_of, ctx->inst_box, ctx->keys, ctx->sw.hist, s);
+    mk.mark(kSort);
+    launch_radix_sort(ctx->keys, ctx->vals, n, ctx->sw, ctx->err, s);
+    launch_inst_keys(ctx->vals, n, ctx->inst_of, ctx->ikeys, s);
+    const int64_t tiles = sort_tiles(n);
+    cudaMemsetAsync(ctx->inst_lookback, 0, (size_t) ctx->inst_passes * tiles * 256 * sizeof(uint32_t), s);
+    cudaMemsetAsync(ctx->inst_tiles, 0, 8 * sizeof(uint32_t), s);
+    launch_radix_pass(ctx->ikeys, nullptr, ctx->ikeys2, ctx->ivals, n, 0, ctx->inst_offsets, ctx->inst_lookback,
+                      ctx->inst_tiles, ctx->err, s);
+    const uint32_t *order = ctx->ivals;
+    if (ctx->inst_passes == 2) {
+        launch_radix_pass(ctx->ikeys2, ctx->ivals, ctx->ikeys, ctx->ivals2, n, 1, ctx->inst_offsets,
+                          ctx->inst_lookback, ctx->inst_tiles, ctx->err, s);
+        order = ctx->ivals2;
+    }
+    launch_compose(order, n, ctx->vals, ctx->keys, ctx->sw.vals_alt, ctx->sw.keys_alt, s);
+    mk.mark(kGather);
+    launch_gather_state(ctx->sw.vals_alt, n, ctx->pos, ctx->vel, ctx->id, ctx->pos2, ctx->vel2, ctx->id2, s);
+    std::swap(ctx->pos, ctx->pos2);
+    std::swap(ctx->vel, ctx->vel2);
+    std::swap(ctx->id, ctx->id2);
+    mk.mark(kBuild);
+    BatchSegments seg;
+    seg.inst_of = ctx->inst_of;
+    seg.inst_theta2 = ctx->inst_theta2;
+    seg.inst_range = ctx->inst_range;
+    seg.inst_root = ctx->inst_root;
+    cudaMemsetAsync(ctx->inst_root, 0xFF, (size_t) ctx->num_inst * sizeof(int), s);
+    launch_build_tree(ctx->sw.keys_alt, ctx->pos, n, ctx->cfg.max_leaf_size, ctx->cfg.order, ctx->cfg.theta, ctx->tw,
+                      ctx->nodes, ctx->err, s, seg);
+    ctx->sorted_codes = ctx->sw.keys_alt;
+    mk.mark(kTraverse);
+    launch_bh_traverse(ctx->cfg.order, ctx->nodes, ctx->tw.num_nodes, ctx->pos, n, ctx->pos, n, ctx->cfg.G,
+                       ctx->cfg.epsilon, ctx->acc, ctx->counts, ctx->trav, ctx->err, s, ctx->groups, ctx->ngroups,
+                       ctx->inst_root);
+    ctx->have_tree = true;
+    ctx->acc_is_bh = true;
+    if (ctx->timing) ctx->times.launches += launches_per_pass(ctx, false, false) + 4 + ctx->inst_passes;
+    return check_cuda(ctx, cudaGetLastError(), "batched force pass");
+}
+
 // One force pass over the current state. Leaves accelerations in ctx->acc (current order).
 int force_pass(nb_ctx *ctx, Marks &mk) {
     const int64_t n = ctx->n;
@@ -246,6 +329,7 @@ int force_pass(nb_ctx *ctx, Marks &mk) {
         if (ctx->timing) ctx->times.launches += 1;
         return check_cuda(ctx, cudaGetLastError(), "naive direct sum");
     }
+    if (ctx->num_inst > 0) return force_pass_batch(ctx, mk);
     if (need_bbox) {
         launch_bbox_reset(ctx->bbox, s);
         launch_bbox_reduce(ctx->pos, n, ctx->bbox, s);
@@ -262,6 +346,7 @@ int force_pass(nb_ctx *ctx, Marks &mk) {
     mk.mark(kBuild);
     launch_build_tree(ctx->keys, ctx->pos, n, ctx->cfg.max_leaf_size, ctx->cfg.order, ctx->cfg.theta, ctx->tw,
                       ctx->nodes, ctx->err, s);
+    ctx->sorted_codes = ctx->keys;
     mk.mark(kTraverse);
     launch_bh_traverse(ctx->cfg.order, ctx->nodes, ctx->tw.num_nodes, ctx->pos, n, ctx->pos, n, ctx->cfg.G,
                        ctx->cfg.epsilon, ctx->acc, ctx->counts, ctx->trav, ctx->err, s);
@@ -355,6 +440,8 @@ int nb_destroy(nb_ctx *ctx) {
     if (!ctx) return NB_OK;
     cudaSetDevice(ctx->cfg.device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    drop_graph(ctx);
+    free_batch(ctx);
     free_buffers(ctx);
     dev_free(ctx->bbox); dev_free(ctx->counts); dev_free(ctx->err); dev_free(ctx->sw.hist);
     dev_free(ctx->sw.offsets); dev_free(ctx->sw.tile_counter); dev_free(ctx->tw.num_nodes); dev_free(ctx->acc64);
@@ -379,6 +466,7 @@ int nb_set_config(nb_ctx *ctx, const nb_config *cfg) {
     if (cfg->device != ctx->cfg.device) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "the device cannot change");
     ctx->cfg = *cfg;
     ctx->have_tree = false;
+    drop_graph(ctx);
     refresh_names(ctx);
     return NB_OK;
 }
@@ -406,6 +494,8 @@ static int set_bodies_impl(nb_ctx *ctx, int64_t n, const void *pm, const void *v
     if (n > 0 && !pm) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "positions are NULL");
     rc = ensure_capacity(ctx, n);
     if (rc != NB_OK) return rc;
+    free_batch(ctx);
+    drop_graph(ctx);
     ctx->n = n;
     const size_t bytes = (size_t) n * sizeof(float4);
     if (n > 0) {
@@ -503,31 +593,77 @@ int nb_get_accelerations_device(nb_ctx *ctx, void *d_acc_out) {
     return copy_acc_out(ctx, d_acc_out, cudaMemcpyDeviceToDevice, false);
 }
 
+static int one_step(nb_ctx *ctx) {
+    Marks mk(ctx);
+    int rc;
+    if (ctx->n > 0) {
+        rc = force_pass(ctx, mk);
+        if (rc != NB_OK) return rc;
+        mk.mark(kIntegrate);
+        const bool reduce_box = ctx->cfg.solver != NB_SOLVER_NAIVE && ctx->num_inst == 0;
+        if (reduce_box) launch_bbox_reset(ctx->bbox, ctx->stream);
+        launch_kick_drift(ctx->pos, ctx->vel, ctx->acc, ctx->n, ctx->cfg.time_step, reduce_box ? ctx->bbox : nullptr,
+                          ctx->stream);
+        ctx->bbox_valid = reduce_box;
+        if (ctx->timing) ctx->times.launches += 1;
+        rc = check_cuda(ctx, cudaGetLastError(), "kick-drift");
+        if (rc != NB_OK) return rc;
+    } else {
+        mk.mark(kMorton); mk.mark(kSort); mk.mark(kGather); mk.mark(kBuild); mk.mark(kTraverse);
+        mk.mark(kIntegrate);
+    }
+    mk.mark(kEnd);
+    mk.commit();
+    ctx->have_acc = true;
+    return NB_OK;
+}
+
+// Two steps captured once and replayed: after two steps the bodies are back in the same buffers,
+// so the graph's pointers stay valid. Timing marks are not captured.
+static int graph_steps(nb_ctx *ctx, int32_t pairs) {
+    if (!ctx->graph2) {
+        // nb_step has run one plain step before the first capture, so the captured steps see the
+        // steady-state shape (bounding box from the previous drift, launch settings initialised)
+        cudaGraph_t g = nullptr;
+        NB_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        int rc = one_step(ctx);
+        if (rc == NB_OK) rc = one_step(ctx);
+        cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+        if (rc != NB_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        NB_TRY(e, "end capture");
+        e = cudaGraphInstantiate(&ctx->graph2, g, 0);
+        cudaGraphDestroy(g);
+        NB_TRY(e, "instantiate graph");
+    }
+    for (int32_t k = 0; k < pairs; ++k) NB_TRY(cudaGraphLaunch(ctx->graph2, ctx->stream), "launch graph");
+    return NB_OK;
+}
+
 int nb_step(nb_ctx *ctx, int32_t steps) {
     int rc = begin(ctx);
     if (rc != NB_OK) return rc;
     if (steps < 0) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "negative step count");
-    for (int32_t k = 0; k < steps; ++k) {
-        Marks mk(ctx);
-        if (ctx->n > 0) {
-            rc = force_pass(ctx, mk);
+    int32_t k = 0;
+    if (ctx->use_graphs && !ctx->timing && ctx->n > 0) {
+        if (!ctx->graph2) {  // the first step runs uncaptured (bounding box of the initial state)
+            if (steps == 0) return NB_OK;
+            rc = one_step(ctx);
             if (rc != NB_OK) return rc;
-            mk.mark(kIntegrate);
-            const bool reduce_box = ctx->cfg.solver != NB_SOLVER_NAIVE;
-            if (reduce_box) launch_bbox_reset(ctx->bbox, ctx->stream);
-            launch_kick_drift(ctx->pos, ctx->vel, ctx->acc, ctx->n, ctx->cfg.time_step,
-                              reduce_box ? ctx->bbox : nullptr, ctx->stream);
-            ctx->bbox_valid = reduce_box;
-            if (ctx->timing) ctx->times.launches += 1;
-            rc = check_cuda(ctx, cudaGetLastError(), "kick-drift");
-            if (rc != NB_OK) return rc;
-        } else {
-            mk.mark(kMorton); mk.mark(kSort); mk.mark(kGather); mk.mark(kBuild); mk.mark(kTraverse);
-            mk.mark(kIntegrate);
+            k = 1;
         }
-        mk.mark(kEnd);
-        mk.commit();
-        ctx->have_acc = true;
+        const int32_t pairs = (steps - k) / 2;
+        if (pairs > 0) {
+            rc = graph_steps(ctx, pairs);
+            if (rc != NB_OK) return rc;
+            k += 2 * pairs;
+        }
+    }
+    for (; k < steps; ++k) {
+        rc = one_step(ctx);
+        if (rc != NB_OK) return rc;
     }
     return NB_OK;
 }
@@ -598,7 +734,8 @@ int nb_get_tree(nb_ctx *ctx, int64_t *num_nodes, int32_t *record_floats, uint64_
     }
     const int64_t n = ctx->n;
     if (sorted_codes && n > 0)
-        NB_TRY(cudaMemcpyAsync(sorted_codes, ctx->keys, (size_t) n * 8, cudaMemcpyDeviceToHost, ctx->stream), "codes");
+        NB_TRY(cudaMemcpyAsync(sorted_codes, ctx->sorted_codes, (size_t) n * 8, cudaMemcpyDeviceToHost, ctx->stream),
+               "codes");
     if (sorted_ids && n > 0)
         NB_TRY(cudaMemcpyAsync(sorted_ids, ctx->id, (size_t) n * 4, cudaMemcpyDeviceToHost, ctx->stream), "ids");
     if (records && nn > 0) {
@@ -640,6 +777,104 @@ int nb_direct_device(nb_ctx *ctx, int64_t n, const void *d_bodies, int64_t nt, c
     else
         return fail(ctx, NB_ERR_INVALID_ARGUMENT, "precision must be 32 or 64");
     return check_cuda(ctx, cudaGetLastError(), "direct sum");
+}
+
+int nb_set_instances(nb_ctx *ctx, int32_t count, const int64_t *sizes, const float *thetas, const float *pos_mass,
+                     const float *velocity) {
+    int rc = begin(ctx);
+    if (rc != NB_OK) return rc;
+    if (count < 1 || count > 65535 || !sizes) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "1..65535 instances required");
+    int64_t n = 0;
+    for (int32_t k = 0; k < count; ++k) {
+        if (sizes[k] < 1) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "every instance needs at least one body");
+        n += sizes[k];
+    }
+    if (n > kMaxBodies) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "body count out of range");
+    if (thetas)
+        for (int32_t k = 0; k < count; ++k)
+            if (!(thetas[k] >= 0.f)) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "theta must be >= 0");
+    rc = set_bodies_impl(ctx, n, pos_mass, velocity, cudaMemcpyHostToDevice);
+    if (rc != NB_OK) return rc;
+    // host-side tables (sizes are fixed for the life of the batch)
+    std::vector<int> inst_of((size_t) n);
+    std::vector<int2> range((size_t) count);
+    std::vector<float> theta2((size_t) count);
+    std::vector<int4> groups;
+    std::vector<uint32_t> offsets(8 * 256 + 8, 0), hist(2 * 256, 0);
+    ctx->inst_start.resize(count);
+    ctx->inst_size.assign(sizes, sizes + count);
+    int64_t start = 0;
+    for (int32_t k = 0; k < count; ++k) {
+        ctx->inst_start[k] = start;
+        for (int64_t i = 0; i < sizes[k]; ++i) inst_of[start + i] = k;
+        range[k] = make_int2((int) start, (int) (start + sizes[k] - 1));
+        const float th = thetas ? thetas[k] : ctx->cfg.theta;
+        theta2[k] = th * th;  // the reference compares against theta * theta in float
+        for (int64_t g = 0; g < sizes[k]; g += 32)
+            groups.push_back(make_int4((int) (start + g), (int) std::min<int64_t>(32, sizes[k] - g), k, 0));
+        hist[k & 255] += (uint32_t) sizes[k];
+        hist[256 + (k >> 8)] += (uint32_t) sizes[k];
+        start += sizes[k];
+    }
+    const int passes = count > 256 ? 2 : 1;
+    for (int p = 0; p < passes; ++p) {
+        uint32_t acc = 0;
+        bool trivial = false;
+        for (int d = 0; d < 256; ++d) {
+            offsets[p * 256 + d] = acc;
+            acc += hist[p * 256 + d];
+            if ((int64_t) hist[p * 256 + d] == n) trivial = true;
+        }
+        offsets[8 * 256 + p] = trivial ? 1u : 0u;
+    }
+    const int64_t tiles = sort_tiles(n);
+    NB_TRY(dev_alloc(&ctx->inst_of, (size_t) n), "alloc batch");
+    NB_TRY(dev_alloc(&ctx->inst_root, (size_t) count), "alloc batch");
+    NB_TRY(dev_alloc(&ctx->inst_theta2, (size_t) count), "alloc batch");
+    NB_TRY(dev_alloc(&ctx->inst_box, (size_t) count * 6), "alloc batch");
+    NB_TRY(dev_alloc(&ctx->inst_range, (size_t) count), "alloc batch");
+    NB_TRY(dev_alloc(&ctx->groups, groups.size()), "alloc batch");
+    NB_TRY(dev_alloc(&ctx->ikeys, (size_t) n), "alloc batch");
+    NB_TRY(dev_alloc(&ctx->ikeys2, (size_t) n), "alloc batch");
+    NB_TRY(dev_alloc(&ctx->ivals, (size_t) n), "alloc batch");
+    NB_TRY(dev_alloc(&ctx->ivals2, (size_t) n), "alloc batch");
+    NB_TRY(dev_alloc(&ctx->inst_offsets, offsets.size()), "alloc batch");
+    NB_TRY(dev_alloc(&ctx->inst_lookback, (size_t) 2 * tiles * 256), "alloc batch");
+    NB_TRY(dev_alloc(&ctx->inst_tiles, 8), "alloc batch");
+    cudaStream_t s = ctx->stream;
+    NB_TRY(cudaMemcpyAsync(ctx->inst_of, inst_of.data(), inst_of.size() * sizeof(int), cudaMemcpyHostToDevice, s), "copy");
+    NB_TRY(cudaMemcpyAsync(ctx->inst_theta2, theta2.data(), theta2.size() * sizeof(float), cudaMemcpyHostToDevice, s),
+           "copy");
+    NB_TRY(cudaMemcpyAsync(ctx->inst_range, range.data(), range.size() * sizeof(int2), cudaMemcpyHostToDevice, s), "copy");
+    NB_TRY(cudaMemcpyAsync(ctx->groups, groups.data(), groups.size() * sizeof(int4), cudaMemcpyHostToDevice, s), "copy");
+    NB_TRY(cudaMemcpyAsync(ctx->inst_offsets, offsets.data(), offsets.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s),
+           "copy");
+    ctx->num_inst = count;
+    ctx->ngroups = (int64_t) groups.size();
+    ctx->inst_passes = passes;
+    return check_cuda(ctx, cudaStreamSynchronize(s), "set instances");
+}
+
+int32_t nb_instance_count(const nb_ctx *ctx) { return ctx ? (ctx->num_inst > 0 ? ctx->num_inst : 1) : -1; }
+
+int nb_get_instance_roots(nb_ctx *ctx, int32_t *roots) {
+    int rc = begin(ctx);
+    if (rc != NB_OK) return rc;
+    if (!roots) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "output is NULL");
+    if (ctx->num_inst == 0) {
+        roots[0] = 0;
+        return NB_OK;
+    }
+    NB_TRY(cudaMemcpyAsync(roots, ctx->inst_root, (size_t) ctx->num_inst * sizeof(int), cudaMemcpyDeviceToHost,
+                           ctx->stream), "read roots");
+    return device_status(ctx);
+}
+
+int nb_enable_graphs(nb_ctx *ctx, int enable) {
+    if (!ctx) return NB_ERR_INVALID_ARGUMENT;
+    ctx->use_graphs = enable != 0;
+    if (!ctx->use_graphs) drop_graph(ctx);
+    return NB_OK;
 }
 
 void *nb_host_alloc(size_t bytes) {

@@ -35,33 +35,41 @@ namespace {
 
 constexpr int kThreads = 256;
 
-__device__ __forceinline__ int prefix_delta(const uint64_t *__restrict__ codes, int n, int i, int j) {
+// Length of the common prefix of the keys (instance, code, index) at sorted positions i and j;
+// -1 outside the array. Without instances the instance field is equal everywhere.
+__device__ __forceinline__ int prefix_delta(const uint64_t *__restrict__ codes, const int *__restrict__ inst_of, int n,
+                                            int i, int j) {
     if (j < 0 || j >= n) return -1;
+    if (inst_of) {
+        const int a = inst_of[i], b = inst_of[j];
+        if (a != b) return __clz(a ^ b);
+    }
     const uint64_t a = codes[i], b = codes[j];
-    return (a != b) ? __clzll(a ^ b) : 64 + __clz(i ^ j);
+    return 32 + ((a != b) ? __clzll(a ^ b) : 64 + __clz(i ^ j));
 }
 
-__global__ void __launch_bounds__(kThreads) karras_kernel(const uint64_t *__restrict__ codes, int n, int leaf,
+__global__ void __launch_bounds__(kThreads) karras_kernel(const uint64_t *__restrict__ codes,
+                                                          const int *__restrict__ inst_of, int n, int leaf,
                                                           int2 *__restrict__ range, int *__restrict__ left,
                                                           int *__restrict__ right, int *__restrict__ parent,
                                                           uint8_t *__restrict__ splittable) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
-    const int dn = prefix_delta(codes, n, i, i + 1);
-    const int dp = prefix_delta(codes, n, i, i - 1);
+    const int dn = prefix_delta(codes, inst_of, n, i, i + 1);
+    const int dp = prefix_delta(codes, inst_of, n, i, i - 1);
     const int d = (dn > dp) ? 1 : -1;
     const int dmin = (d > 0) ? dp : dn;
     int lmax = 2;
-    while (prefix_delta(codes, n, i, i + lmax * d) > dmin) lmax <<= 1;
+    while (prefix_delta(codes, inst_of, n, i, i + lmax * d) > dmin) lmax <<= 1;
     int l = 0;
     for (int t = lmax >> 1; t >= 1; t >>= 1)
-        if (prefix_delta(codes, n, i, i + (l + t) * d) > dmin) l += t;
+        if (prefix_delta(codes, inst_of, n, i, i + (l + t) * d) > dmin) l += t;
     const int j = i + l * d;
-    const int dnode = prefix_delta(codes, n, i, j);
+    const int dnode = prefix_delta(codes, inst_of, n, i, j);
     int s = 0, t = l;
     do {
         t = (t + 1) >> 1;
-        if (prefix_delta(codes, n, i, i + (s + t) * d) > dnode) s += t;
+        if (prefix_delta(codes, inst_of, n, i, i + (s + t) * d) > dnode) s += t;
     } while (t > 1);
     const int gamma = i + s * d + (d < 0 ? -1 : 0);
     const int first = min(i, j), last = max(i, j);
@@ -72,7 +80,9 @@ __global__ void __launch_bounds__(kThreads) karras_kernel(const uint64_t *__rest
     range[i] = make_int2(first, last);
     if (lc >= 0) parent[lc] = i;
     if (rc >= 0) parent[rc] = i;
-    splittable[i] = (uint8_t) ((last - first + 1 > leaf) && (codes[first] != codes[last]));
+    // A node spanning several instances only connects their trees: it is always split.
+    const bool spans = inst_of && inst_of[first] != inst_of[last];
+    splittable[i] = (uint8_t) (spans || ((last - first + 1 > leaf) && (codes[first] != codes[last])));
 }
 
 template<int ORDER>
@@ -267,9 +277,21 @@ __device__ void write_record(const NodeArrays &nodes, int pre, const Summ<ORDER>
     }
 }
 
+// The MAC threshold parameter of the node covering bodies [first, last], and the registration
+// of an instance root (a node whose range is exactly one instance).
+__device__ __forceinline__ float node_theta2(const BatchSegments &seg, float t, int first) {
+    return seg.inst_theta2 ? seg.inst_theta2[seg.inst_of[first]] : t;
+}
+__device__ __forceinline__ void register_root(const BatchSegments &seg, int pre, int first, int last) {
+    if (!seg.inst_root) return;
+    const int k = seg.inst_of ? seg.inst_of[first] : 0;
+    const int2 r = seg.inst_range[k];
+    if (r.x == first && r.y == last) seg.inst_root[k] = pre;
+}
+
 template<int ORDER>
 __global__ void __launch_bounds__(kThreads) emit_kernel(int n, TreeWorkspace tw, float t, NodeArrays nodes,
-                                                        uint32_t *err) {
+                                                        uint32_t *err, BatchSegments seg) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1 || !tw.splittable[i]) return;
     int pre = 0;
@@ -287,14 +309,19 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(int n, TreeWorkspace tw,
     const int lc = tw.left[i], rc = tw.right[i];
     const int lslot = slot_of(lc, n);
     const int right_pre = pre + 1 + tw.cnt[lslot];
-    write_record<ORDER>(nodes, pre, load_slot<ORDER>(tw, i), t, right_pre, -1, err);
+    const int2 ri = tw.range[i];
+    write_record<ORDER>(nodes, pre, load_slot<ORDER>(tw, i), node_theta2(seg, t, ri.x), right_pre, -1, err);
+    register_root(seg, pre, ri.x, ri.y);
     if (is_final_leaf(tw.splittable, lc)) {
         int2 r = lc < 0 ? make_int2(~lc, ~lc) : tw.range[lc];
-        write_record<ORDER>(nodes, pre + 1, load_slot<ORDER>(tw, lslot), t, r.x, r.y + 1, err);
+        write_record<ORDER>(nodes, pre + 1, load_slot<ORDER>(tw, lslot), node_theta2(seg, t, r.x), r.x, r.y + 1, err);
+        register_root(seg, pre + 1, r.x, r.y);
     }
     if (is_final_leaf(tw.splittable, rc)) {
         int2 r = rc < 0 ? make_int2(~rc, ~rc) : tw.range[rc];
-        write_record<ORDER>(nodes, right_pre, load_slot<ORDER>(tw, slot_of(rc, n)), t, r.x, r.y + 1, err);
+        write_record<ORDER>(nodes, right_pre, load_slot<ORDER>(tw, slot_of(rc, n)), node_theta2(seg, t, r.x), r.x,
+                            r.y + 1, err);
+        register_root(seg, right_pre, r.x, r.y);
     }
     if (i == 0) *tw.num_nodes = tw.cnt[i];
 }
@@ -303,16 +330,18 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(int n, TreeWorkspace tw,
 // or every code equal).
 template<int ORDER>
 __global__ void root_leaf_kernel(const float4 *__restrict__ bodies, int n, TreeWorkspace tw, float t,
-                                 NodeArrays nodes, uint32_t *err) {
+                                 NodeArrays nodes, uint32_t *err, BatchSegments seg) {
     if (n > 1 && tw.splittable[0]) return;
-    write_record<ORDER>(nodes, 0, leaf_summary<ORDER>(bodies, 0, n - 1), t, 0, n, err);
+    write_record<ORDER>(nodes, 0, leaf_summary<ORDER>(bodies, 0, n - 1), node_theta2(seg, t, 0), 0, n, err);
+    register_root(seg, 0, 0, n - 1);
     *tw.num_nodes = 1;
 }
 
 }  // namespace
 
 void launch_build_tree(const uint64_t *sorted_codes, const float4 *bodies, int64_t n64, int leaf, int order,
-                       float theta, TreeWorkspace &tw, const NodeArrays &nodes, uint32_t *err, cudaStream_t s) {
+                       float theta, TreeWorkspace &tw, const NodeArrays &nodes, uint32_t *err, cudaStream_t s,
+                       const BatchSegments &seg) {
     const int n = (int) n64;
     if (n <= 0) {
         cudaMemsetAsync(tw.num_nodes, 0, sizeof(int), s);
@@ -322,22 +351,22 @@ void launch_build_tree(const uint64_t *sorted_codes, const float4 *bodies, int64
     const int internal = n - 1;
     const int blocks = internal > 0 ? (internal + kThreads - 1) / kThreads : 1;
     if (internal > 0) {
-        karras_kernel<<<blocks, kThreads, 0, s>>>(sorted_codes, n, leaf, tw.range, tw.left, tw.right, tw.parent,
-                                                  tw.splittable);
+        karras_kernel<<<blocks, kThreads, 0, s>>>(sorted_codes, seg.inst_of, n, leaf, tw.range, tw.left, tw.right,
+                                                  tw.parent, tw.splittable);
         cudaMemsetAsync(tw.visit, 0, (size_t) internal * sizeof(int), s);
     }
     if (order == 1) {
         if (internal > 0) {
             summarize_kernel<1><<<blocks, kThreads, 0, s>>>(bodies, n, tw, err);
-            emit_kernel<1><<<blocks, kThreads, 0, s>>>(n, tw, t, nodes, err);
+            emit_kernel<1><<<blocks, kThreads, 0, s>>>(n, tw, t, nodes, err, seg);
         }
-        root_leaf_kernel<1><<<1, 1, 0, s>>>(bodies, n, tw, t, nodes, err);
+        root_leaf_kernel<1><<<1, 1, 0, s>>>(bodies, n, tw, t, nodes, err, seg);
     } else {
         if (internal > 0) {
             summarize_kernel<2><<<blocks, kThreads, 0, s>>>(bodies, n, tw, err);
-            emit_kernel<2><<<blocks, kThreads, 0, s>>>(n, tw, t, nodes, err);
+            emit_kernel<2><<<blocks, kThreads, 0, s>>>(n, tw, t, nodes, err, seg);
         }
-        root_leaf_kernel<2><<<1, 1, 0, s>>>(bodies, n, tw, t, nodes, err);
+        root_leaf_kernel<2><<<1, 1, 0, s>>>(bodies, n, tw, t, nodes, err, seg);
     }
 }
 

@@ -43,6 +43,28 @@ __host__ __device__ __forceinline__ float ordered_to_float(uint32_t o) {
 #endif
 }
 
+// Morton code of one position (MortonSort.h:46-73): v = (p - min) / scale, clamp(v * 2^21, 0,
+// 2^21 - 1) per axis, truncated and interleaved x*4 + y*2 + z. NaN (zero scale) maps to cell 0.
+__device__ __forceinline__ uint64_t expand_bits21(uint64_t i) {
+    i &= 0x1fffff;
+    i = (i | i << 32) & 0x1f00000000ffffULL;
+    i = (i | i << 16) & 0x1f0000ff0000ffULL;
+    i = (i | i << 8) & 0x100f00f00f00f00fULL;
+    i = (i | i << 4) & 0x10c30c30c30c30c3ULL;
+    i = (i | i << 2) & 0x1249249249249249ULL;
+    return i;
+}
+__device__ __forceinline__ uint64_t axis_cell(float v) {
+    const float c = gmin(gmax(fmul(v, 2097152.f), 0.f), 2097151.f);
+    return (c == c) ? __float2ull_rz(c) : 0ull;
+}
+__device__ __forceinline__ uint64_t morton_code(float4 p, const float mn[3], float scale) {
+    const uint64_t cx = axis_cell(fdiv(fsub(p.x, mn[0]), scale));
+    const uint64_t cy = axis_cell(fdiv(fsub(p.y, mn[1]), scale));
+    const uint64_t cz = axis_cell(fdiv(fsub(p.z, mn[2]), scale));
+    return expand_bits21(cx) * 4u + expand_bits21(cy) * 2u + expand_bits21(cz);
+}
+
 // Global bounding box accumulator: 6 ordered uints, all reduced with atomicMin.
 // [0..2] = ordered(min.xyz), [3..5] = ~ordered(max.xyz). Reset by filling with 0xFF bytes.
 struct BBoxAccum {
@@ -111,6 +133,22 @@ size_t sort_lookback_words(int64_t n);
 // Sorts (keys, iota) by key; the sorted keys and slot indices end in keys/vals (ping-pong inside).
 void launch_radix_sort(uint64_t *keys, uint32_t *vals, int64_t n, SortWorkspace &ws, uint32_t *err,
                        cudaStream_t s);
+// One stable one-sweep pass on digit `pass` (bits 8*pass .. 8*pass+7) of the keys. offsets holds
+// the exclusive digit prefixes at [pass*256 + d] and a trivial-pass flag at [8*256 + pass];
+// lookback (pass x tiles x 256 words) and tile_counter[pass] must be zero. Pass 0 ignores vals_in
+// and emits the input positions as values.
+void launch_radix_pass(const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out, uint32_t *vals_out,
+                       int64_t n, int pass, const uint32_t *offsets, uint32_t *lookback, uint32_t *tile_counter,
+                       uint32_t *err, cudaStream_t s);
+
+// Several independent instances laid out back to back in one body array (device pointers).
+// With inst_of == nullptr the body array is a single instance.
+struct BatchSegments {
+    const int *inst_of = nullptr;        // instance of each body position (positions stay in their segment)
+    const float *inst_theta2 = nullptr;  // RN(theta * theta) per instance
+    const int2 *inst_range = nullptr;    // first and last (inclusive) body position per instance
+    int *inst_root = nullptr;            // written by the build: preorder index of each instance's root
+};
 
 // lbvh_build.cu
 struct TreeWorkspace {
@@ -126,7 +164,8 @@ struct TreeWorkspace {
     int64_t capacity = 0;
 };
 void launch_build_tree(const uint64_t *sorted_codes, const float4 *bodies, int64_t n, int leaf, int order, float theta,
-                       TreeWorkspace &tw, const NodeArrays &nodes, uint32_t *err, cudaStream_t s);
+                       TreeWorkspace &tw, const NodeArrays &nodes, uint32_t *err, cudaStream_t s,
+                       const BatchSegments &seg = BatchSegments());
 
 // traverse.cu
 struct TraverseWorkspace {
@@ -137,9 +176,13 @@ struct TraverseWorkspace {
 constexpr int kTraverseStack = 4608;
 // Resident warps of the persistent traversal grid on `device` (for sizing TraverseWorkspace).
 int64_t traverse_resident_warps(int device);
+// groups (optional): one int4 (first target, target count <= 32, instance, 0) per warp task; the
+// traversal of a group starts at inst_root[instance]. Without groups, targets are cut into
+// consecutive groups of 32 that start at node 0.
 void launch_bh_traverse(int order, const NodeArrays &nodes, const int *num_nodes, const float4 *bodies, int64_t n_bodies,
                         const float4 *targets, int64_t n_targets, float G, float eps, float4 *acc,
-                        unsigned long long *counts, TraverseWorkspace &ws, uint32_t *err, cudaStream_t s);
+                        unsigned long long *counts, TraverseWorkspace &ws, uint32_t *err, cudaStream_t s,
+                        const int4 *groups = nullptr, int64_t num_groups = 0, const int *inst_root = nullptr);
 
 // direct_sum.cu
 void launch_direct_f32(const float4 *bodies, int64_t n, const float4 *targets, int64_t nt, float G, float eps,
@@ -154,6 +197,14 @@ void launch_scatter_by_id(const uint32_t *id, int64_t n, const float4 *src, floa
 void launch_kick_drift(float4 *pos, float4 *vel, const float4 *acc, int64_t n, float dt, BBoxAccum *next_bbox,
                        cudaStream_t s);
 void launch_iota(uint32_t *id, int64_t n, cudaStream_t s);
+
+// batch.cu
+void launch_seg_bbox(const float4 *pos, const int2 *inst_range, int num_inst, float *inst_box, cudaStream_t s);
+void launch_seg_morton(const float4 *pos, int64_t n, const int *inst_of, const float *inst_box, uint64_t *codes,
+                       uint32_t *hist, cudaStream_t s);
+void launch_inst_keys(const uint32_t *slot, int64_t n, const int *inst_of, uint64_t *ikeys, cudaStream_t s);
+void launch_compose(const uint32_t *order, int64_t n, const uint32_t *slot, const uint64_t *codes, uint32_t *perm,
+                    uint64_t *codes_out, cudaStream_t s);
 
 // Largest number of bodies one context accepts (30-bit counts in the sort's look-back words,
 // 31-bit body indices in the tree).

@@ -223,6 +223,14 @@ int64_t sort_tiles(int64_t n) { return (n + kTile - 1) / kTile; }
 
 size_t sort_lookback_words(int64_t n) { return (size_t) kPasses * (size_t) (sort_tiles(n) > 0 ? sort_tiles(n) : 1) * 256; }
 
+void launch_radix_pass(const uint64_t *keys_in, const uint32_t *vals_in, uint64_t *keys_out, uint32_t *vals_out,
+                       int64_t n, int pass, const uint32_t *offsets, uint32_t *lookback, uint32_t *tile_counter,
+                       uint32_t *err, cudaStream_t s) {
+    if (n <= 0) return;
+    onesweep_kernel<<<(unsigned) sort_tiles(n), kThreads, 0, s>>>(keys_in, vals_in, keys_out, vals_out, n, pass,
+                                                                   offsets, lookback, tile_counter, err);
+}
+
 void launch_radix_sort(uint64_t *keys, uint32_t *vals, int64_t n, SortWorkspace &ws, uint32_t *err,
                        cudaStream_t s) {
     if (n <= 0) return;

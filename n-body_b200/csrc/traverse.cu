@@ -208,7 +208,8 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
                                                       float eps, float4 *__restrict__ acc,
                                                       unsigned long long *__restrict__ counts,
                                                       int2 *__restrict__ stack_base, unsigned *__restrict__ group_counter,
-                                                      uint32_t *__restrict__ err) {
+                                                      uint32_t *__restrict__ err, const int4 *__restrict__ groups,
+                                                      int num_group_tasks, const int *__restrict__ inst_root) {
     __shared__ WarpLists lists[kWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     WarpLists &L = lists[warp];
@@ -217,7 +218,7 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
     const int2 *__restrict__ link = nodes.link;
     const float4 *__restrict__ pay = nodes.pay;
     const int num_nodes = *num_nodes_p;
-    const int num_groups = (n_targets + 31) / 32;
+    const int num_groups = groups ? num_group_tasks : (n_targets + 31) / 32;
     const uint32_t lt = lanemask_lt();
     // A valid tree needs fewer chunk rounds than it has nodes for one group; the cap only bounds
     // the work on a corrupted tree.
@@ -229,8 +230,15 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
         if (lane == 0) g = (int) atomicAdd(group_counter, 1u);
         g = __shfl_sync(kFull, g, 0);
         if (g >= num_groups) break;
-        const int i = g * 32 + lane;
-        const bool valid = i < n_targets;
+        int first = g * 32, count = min(32, n_targets - g * 32), root = 0;
+        if (groups) {
+            const int4 ge = groups[g];
+            first = ge.x;
+            count = ge.y;
+            root = inst_root[ge.z];
+        }
+        const int i = first + lane;
+        const bool valid = lane < count && i < n_targets;
         const float4 p = valid ? targets[i] : make_float4(0.f, 0.f, 0.f, 0.f);
         const uint32_t full = __ballot_sync(kFull, valid);
         float lo[3] = {valid ? p.x : FLT_MAX, valid ? p.y : FLT_MAX, valid ? p.z : FLT_MAX};
@@ -245,9 +253,11 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
         }
         L.tpos[lane] = p;
         int top = 0, napprox = 0, npp = 0, nmixed = 0, npriv = 0;
-        if (num_nodes > 0) {
-            if (lane == 0) stack[0] = make_int2(0, (int) full);
+        if (num_nodes > 0 && root >= 0 && root < num_nodes) {
+            if (lane == 0) stack[0] = make_int2(root, (int) full);
             top = 1;
+        } else if (num_nodes > 0 && lane == 0) {
+            atomicOr(err, (uint32_t) kErrTraverseLimit);  // a group without a valid tree root
         }
         __syncwarp();
         float ax = 0.f, ay = 0.f, az = 0.f;
@@ -422,17 +432,19 @@ int sm_count(int device) {
 template<int ORDER, bool EPS0>
 void launch_variant(const NodeArrays &nodes, const int *num_nodes, const float4 *bodies, int n_bodies,
                     const float4 *targets, int nt, float G, float eps, float4 *acc, unsigned long long *counts,
-                    TraverseWorkspace &ws, uint32_t *err, cudaStream_t s) {
+                    TraverseWorkspace &ws, uint32_t *err, cudaStream_t s, const int4 *gtab, int64_t ngroups,
+                    const int *inst_root) {
     int device = 0;
     cudaGetDevice(&device);
     int64_t blocks = (int64_t) sm_count(device) * blocks_per_sm<ORDER, EPS0>();
     blocks = std::min<int64_t>(blocks, ws.warps / kWarps);
-    const int64_t groups = (nt + 31) / 32;
+    const int64_t groups = gtab ? ngroups : (nt + 31) / 32;
     blocks = std::min<int64_t>(blocks, (groups + kWarps - 1) / kWarps);
     if (blocks < 1) blocks = 1;
     cudaMemsetAsync(ws.group_counter, 0, sizeof(unsigned), s);
     bh_kernel<ORDER, EPS0><<<(unsigned) blocks, kThreads, 0, s>>>(nodes, num_nodes, bodies, n_bodies, targets, nt, G,
-                                                                   eps, acc, counts, ws.stack, ws.group_counter, err);
+                                                                   eps, acc, counts, ws.stack, ws.group_counter, err,
+                                                                   gtab, (int) ngroups, inst_root);
 }
 
 }  // namespace
@@ -445,15 +457,16 @@ int64_t traverse_resident_warps(int device) {
 
 void launch_bh_traverse(int order, const NodeArrays &nodes, const int *num_nodes, const float4 *bodies, int64_t n_bodies,
                         const float4 *targets, int64_t n_targets, float G, float eps, float4 *acc,
-                        unsigned long long *counts, TraverseWorkspace &ws, uint32_t *err, cudaStream_t s) {
+                        unsigned long long *counts, TraverseWorkspace &ws, uint32_t *err, cudaStream_t s,
+                        const int4 *gtab, int64_t ngroups, const int *inst_root) {
     if (n_targets <= 0) return;
     const int nb = (int) n_bodies, nt = (int) n_targets;
     if (order == 1) {
-        if (eps == 0.f) launch_variant<1, true>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s);
-        else launch_variant<1, false>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s);
+        if (eps == 0.f) launch_variant<1, true>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s, gtab, ngroups, inst_root);
+        else launch_variant<1, false>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s, gtab, ngroups, inst_root);
     } else {
-        if (eps == 0.f) launch_variant<2, true>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s);
-        else launch_variant<2, false>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s);
+        if (eps == 0.f) launch_variant<2, true>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s, gtab, ngroups, inst_root);
+        else launch_variant<2, false>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s, gtab, ngroups, inst_root);
     }
 }
 

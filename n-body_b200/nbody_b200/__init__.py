@@ -115,6 +115,10 @@ SIGNATURES = {
     "nb_get_tree": (C.c_int, [_vp, C.POINTER(_i64), C.POINTER(_i32), _vp, _vp, _vp, _vp]),
     "nb_direct_device": (C.c_int, [_vp, _i64, _vp, _i64, _vp, _vp, _i32]),
     "nb_sort_codes_noalloc": (C.c_int, [_vp, _vp, _vp, _i64, _vp]),
+    "nb_set_instances": (C.c_int, [_vp, _i32, _vp, _vp, _vp, _vp]),
+    "nb_instance_count": (_i32, [_vp]),
+    "nb_get_instance_roots": (C.c_int, [_vp, _vp]),
+    "nb_enable_graphs": (C.c_int, [_vp, C.c_int]),
     "nb_host_alloc": (_vp, [C.c_size_t]),
     "nb_host_free": (None, [_vp]),
 }
@@ -262,6 +266,26 @@ class Solver:
     def set_bodies_device(self, n: int, d_pos_mass: int, d_vel: int | None = None):
         self._n = n
         self._check(lib().nb_set_bodies_device(self._ctx, n, d_pos_mass, d_vel))
+
+    def set_instances(self, sizes, bodies, velocities=None, thetas=None):
+        """Batched independent instances laid out back to back (nb_set_instances)."""
+        sizes = np.ascontiguousarray(sizes, np.int64)
+        pm = _bodies(bodies)
+        if int(sizes.sum()) != len(pm):
+            raise ValueError("sizes do not add up to the number of bodies")
+        vel = None if velocities is None else _bodies(velocities, "velocities")
+        th = None if thetas is None else np.ascontiguousarray(thetas, np.float32)
+        self._n = len(pm)
+        self._check(lib().nb_set_instances(self._ctx, len(sizes), _ptr(sizes), None if th is None else _ptr(th),
+                                           _ptr(pm), None if vel is None else _ptr(vel)))
+
+    def instance_roots(self) -> np.ndarray:
+        roots = np.zeros(max(int(lib().nb_instance_count(self._ctx)), 1), np.int32)
+        self._check(lib().nb_get_instance_roots(self._ctx, _ptr(roots)))
+        return roots
+
+    def enable_graphs(self, on: bool = True):
+        self._check(lib().nb_enable_graphs(self._ctx, int(on)))
 
     def body_count(self) -> int:
         return int(lib().nb_body_count(self._ctx))
