@@ -63,8 +63,11 @@ def parse():
     ap.add_argument("--n", type=int, default=N_BODIES)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["plummer-1m", "batched"], default="plummer-1m",
-                    help="plummer-1m: one N=2^20 instance (the headline); batched: 256 uneven instances")
+    ap.add_argument("--workload", choices=["plummer-1m", "batched", "serving"], default="plummer-1m",
+                    help="plummer-1m: one N=2^20 instance (the headline); batched: 256 uneven instances; "
+                         "serving: Poisson request stream into the continuous-batching server")
+    ap.add_argument("--duration", type=float, default=20.0, help="serving: seconds of arrivals per run")
+    ap.add_argument("--rate", type=float, default=40.0, help="serving: arrivals per second (open loop)")
     ap.add_argument("--instances", type=int, default=256)
     return ap.parse_args()
 
@@ -482,12 +485,113 @@ def run_batched(args):
         print(json.dumps(line), flush=True)
 
 
+def serving_pools(seed=45, n_max=1 << 21):
+    """Two shuffled body pools (Plummer, uniform ball) that requests take prefixes of: a prefix of
+    a shuffled sample is itself a sample of the distribution."""
+    from nbody_b200 import scenarios
+
+    rng = np.random.default_rng(seed)
+    pools = []
+    for kind, gen in (("plummer", scenarios.plummer), ("uniform", scenarios.uniform_ball)):
+        pm, vel = gen(n_max, seed=seed)
+        perm = rng.permutation(n_max)
+        pools.append((kind, pm[perm].copy(), vel[perm].copy()))
+    return pools
+
+
+def serve_run(nb, pools, rate, duration, rng, eps, steps_range=(10, 1000), n_range=(2048, 1 << 21),
+              budget=150 * 10 ** 9, drain=0.0):
+    """Open-loop Poisson arrivals for `duration` seconds (then `drain` more seconds of ticks).
+    Latency = completion time - arrival time, wall clock."""
+    arrivals = []
+    t = rng.exponential(1.0 / rate)
+    while t < duration:
+        kind, pm, vel = pools[rng.integers(0, 2)]
+        n = int(np.round(np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1])))))
+        steps = int(rng.integers(steps_range[0], steps_range[1] + 1))
+        theta = float(rng.uniform(0.4, 0.7))
+        arrivals.append((t, n, steps, theta, pm, vel))
+        t += rng.exponential(1.0 / rate)
+    sv = nb.Server(rule=nb.Gravity(1.0, eps), order=ORDER, max_leaf_size=LEAF, time_step=DT, hbm_budget_bytes=budget)
+    pending = {}  # id -> arrival time
+    latencies = []
+    t0 = time.perf_counter()
+    nxt = 0
+    while True:
+        now = time.perf_counter() - t0
+        if now > duration + drain:
+            break
+        while nxt < len(arrivals) and arrivals[nxt][0] <= now:
+            ta, n, steps, theta, pm, vel = arrivals[nxt]
+            rid = sv.submit(pm[:n], vel[:n], theta=theta, steps=steps)
+            pending[rid] = ta
+            nxt += 1
+        if sv.stats()["running"] == 0 and sv.stats()["queued"] == 0:
+            if nxt >= len(arrivals):
+                if drain > 0:
+                    break
+            time.sleep(0.001)
+            sv.tick()
+            continue
+        if sv.tick():
+            done_now = time.perf_counter() - t0
+            for rid in list(pending):
+                st, _ = sv.status(rid)
+                if st == nb.Server.DONE:
+                    latencies.append(done_now - pending.pop(rid))
+                    sv.take_result(rid, 1)
+    elapsed = time.perf_counter() - t0
+    st = sv.stats()
+    sv.close()
+    lat = np.array(latencies) if latencies else np.array([np.nan])
+    return {
+        "arrival_rate_per_s": rate, "duration_s": duration, "submitted": nxt, "completed": len(latencies),
+        "running_at_end": st["running"], "queued_at_end": st["queued"], "ticks": st["ticks"],
+        "relayouts": st["relayouts"], "body_steps": st["body_steps"],
+        "throughput_body_steps_per_s": st["body_steps"] / elapsed,
+        "latency_p50_s": float(np.nanpercentile(lat, 50)), "latency_p99_s": float(np.nanpercentile(lat, 99)),
+        "offered_body_steps_per_s": float(sum(a[1] * a[2] for a in arrivals) / duration),
+    }
+
+
+def run_serving(args):
+    import torch
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    import nbody_b200 as nb
+
+    eps = float(np.float32(BATCH_SOFTENING) * np.float32(BATCH_SOFTENING))
+    pools = serving_pools()
+    rng = np.random.default_rng(46 + rank)
+    overload = serve_run(nb, pools, args.rate, args.duration, rng, eps)
+    # calibrated run: arrival rate at 70 % of the measured capacity for the mean request size
+    mean_work = np.mean([np.exp(rng.uniform(np.log(2048), np.log(1 << 21))) for _ in range(20000)]) * 505.0
+    rate = max(0.7 * overload["throughput_body_steps_per_s"] / mean_work, 0.05)
+    calibrated = serve_run(nb, pools, rate, args.duration, rng, eps, drain=args.duration)
+    line = {
+        "metric": "serving: aggregate body-steps/s and request latency p50/p99 (Poisson arrivals)",
+        "value": overload["throughput_body_steps_per_s"], "unit": "body-steps/s", "n_gpus": world,
+        "steps": overload["ticks"], "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (Plummer or uniform ball, 50/50)",
+        "config": {"workload": "serving-poisson", "n_range": [2048, 1 << 21], "steps_range": [10, 1000],
+                   "theta_range": [0.4, 0.7], "softening": BATCH_SOFTENING, "hbm_budget_bytes": 150 * 10 ** 9,
+                   "order": ORDER, "leaf_size": LEAF},
+        "overload_run": overload,
+        "calibrated_run": calibrated,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "batched":
         run_batched(args)
+    elif args.workload == "serving":
+        run_serving(args)
     else:
         run_ours(args)
 

@@ -163,6 +163,35 @@ int nb_get_instance_roots(nb_ctx *ctx, int32_t *roots);
  * timing, when enabled, runs the steps uncaptured). */
 int nb_enable_graphs(nb_ctx *ctx, int enable);
 
+/* Serving: continuous batching of independent simulations on one device (no reference
+ * counterpart beyond Solver::step per simulation). A request is a body set with its own theta and
+ * step count. nb_server_tick retires finished requests (copying their final bodies out), admits
+ * queued ones in arrival order while their resident memory fits the budget, and advances every
+ * running request by one step in one batched force pass. Each request's result equals running it
+ * alone (bit-identical). */
+typedef struct nb_server nb_server;
+typedef struct nb_server_stats {
+    int64_t submitted, queued, running, completed;
+    int64_t body_steps;      /* body-steps advanced so far */
+    int64_t ticks, relayouts;
+    uint64_t resident_bytes; /* budget charge of the running requests */
+} nb_server_stats;
+int nb_server_create(const nb_config *cfg, uint64_t hbm_budget_bytes, nb_server **out);
+int nb_server_destroy(nb_server *sv);
+const char *nb_server_last_error(const nb_server *sv);
+/* The server's solver context (for nb_set_stream, nb_enable_timing, nb_get_counts). */
+void *nb_server_context(nb_server *sv);
+/* Queue a request (bodies copied; velocity may be NULL). Fails with NB_ERR_OUT_OF_MEMORY when
+ * the request alone exceeds the budget. */
+int nb_server_submit(nb_server *sv, int64_t n, const float *pos_mass, const float *velocity, float theta,
+                     int32_t steps, int64_t *request_id);
+int nb_server_tick(nb_server *sv, int32_t *completed_now);
+/* state: 0 queued, 1 running, 2 done. */
+int nb_server_status(nb_server *sv, int64_t request_id, int32_t *state, int32_t *steps_done);
+/* Final bodies of a done request in its caller order (then the request is forgotten). */
+int nb_server_take_result(nb_server *sv, int64_t request_id, float *pos_mass, float *velocity);
+int nb_server_get_stats(nb_server *sv, nb_server_stats *out);
+
 /* Direct sum on device pointers: accelerations of nt targets (4 floats each) from n bodies.
  * precision 32: FP32, acc 4 floats per target (NaiveSolver arithmetic).
  * precision 64: FP64 accumulation, acc 3 doubles per target (accuracy reference). */

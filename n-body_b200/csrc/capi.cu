@@ -13,6 +13,8 @@
 #include <array>
 #include <cstdio>
 #include <cstring>
+#include <deque>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -78,6 +80,8 @@ struct nb_ctx {
     // CUDA graph of two consecutive steps (bodies ping-pong between two buffers each step)
     bool use_graphs = false;
     cudaGraphExec_t graph2 = nullptr;
+    float4 *graph_pos = nullptr;   // the body buffer the captured pair starts from
+    int64_t steps_since_set = 0;   // plain or captured steps since the body set was replaced
 
     bool bbox_valid = false;  // bbox already holds the box of the current positions
     bool have_tree = false;
@@ -496,6 +500,7 @@ static int set_bodies_impl(nb_ctx *ctx, int64_t n, const void *pm, const void *v
     if (rc != NB_OK) return rc;
     free_batch(ctx);
     drop_graph(ctx);
+    ctx->steps_since_set = 0;
     ctx->n = n;
     const size_t bytes = (size_t) n * sizeof(float4);
     if (n > 0) {
@@ -615,20 +620,23 @@ static int one_step(nb_ctx *ctx) {
     mk.mark(kEnd);
     mk.commit();
     ctx->have_acc = true;
+    ctx->steps_since_set += 1;
     return NB_OK;
 }
 
 // Two steps captured once and replayed: after two steps the bodies are back in the same buffers,
 // so the graph's pointers stay valid. Timing marks are not captured.
-static int graph_steps(nb_ctx *ctx, int32_t pairs) {
+static int graph_pair(nb_ctx *ctx) {
     if (!ctx->graph2) {
-        // nb_step has run one plain step before the first capture, so the captured steps see the
-        // steady-state shape (bounding box from the previous drift, launch settings initialised)
+        // captured steps see the steady-state shape: the previous drift already reduced the box
+        // and every lazily initialised launch setting is in place
         cudaGraph_t g = nullptr;
+        ctx->graph_pos = ctx->pos;
         NB_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
         int rc = one_step(ctx);
         if (rc == NB_OK) rc = one_step(ctx);
         cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+        ctx->steps_since_set -= 2;  // recorded, not executed
         if (rc != NB_OK) {
             if (g) cudaGraphDestroy(g);
             return rc;
@@ -638,7 +646,9 @@ static int graph_steps(nb_ctx *ctx, int32_t pairs) {
         cudaGraphDestroy(g);
         NB_TRY(e, "instantiate graph");
     }
-    for (int32_t k = 0; k < pairs; ++k) NB_TRY(cudaGraphLaunch(ctx->graph2, ctx->stream), "launch graph");
+    NB_TRY(cudaGraphLaunch(ctx->graph2, ctx->stream), "launch graph");
+    ctx->steps_since_set += 2;
+    ctx->have_acc = true;
     return NB_OK;
 }
 
@@ -647,23 +657,19 @@ int nb_step(nb_ctx *ctx, int32_t steps) {
     if (rc != NB_OK) return rc;
     if (steps < 0) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "negative step count");
     int32_t k = 0;
-    if (ctx->use_graphs && !ctx->timing && ctx->n > 0) {
-        if (!ctx->graph2) {  // the first step runs uncaptured (bounding box of the initial state)
-            if (steps == 0) return NB_OK;
-            rc = one_step(ctx);
+    while (k < steps) {
+        const bool pair = ctx->use_graphs && !ctx->timing && ctx->n > 0 && steps - k >= 2 && ctx->steps_since_set > 0;
+        // The captured pair reads and writes the buffers it was recorded with; each plain force
+        // pass swaps the ping-pong buffers, so replay only when the bodies sit where it expects.
+        if (pair && (!ctx->graph2 || ctx->pos == ctx->graph_pos)) {
+            rc = graph_pair(ctx);
             if (rc != NB_OK) return rc;
-            k = 1;
+            k += 2;
+            continue;
         }
-        const int32_t pairs = (steps - k) / 2;
-        if (pairs > 0) {
-            rc = graph_steps(ctx, pairs);
-            if (rc != NB_OK) return rc;
-            k += 2 * pairs;
-        }
-    }
-    for (; k < steps; ++k) {
         rc = one_step(ctx);
         if (rc != NB_OK) return rc;
+        k += 1;
     }
     return NB_OK;
 }
@@ -779,23 +785,15 @@ int nb_direct_device(nb_ctx *ctx, int64_t n, const void *d_bodies, int64_t nt, c
     return check_cuda(ctx, cudaGetLastError(), "direct sum");
 }
 
-int nb_set_instances(nb_ctx *ctx, int32_t count, const int64_t *sizes, const float *thetas, const float *pos_mass,
-                     const float *velocity) {
-    int rc = begin(ctx);
-    if (rc != NB_OK) return rc;
-    if (count < 1 || count > 65535 || !sizes) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "1..65535 instances required");
-    int64_t n = 0;
-    for (int32_t k = 0; k < count; ++k) {
-        if (sizes[k] < 1) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "every instance needs at least one body");
-        n += sizes[k];
-    }
-    if (n > kMaxBodies) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "body count out of range");
-    if (thetas)
-        for (int32_t k = 0; k < count; ++k)
-            if (!(thetas[k] >= 0.f)) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "theta must be >= 0");
-    rc = set_bodies_impl(ctx, n, pos_mass, velocity, cudaMemcpyHostToDevice);
-    if (rc != NB_OK) return rc;
-    // host-side tables (sizes are fixed for the life of the batch)
+// Builds the batch tables for `count` instances whose bodies already sit back to back in the
+// context's state arrays (ctx->n bodies in total).
+static int build_batch_tables(nb_ctx *ctx, int32_t count, const int64_t *sizes, const float *thetas) {
+    const int64_t n = ctx->n;
+    dev_free(ctx->inst_of); dev_free(ctx->inst_root); dev_free(ctx->inst_theta2); dev_free(ctx->inst_box);
+    dev_free(ctx->inst_range); dev_free(ctx->groups); dev_free(ctx->ikeys); dev_free(ctx->ikeys2);
+    dev_free(ctx->ivals); dev_free(ctx->ivals2); dev_free(ctx->inst_offsets); dev_free(ctx->inst_lookback);
+    dev_free(ctx->inst_tiles);
+    drop_graph(ctx);
     std::vector<int> inst_of((size_t) n);
     std::vector<int2> range((size_t) count);
     std::vector<float> theta2((size_t) count);
@@ -852,7 +850,35 @@ int nb_set_instances(nb_ctx *ctx, int32_t count, const int64_t *sizes, const flo
     ctx->num_inst = count;
     ctx->ngroups = (int64_t) groups.size();
     ctx->inst_passes = passes;
-    return check_cuda(ctx, cudaStreamSynchronize(s), "set instances");
+    // host vectors are released on return: wait for the copies out of them
+    return check_cuda(ctx, cudaStreamSynchronize(s), "batch tables");
+}
+
+static int check_instances(nb_ctx *ctx, int32_t count, const int64_t *sizes, const float *thetas, int64_t *total) {
+    if (count < 1 || count > 65535 || !sizes) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "1..65535 instances required");
+    int64_t n = 0;
+    for (int32_t k = 0; k < count; ++k) {
+        if (sizes[k] < 1) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "every instance needs at least one body");
+        n += sizes[k];
+    }
+    if (n > kMaxBodies) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "body count out of range");
+    if (thetas)
+        for (int32_t k = 0; k < count; ++k)
+            if (!(thetas[k] >= 0.f)) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "theta must be >= 0");
+    *total = n;
+    return NB_OK;
+}
+
+int nb_set_instances(nb_ctx *ctx, int32_t count, const int64_t *sizes, const float *thetas, const float *pos_mass,
+                     const float *velocity) {
+    int rc = begin(ctx);
+    if (rc != NB_OK) return rc;
+    int64_t n = 0;
+    rc = check_instances(ctx, count, sizes, thetas, &n);
+    if (rc != NB_OK) return rc;
+    rc = set_bodies_impl(ctx, n, pos_mass, velocity, cudaMemcpyHostToDevice);
+    if (rc != NB_OK) return rc;
+    return build_batch_tables(ctx, count, sizes, thetas);
 }
 
 int32_t nb_instance_count(const nb_ctx *ctx) { return ctx ? (ctx->num_inst > 0 ? ctx->num_inst : 1) : -1; }
@@ -885,6 +911,313 @@ void *nb_host_alloc(size_t bytes) {
 
 void nb_host_free(void *p) {
     if (p) cudaFreeHost(p);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// Serving: continuous batching of independent simulations on one device.
+//
+// Requests (a body set, theta and a step count) queue on the host until the resident-memory
+// budget admits them. Every tick retires finished requests (their final bodies are copied out),
+// admits queued ones in arrival order while they fit, re-lays out the device state when the set
+// changed (survivors move device-to-device, newcomers are copied in once), and advances every
+// running request by one step in ONE batched force pass (nb_set_instances' pipeline). Each
+// request keeps its bodies and its per-step tree on the device from admission to completion.
+// A request's arithmetic is exactly that of running it alone, so its result does not depend on
+// what else is in the batch.
+// ---------------------------------------------------------------------------------------------
+
+namespace {
+
+// Device bytes one resident body costs the context (state, sort, tree and batch buffers, with
+// the growth headroom of a re-layout); admission charges this per body against the budget.
+constexpr uint64_t kResidentBytesPerBody = 544;
+
+struct ServedRequest {
+    int64_t id = 0;
+    int64_t n = 0;
+    float theta = 0.f;
+    int32_t steps = 0, done = 0;
+    int32_t state = 0;   // 0 queued, 1 running, 2 done
+    int64_t start = -1;  // first body position in the batch while resident
+    std::vector<float> pm, vel;  // input until admitted, result once done
+};
+
+}  // namespace
+
+struct nb_server {
+    nb_ctx *ctx = nullptr;
+    uint64_t budget = 0;
+    std::string error;
+    int64_t next_id = 1;
+    std::deque<ServedRequest *> queue;
+    std::vector<ServedRequest *> active;
+    std::map<int64_t, ServedRequest *> all;
+    float4 *tpos = nullptr, *tvel = nullptr;
+    uint32_t *tid = nullptr;
+    int64_t tcap = 0;
+    nb_server_stats stats{};
+};
+
+static int server_fail(nb_server *sv, int rc) {
+    if (sv && sv->ctx) sv->error = sv->ctx->error;
+    return rc;
+}
+
+static int server_relayout(nb_server *sv) {
+    nb_ctx *ctx = sv->ctx;
+    cudaStream_t s = ctx->stream;
+    int64_t total = 0;
+    for (auto *r: sv->active) total += r->n;
+    if (total > sv->tcap) {
+        dev_free(sv->tpos); dev_free(sv->tvel); dev_free(sv->tid);
+        sv->tcap = 0;
+        if (dev_alloc(&sv->tpos, (size_t) total) != cudaSuccess || dev_alloc(&sv->tvel, (size_t) total) != cudaSuccess ||
+            dev_alloc(&sv->tid, (size_t) total) != cudaSuccess) {
+            sv->error = "out of device memory for the re-layout";
+            return NB_ERR_OUT_OF_MEMORY;
+        }
+        sv->tcap = total;
+    }
+    int64_t off = 0;
+    for (auto *r: sv->active) {
+        const size_t bytes = (size_t) r->n * sizeof(float4);
+        if (r->start >= 0) {  // resident: move device-to-device, rebase the caller indices
+            if (cudaMemcpyAsync(sv->tpos + off, ctx->pos + r->start, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+                cudaMemcpyAsync(sv->tvel + off, ctx->vel + r->start, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+                cudaMemcpyAsync(sv->tid + off, ctx->id + r->start, (size_t) r->n * 4, cudaMemcpyDeviceToDevice, s) !=
+                    cudaSuccess) {
+                sv->error = "re-layout copy failed";
+                return NB_ERR_CUDA;
+            }
+            launch_add_offset(sv->tid + off, r->n, off - r->start, s);
+        } else {  // newcomer: one copy in
+            if (cudaMemcpyAsync(sv->tpos + off, r->pm.data(), bytes, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+                cudaMemcpyAsync(sv->tvel + off, r->vel.data(), bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+                sv->error = "copy-in failed";
+                return NB_ERR_CUDA;
+            }
+            launch_iota(sv->tid + off, r->n, s, (uint32_t) off);
+        }
+        r->start = off;
+        off += r->n;
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+        sv->error = "re-layout failed";
+        return NB_ERR_CUDA;
+    }
+    for (auto *r: sv->active) {  // host input copies are no longer needed
+        std::vector<float>().swap(r->pm);
+        std::vector<float>().swap(r->vel);
+    }
+    int rc = ensure_capacity(ctx, total);
+    if (rc != NB_OK) return server_fail(sv, rc);
+    free_batch(ctx);
+    drop_graph(ctx);
+    ctx->n = total;
+    ctx->steps_since_set = 0;
+    ctx->bbox_valid = false;
+    ctx->have_tree = false;
+    ctx->have_acc = false;
+    sv->stats.relayouts += 1;
+    if (total == 0) return NB_OK;
+    const size_t bytes = (size_t) total * sizeof(float4);
+    if (cudaMemcpyAsync(ctx->pos, sv->tpos, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(ctx->vel, sv->tvel, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(ctx->id, sv->tid, (size_t) total * 4, cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+        sv->error = "re-layout copy failed";
+        return NB_ERR_CUDA;
+    }
+    std::vector<int64_t> sizes;
+    std::vector<float> thetas;
+    for (auto *r: sv->active) {
+        sizes.push_back(r->n);
+        thetas.push_back(r->theta);
+    }
+    rc = build_batch_tables(ctx, (int32_t) sizes.size(), sizes.data(), thetas.data());
+    return rc == NB_OK ? NB_OK : server_fail(sv, rc);
+}
+
+// Copies a running request's bodies out, in its caller order.
+static int server_collect(nb_server *sv, ServedRequest *r) {
+    nb_ctx *ctx = sv->ctx;
+    std::vector<float4> pos((size_t) r->n), vel((size_t) r->n);
+    std::vector<uint32_t> ids((size_t) r->n);
+    cudaStream_t s = ctx->stream;
+    if (cudaMemcpyAsync(pos.data(), ctx->pos + r->start, (size_t) r->n * 16, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaMemcpyAsync(vel.data(), ctx->vel + r->start, (size_t) r->n * 16, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaMemcpyAsync(ids.data(), ctx->id + r->start, (size_t) r->n * 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        sv->error = "copy-out failed";
+        return NB_ERR_CUDA;
+    }
+    r->pm.assign((size_t) r->n * 4, 0.f);
+    r->vel.assign((size_t) r->n * 4, 0.f);
+    for (int64_t k = 0; k < r->n; ++k) {
+        const int64_t local = (int64_t) ids[k] - r->start;
+        if (local < 0 || local >= r->n) {
+            sv->error = "corrupt body ids in a served request";
+            return NB_ERR_DEVICE_CHECK;
+        }
+        std::memcpy(&r->pm[4 * local], &pos[k], 16);
+        std::memcpy(&r->vel[4 * local], &vel[k], 16);
+    }
+    return NB_OK;
+}
+
+extern "C" {
+
+int nb_server_create(const nb_config *cfg, uint64_t hbm_budget_bytes, nb_server **out) {
+    if (!out) return NB_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    nb_ctx *ctx = nullptr;
+    int rc = nb_create(cfg, &ctx);
+    if (rc != NB_OK) return rc;
+    if (cfg->solver != NB_SOLVER_LINEAR_BVH) {
+        nb_destroy(ctx);
+        return NB_ERR_UNSUPPORTED;
+    }
+    nb_server *sv = new nb_server();
+    sv->ctx = ctx;
+    sv->budget = hbm_budget_bytes;
+    *out = sv;
+    return NB_OK;
+}
+
+int nb_server_destroy(nb_server *sv) {
+    if (!sv) return NB_OK;
+    for (auto &kv: sv->all) delete kv.second;
+    cudaSetDevice(sv->ctx->cfg.device);
+    dev_free(sv->tpos); dev_free(sv->tvel); dev_free(sv->tid);
+    nb_destroy(sv->ctx);
+    delete sv;
+    return NB_OK;
+}
+
+const char *nb_server_last_error(const nb_server *sv) { return sv ? sv->error.c_str() : "no server"; }
+
+void *nb_server_context(nb_server *sv) { return sv ? (void *) sv->ctx : nullptr; }
+
+int nb_server_submit(nb_server *sv, int64_t n, const float *pos_mass, const float *velocity, float theta,
+                     int32_t steps, int64_t *request_id) {
+    if (!sv || !request_id) return NB_ERR_INVALID_ARGUMENT;
+    if (n < 1 || !pos_mass || steps < 0 || !(theta >= 0.f)) {
+        sv->error = "a request needs at least one body, theta >= 0 and steps >= 0";
+        return NB_ERR_INVALID_ARGUMENT;
+    }
+    if ((uint64_t) n * kResidentBytesPerBody > sv->budget) {
+        sv->error = "request larger than the whole memory budget";
+        return NB_ERR_OUT_OF_MEMORY;
+    }
+    auto *r = new ServedRequest();
+    r->id = sv->next_id++;
+    r->n = n;
+    r->theta = theta;
+    r->steps = steps;
+    r->pm.assign(pos_mass, pos_mass + 4 * n);
+    if (velocity) r->vel.assign(velocity, velocity + 4 * n);
+    else r->vel.assign((size_t) 4 * n, 0.f);
+    sv->all[r->id] = r;
+    sv->queue.push_back(r);
+    sv->stats.submitted += 1;
+    *request_id = r->id;
+    return NB_OK;
+}
+
+int nb_server_tick(nb_server *sv, int32_t *completed_now) {
+    if (!sv) return NB_ERR_INVALID_ARGUMENT;
+    nb_ctx *ctx = sv->ctx;
+    if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return NB_ERR_CUDA;
+    int32_t completed = 0;
+    bool changed = false;
+    // 1. retire requests whose steps are done
+    std::vector<ServedRequest *> keep;
+    for (auto *r: sv->active) {
+        if (r->done >= r->steps) {
+            int rc = server_collect(sv, r);
+            if (rc != NB_OK) return rc;
+            r->state = 2;
+            r->start = -1;
+            ++completed;
+            changed = true;
+        } else {
+            keep.push_back(r);
+        }
+    }
+    sv->active.swap(keep);
+    // 2. admit queued requests in arrival order while they fit the budget
+    uint64_t resident = 0;
+    for (auto *r: sv->active) resident += (uint64_t) r->n * kResidentBytesPerBody;
+    while (!sv->queue.empty()) {
+        ServedRequest *r = sv->queue.front();
+        const uint64_t need = (uint64_t) r->n * kResidentBytesPerBody;
+        if (resident + need > sv->budget) break;
+        sv->queue.pop_front();
+        if (r->steps == 0) {  // nothing to run: the result is the input
+            r->state = 2;
+            ++completed;
+            continue;
+        }
+        r->state = 1;
+        r->start = -1;
+        sv->active.push_back(r);
+        resident += need;
+        changed = true;
+    }
+    if (changed) {
+        int rc = server_relayout(sv);
+        if (rc != NB_OK) return rc;
+    }
+    // 3. one batched step for every running request
+    if (!sv->active.empty()) {
+        int rc = nb_step(ctx, 1);
+        if (rc != NB_OK) return server_fail(sv, rc);
+        for (auto *r: sv->active) {
+            r->done += 1;
+            sv->stats.body_steps += r->n;
+        }
+    }
+    sv->stats.ticks += 1;
+    sv->stats.completed += completed;
+    sv->stats.queued = (int64_t) sv->queue.size();
+    sv->stats.running = (int64_t) sv->active.size();
+    sv->stats.resident_bytes = resident;
+    if (completed_now) *completed_now = completed;
+    return NB_OK;
+}
+
+int nb_server_status(nb_server *sv, int64_t request_id, int32_t *state, int32_t *steps_done) {
+    if (!sv) return NB_ERR_INVALID_ARGUMENT;
+    auto it = sv->all.find(request_id);
+    if (it == sv->all.end()) {
+        sv->error = "unknown request";
+        return NB_ERR_INVALID_ARGUMENT;
+    }
+    if (state) *state = it->second->state;
+    if (steps_done) *steps_done = it->second->done;
+    return NB_OK;
+}
+
+int nb_server_take_result(nb_server *sv, int64_t request_id, float *pos_mass, float *velocity) {
+    if (!sv) return NB_ERR_INVALID_ARGUMENT;
+    auto it = sv->all.find(request_id);
+    if (it == sv->all.end() || it->second->state != 2) {
+        sv->error = "request unknown or not done";
+        return NB_ERR_INVALID_ARGUMENT;
+    }
+    ServedRequest *r = it->second;
+    if (pos_mass) std::memcpy(pos_mass, r->pm.data(), r->pm.size() * sizeof(float));
+    if (velocity) std::memcpy(velocity, r->vel.data(), r->vel.size() * sizeof(float));
+    sv->all.erase(it);
+    delete r;
+    return NB_OK;
+}
+
+int nb_server_get_stats(nb_server *sv, nb_server_stats *out) {
+    if (!sv || !out) return NB_ERR_INVALID_ARGUMENT;
+    *out = sv->stats;
+    return NB_OK;
 }
 
 }  // extern "C"

@@ -45,9 +45,14 @@ __global__ void __launch_bounds__(kThreads) scatter_by_id_kernel(const uint32_t 
     if (d < (uint64_t) n) dst[d] = src[k];
 }
 
-__global__ void __launch_bounds__(kThreads) iota_kernel(uint32_t *__restrict__ id, int64_t n) {
+__global__ void __launch_bounds__(kThreads) iota_kernel(uint32_t *__restrict__ id, int64_t n, uint32_t first) {
     const int64_t k = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < n) id[k] = (uint32_t) k;
+    if (k < n) id[k] = first + (uint32_t) k;
+}
+
+__global__ void __launch_bounds__(kThreads) add_offset_kernel(uint32_t *__restrict__ id, int64_t n, int64_t delta) {
+    const int64_t k = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) id[k] = (uint32_t) ((int64_t) id[k] + delta);
 }
 
 __global__ void __launch_bounds__(kThreads) kick_drift_kernel(float4 *__restrict__ pos, float4 *__restrict__ vel,
@@ -110,9 +115,14 @@ void launch_scatter_by_id(const uint32_t *id, int64_t n, const float4 *src, floa
     scatter_by_id_kernel<<<blocks_for(n), kThreads, 0, s>>>(id, n, src, dst);
 }
 
-void launch_iota(uint32_t *id, int64_t n, cudaStream_t s) {
+void launch_iota(uint32_t *id, int64_t n, cudaStream_t s, uint32_t first) {
     if (n <= 0) return;
-    iota_kernel<<<blocks_for(n), kThreads, 0, s>>>(id, n);
+    iota_kernel<<<blocks_for(n), kThreads, 0, s>>>(id, n, first);
+}
+
+void launch_add_offset(uint32_t *id, int64_t n, int64_t delta, cudaStream_t s) {
+    if (n <= 0 || delta == 0) return;
+    add_offset_kernel<<<blocks_for(n), kThreads, 0, s>>>(id, n, delta);
 }
 
 void launch_kick_drift(float4 *pos, float4 *vel, const float4 *acc, int64_t n, float dt, BBoxAccum *next_bbox,

@@ -196,7 +196,8 @@ void launch_gather_state(const uint32_t *perm, int64_t n, const float4 *pos, con
 void launch_scatter_by_id(const uint32_t *id, int64_t n, const float4 *src, float4 *dst, cudaStream_t s);
 void launch_kick_drift(float4 *pos, float4 *vel, const float4 *acc, int64_t n, float dt, BBoxAccum *next_bbox,
                        cudaStream_t s);
-void launch_iota(uint32_t *id, int64_t n, cudaStream_t s);
+void launch_iota(uint32_t *id, int64_t n, cudaStream_t s, uint32_t first = 0);
+void launch_add_offset(uint32_t *id, int64_t n, int64_t delta, cudaStream_t s);
 
 // batch.cu
 void launch_seg_bbox(const float4 *pos, const int2 *inst_range, int num_inst, float *inst_box, cudaStream_t s);

@@ -67,6 +67,22 @@ class Counts(C.Structure):
     ]
 
 
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_int64),
+        ("queued", C.c_int64),
+        ("running", C.c_int64),
+        ("completed", C.c_int64),
+        ("body_steps", C.c_int64),
+        ("ticks", C.c_int64),
+        ("relayouts", C.c_int64),
+        ("resident_bytes", C.c_uint64),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class PhaseTimes(C.Structure):
     _fields_ = [
         ("bbox_ms", C.c_double),
@@ -119,6 +135,15 @@ SIGNATURES = {
     "nb_instance_count": (_i32, [_vp]),
     "nb_get_instance_roots": (C.c_int, [_vp, _vp]),
     "nb_enable_graphs": (C.c_int, [_vp, C.c_int]),
+    "nb_server_create": (C.c_int, [C.POINTER(Config), C.c_uint64, C.POINTER(_vp)]),
+    "nb_server_destroy": (C.c_int, [_vp]),
+    "nb_server_last_error": (C.c_char_p, [_vp]),
+    "nb_server_context": (_vp, [_vp]),
+    "nb_server_submit": (C.c_int, [_vp, _i64, _vp, _vp, C.c_float, _i32, C.POINTER(_i64)]),
+    "nb_server_tick": (C.c_int, [_vp, C.POINTER(_i32)]),
+    "nb_server_status": (C.c_int, [_vp, _i64, C.POINTER(_i32), C.POINTER(_i32)]),
+    "nb_server_take_result": (C.c_int, [_vp, _i64, _vp, _vp]),
+    "nb_server_get_stats": (C.c_int, [_vp, C.POINTER(ServerStats)]),
     "nb_host_alloc": (_vp, [C.c_size_t]),
     "nb_host_free": (None, [_vp]),
 }
@@ -370,6 +395,81 @@ class NaiveSolver(Solver):
     """NaiveSolver (NaiveSolver.h:12-53): FP32 direct sum over all pairs."""
 
     _solver_kind = SOLVER_NAIVE
+
+
+class Server:
+    """Continuous-batching server of independent simulations (nb_server_*)."""
+
+    QUEUED, RUNNING, DONE = 0, 1, 2
+
+    def __init__(self, rule: Gravity | None = None, order: int = 2, max_leaf_size: int = 16, time_step: float = 1e-3,
+                 hbm_budget_bytes: int = 150 * 10 ** 9, device: int = 0):
+        rule = rule or Gravity()
+        cfg = default_config()
+        cfg.order = order
+        cfg.G = rule.G
+        cfg.epsilon = rule.epsilon
+        cfg.max_leaf_size = max_leaf_size
+        cfg.time_step = time_step
+        cfg.device = device
+        h = C.c_void_p()
+        rc = lib().nb_server_create(C.byref(cfg), hbm_budget_bytes, C.byref(h))
+        if rc != NB_OK:
+            raise NBodyError(rc, "nb_server_create failed (no usable sm_100 GPU?)")
+        self._h = h
+
+    def _check(self, rc):
+        if rc != NB_OK:
+            raise NBodyError(rc, lib().nb_server_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            lib().nb_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def context(self):
+        return lib().nb_server_context(self._h)
+
+    def submit(self, bodies, velocities=None, theta: float = 0.5, steps: int = 1) -> int:
+        pm = _bodies(bodies)
+        vel = None if velocities is None else _bodies(velocities, "velocities")
+        rid = C.c_int64()
+        self._check(lib().nb_server_submit(self._h, len(pm), _ptr(pm), None if vel is None else _ptr(vel),
+                                           float(theta), int(steps), C.byref(rid)))
+        return rid.value
+
+    def tick(self) -> int:
+        done = C.c_int32()
+        self._check(lib().nb_server_tick(self._h, C.byref(done)))
+        return done.value
+
+    def status(self, rid: int):
+        st, steps = C.c_int32(), C.c_int32()
+        self._check(lib().nb_server_status(self._h, rid, C.byref(st), C.byref(steps)))
+        return st.value, steps.value
+
+    def take_result(self, rid: int, n: int):
+        pm = np.zeros((n, 4), np.float32)
+        vel = np.zeros((n, 4), np.float32)
+        self._check(lib().nb_server_take_result(self._h, rid, _ptr(pm), _ptr(vel)))
+        return pm, vel
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        self._check(lib().nb_server_get_stats(self._h, C.byref(s)))
+        return s.as_dict()
 
 
 def decode_records(records: np.ndarray, order: int) -> dict:
