@@ -513,7 +513,7 @@ def serve_run(nb, pools, rate, duration, rng, eps, steps_range=(10, 1000), n_ran
         arrivals.append((t, n, steps, theta, pm, vel))
         t += rng.exponential(1.0 / rate)
     sv = nb.Server(rule=nb.Gravity(1.0, eps), order=ORDER, max_leaf_size=LEAF, time_step=DT, hbm_budget_bytes=budget)
-    pending = {}  # id -> arrival time
+    pending = {}  # id -> (arrival time, bodies)
     latencies = []
     t0 = time.perf_counter()
     nxt = 0
@@ -524,22 +524,21 @@ def serve_run(nb, pools, rate, duration, rng, eps, steps_range=(10, 1000), n_ran
         while nxt < len(arrivals) and arrivals[nxt][0] <= now:
             ta, n, steps, theta, pm, vel = arrivals[nxt]
             rid = sv.submit(pm[:n], vel[:n], theta=theta, steps=steps)
-            pending[rid] = ta
+            pending[rid] = (ta, n)
             nxt += 1
-        if sv.stats()["running"] == 0 and sv.stats()["queued"] == 0:
+        st = sv.stats()
+        if st["running"] == 0 and st["queued"] == 0:
             if nxt >= len(arrivals):
-                if drain > 0:
-                    break
-            time.sleep(0.001)
-            sv.tick()
+                break  # everything submitted has completed
+            time.sleep(0.0005)
             continue
         if sv.tick():
             done_now = time.perf_counter() - t0
             for rid in list(pending):
-                st, _ = sv.status(rid)
-                if st == nb.Server.DONE:
-                    latencies.append(done_now - pending.pop(rid))
-                    sv.take_result(rid, 1)
+                if sv.status(rid)[0] == nb.Server.DONE:
+                    ta, n = pending.pop(rid)
+                    latencies.append(done_now - ta)
+                    sv.take_result(rid, n)
     elapsed = time.perf_counter() - t0
     st = sv.stats()
     sv.close()
