@@ -1216,6 +1216,8 @@ int nb_server_take_result(nb_server *sv, int64_t request_id, float *pos_mass, fl
 
 int nb_server_get_stats(nb_server *sv, nb_server_stats *out) {
     if (!sv || !out) return NB_ERR_INVALID_ARGUMENT;
+    sv->stats.queued = (int64_t) sv->queue.size();
+    sv->stats.running = (int64_t) sv->active.size();
     *out = sv->stats;
     return NB_OK;
 }
