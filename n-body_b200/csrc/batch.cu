@@ -113,7 +113,27 @@ __global__ void __launch_bounds__(kThreads) compose_kernel(const uint32_t *__res
 
 unsigned blocks_for(int64_t n) { return (unsigned) ((n + kThreads - 1) / kThreads); }
 
+// One block per instance: the instance id of each of its body positions, and its 32-target
+// traversal groups (first target, count, instance) starting at group_first[k].
+__global__ void __launch_bounds__(kThreads) fill_tables_kernel(const int2 *__restrict__ inst_range,
+                                                               const int *__restrict__ group_first,
+                                                               int *__restrict__ inst_of, int4 *__restrict__ groups) {
+    const int k = blockIdx.x;
+    const int2 r = inst_range[k];
+    for (int i = r.x + threadIdx.x; i <= r.y; i += blockDim.x) inst_of[i] = k;
+    const int n = r.y - r.x + 1;
+    const int g0 = group_first[k];
+    for (int j = threadIdx.x; j * 32 < n; j += blockDim.x)
+        groups[g0 + j] = make_int4(r.x + 32 * j, min(32, n - 32 * j), k, 0);
+}
+
 }  // namespace
+
+void launch_fill_tables(const int2 *inst_range, const int *group_first, int num_inst, int *inst_of, int4 *groups,
+                        cudaStream_t s) {
+    if (num_inst <= 0) return;
+    fill_tables_kernel<<<num_inst, kThreads, 0, s>>>(inst_range, group_first, inst_of, groups);
+}
 
 void launch_seg_bbox(const float4 *pos, const int2 *inst_range, int num_inst, float *inst_box, cudaStream_t s) {
     if (num_inst <= 0) return;

@@ -75,6 +75,8 @@ struct nb_ctx {
     uint32_t *ivals = nullptr, *ivals2 = nullptr;
     uint32_t *inst_offsets = nullptr, *inst_lookback = nullptr, *inst_tiles = nullptr;
     int inst_passes = 0;
+    int64_t batch_body_cap = 0, batch_inst_cap = 0, batch_group_cap = 0;  // grow-only batch buffers
+    int *group_first = nullptr;
     const uint64_t *sorted_codes = nullptr;  // buffer holding the last pass's sorted codes
 
     // CUDA graph of two consecutive steps (bodies ping-pong between two buffers each step)
@@ -147,7 +149,8 @@ void free_batch(nb_ctx *ctx) {
     dev_free(ctx->inst_of); dev_free(ctx->inst_root); dev_free(ctx->inst_theta2); dev_free(ctx->inst_box);
     dev_free(ctx->inst_range); dev_free(ctx->groups); dev_free(ctx->ikeys); dev_free(ctx->ikeys2);
     dev_free(ctx->ivals); dev_free(ctx->ivals2); dev_free(ctx->inst_offsets); dev_free(ctx->inst_lookback);
-    dev_free(ctx->inst_tiles);
+    dev_free(ctx->inst_tiles); dev_free(ctx->group_first);
+    ctx->batch_body_cap = ctx->batch_inst_cap = ctx->batch_group_cap = 0;
     ctx->num_inst = 0;
     ctx->ngroups = 0;
     ctx->inst_start.clear();
@@ -789,27 +792,21 @@ int nb_direct_device(nb_ctx *ctx, int64_t n, const void *d_bodies, int64_t nt, c
 // context's state arrays (ctx->n bodies in total).
 static int build_batch_tables(nb_ctx *ctx, int32_t count, const int64_t *sizes, const float *thetas) {
     const int64_t n = ctx->n;
-    dev_free(ctx->inst_of); dev_free(ctx->inst_root); dev_free(ctx->inst_theta2); dev_free(ctx->inst_box);
-    dev_free(ctx->inst_range); dev_free(ctx->groups); dev_free(ctx->ikeys); dev_free(ctx->ikeys2);
-    dev_free(ctx->ivals); dev_free(ctx->ivals2); dev_free(ctx->inst_offsets); dev_free(ctx->inst_lookback);
-    dev_free(ctx->inst_tiles);
     drop_graph(ctx);
-    std::vector<int> inst_of((size_t) n);
     std::vector<int2> range((size_t) count);
+    std::vector<int> group_first((size_t) count);
     std::vector<float> theta2((size_t) count);
-    std::vector<int4> groups;
     std::vector<uint32_t> offsets(8 * 256 + 8, 0), hist(2 * 256, 0);
     ctx->inst_start.resize(count);
     ctx->inst_size.assign(sizes, sizes + count);
-    int64_t start = 0;
+    int64_t start = 0, ngroups = 0;
     for (int32_t k = 0; k < count; ++k) {
         ctx->inst_start[k] = start;
-        for (int64_t i = 0; i < sizes[k]; ++i) inst_of[start + i] = k;
         range[k] = make_int2((int) start, (int) (start + sizes[k] - 1));
+        group_first[k] = (int) ngroups;
+        ngroups += (sizes[k] + 31) / 32;
         const float th = thetas ? thetas[k] : ctx->cfg.theta;
         theta2[k] = th * th;  // the reference compares against theta * theta in float
-        for (int64_t g = 0; g < sizes[k]; g += 32)
-            groups.push_back(make_int4((int) (start + g), (int) std::min<int64_t>(32, sizes[k] - g), k, 0));
         hist[k & 255] += (uint32_t) sizes[k];
         hist[256 + (k >> 8)] += (uint32_t) sizes[k];
         start += sizes[k];
@@ -826,29 +823,51 @@ static int build_batch_tables(nb_ctx *ctx, int32_t count, const int64_t *sizes, 
         offsets[8 * 256 + p] = trivial ? 1u : 0u;
     }
     const int64_t tiles = sort_tiles(n);
-    NB_TRY(dev_alloc(&ctx->inst_of, (size_t) n), "alloc batch");
-    NB_TRY(dev_alloc(&ctx->inst_root, (size_t) count), "alloc batch");
-    NB_TRY(dev_alloc(&ctx->inst_theta2, (size_t) count), "alloc batch");
-    NB_TRY(dev_alloc(&ctx->inst_box, (size_t) count * 6), "alloc batch");
-    NB_TRY(dev_alloc(&ctx->inst_range, (size_t) count), "alloc batch");
-    NB_TRY(dev_alloc(&ctx->groups, groups.size()), "alloc batch");
-    NB_TRY(dev_alloc(&ctx->ikeys, (size_t) n), "alloc batch");
-    NB_TRY(dev_alloc(&ctx->ikeys2, (size_t) n), "alloc batch");
-    NB_TRY(dev_alloc(&ctx->ivals, (size_t) n), "alloc batch");
-    NB_TRY(dev_alloc(&ctx->ivals2, (size_t) n), "alloc batch");
-    NB_TRY(dev_alloc(&ctx->inst_offsets, offsets.size()), "alloc batch");
-    NB_TRY(dev_alloc(&ctx->inst_lookback, (size_t) 2 * tiles * 256), "alloc batch");
-    NB_TRY(dev_alloc(&ctx->inst_tiles, 8), "alloc batch");
+    if (n > ctx->batch_body_cap) {  // per-body buffers grow only
+        dev_free(ctx->inst_of); dev_free(ctx->ikeys); dev_free(ctx->ikeys2); dev_free(ctx->ivals);
+        dev_free(ctx->ivals2); dev_free(ctx->inst_lookback);
+        ctx->batch_body_cap = 0;
+        const int64_t cap = std::max<int64_t>(n, 1);
+        NB_TRY(dev_alloc(&ctx->inst_of, (size_t) cap), "alloc batch");
+        NB_TRY(dev_alloc(&ctx->ikeys, (size_t) cap), "alloc batch");
+        NB_TRY(dev_alloc(&ctx->ikeys2, (size_t) cap), "alloc batch");
+        NB_TRY(dev_alloc(&ctx->ivals, (size_t) cap), "alloc batch");
+        NB_TRY(dev_alloc(&ctx->ivals2, (size_t) cap), "alloc batch");
+        NB_TRY(dev_alloc(&ctx->inst_lookback, (size_t) 2 * sort_tiles(cap) * 256), "alloc batch");
+        ctx->batch_body_cap = cap;
+    }
+    if (count > ctx->batch_inst_cap) {
+        dev_free(ctx->inst_root); dev_free(ctx->inst_theta2); dev_free(ctx->inst_box); dev_free(ctx->inst_range);
+        dev_free(ctx->group_first);
+        ctx->batch_inst_cap = 0;
+        NB_TRY(dev_alloc(&ctx->inst_root, (size_t) count), "alloc batch");
+        NB_TRY(dev_alloc(&ctx->inst_theta2, (size_t) count), "alloc batch");
+        NB_TRY(dev_alloc(&ctx->inst_box, (size_t) count * 6), "alloc batch");
+        NB_TRY(dev_alloc(&ctx->inst_range, (size_t) count), "alloc batch");
+        NB_TRY(dev_alloc(&ctx->group_first, (size_t) count), "alloc batch");
+        ctx->batch_inst_cap = count;
+    }
+    if (ngroups > ctx->batch_group_cap) {
+        dev_free(ctx->groups);
+        ctx->batch_group_cap = 0;
+        NB_TRY(dev_alloc(&ctx->groups, (size_t) ngroups), "alloc batch");
+        ctx->batch_group_cap = ngroups;
+    }
+    if (!ctx->inst_offsets) NB_TRY(dev_alloc(&ctx->inst_offsets, offsets.size()), "alloc batch");
+    if (!ctx->inst_tiles) NB_TRY(dev_alloc(&ctx->inst_tiles, 8), "alloc batch");
+    (void) tiles;
+    int *group_first_dev = ctx->group_first;
     cudaStream_t s = ctx->stream;
-    NB_TRY(cudaMemcpyAsync(ctx->inst_of, inst_of.data(), inst_of.size() * sizeof(int), cudaMemcpyHostToDevice, s), "copy");
     NB_TRY(cudaMemcpyAsync(ctx->inst_theta2, theta2.data(), theta2.size() * sizeof(float), cudaMemcpyHostToDevice, s),
            "copy");
     NB_TRY(cudaMemcpyAsync(ctx->inst_range, range.data(), range.size() * sizeof(int2), cudaMemcpyHostToDevice, s), "copy");
-    NB_TRY(cudaMemcpyAsync(ctx->groups, groups.data(), groups.size() * sizeof(int4), cudaMemcpyHostToDevice, s), "copy");
+    NB_TRY(cudaMemcpyAsync(group_first_dev, group_first.data(), group_first.size() * sizeof(int), cudaMemcpyHostToDevice,
+                           s), "copy");
+    launch_fill_tables(ctx->inst_range, group_first_dev, count, ctx->inst_of, ctx->groups, s);
     NB_TRY(cudaMemcpyAsync(ctx->inst_offsets, offsets.data(), offsets.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s),
            "copy");
     ctx->num_inst = count;
-    ctx->ngroups = (int64_t) groups.size();
+    ctx->ngroups = ngroups;
     ctx->inst_passes = passes;
     // host vectors are released on return: wait for the copies out of them
     return check_cuda(ctx, cudaStreamSynchronize(s), "batch tables");
@@ -1013,8 +1032,8 @@ static int server_relayout(nb_server *sv) {
     }
     int rc = ensure_capacity(ctx, total);
     if (rc != NB_OK) return server_fail(sv, rc);
-    free_batch(ctx);
     drop_graph(ctx);
+    ctx->num_inst = 0;  // the batch buffers stay allocated; the tables are rebuilt below
     ctx->n = total;
     ctx->steps_since_set = 0;
     ctx->bbox_valid = false;

@@ -206,6 +206,8 @@ void launch_seg_morton(const float4 *pos, int64_t n, const int *inst_of, const f
 void launch_inst_keys(const uint32_t *slot, int64_t n, const int *inst_of, uint64_t *ikeys, cudaStream_t s);
 void launch_compose(const uint32_t *order, int64_t n, const uint32_t *slot, const uint64_t *codes, uint32_t *perm,
                     uint64_t *codes_out, cudaStream_t s);
+void launch_fill_tables(const int2 *inst_range, const int *group_first, int num_inst, int *inst_of, int4 *groups,
+                        cudaStream_t s);
 
 // Largest number of bodies one context accepts (30-bit counts in the sort's look-back words,
 // 31-bit body indices in the tree).
