@@ -47,15 +47,21 @@ typedef enum nb_solver {
      * order 1 = LinearBVHSolver ("linear-bvh"), order 2 = QuadrupoleLinearBVHSolver ("linear-bvh-4p"). */
     NB_SOLVER_LINEAR_BVH = 0,
     /* NaiveSolver (src/NBody/Simulation/Solvers/NaiveSolver.h:12-53, "naive"): FP32 direct sum. */
-    NB_SOLVER_NAIVE = 1
+    NB_SOLVER_NAIVE = 1,
+    /* MultipoleImplicitLinearBVHFMMSolver<3> (ImplicitLinearBVHFMMSolver.h:15-33 over
+     * ImplicitDualTraversalSolver.h:17-82, "implicit-linear-bvh-fmm-8p"): dual-tree traversal under
+     * DiagonalOverSeparation, octupole node moments, local fields of order 4. Requires order 3. */
+    NB_SOLVER_DUAL_LINEAR_BVH = 2
 } nb_solver;
 
 typedef struct nb_config {
     int32_t solver;        /* nb_solver */
-    int32_t order;         /* multipole order of the node summaries: 1 (centre of mass) or 2 (quadrupole) */
+    int32_t order;         /* multipole order of the node summaries: 1 (centre of mass) or 2 (quadrupole);
+                            * 3 (octupole) with NB_SOLVER_DUAL_LINEAR_BVH */
     float G;               /* Gravity::g()        (Gravity.h:195, 407) */
     float epsilon;         /* Gravity::epsilon(): added to r^2 (Gravity.h:207) */
-    float theta;           /* ActiveTreeSolver::theta() (ActiveTreeSolver.h:78-80) */
+    float theta;           /* ActiveTreeSolver::theta() (ActiveTreeSolver.h:78-80); the dual solver's
+                            * DiagonalOverSeparation::theta() (DiagonalOverSeparation.h:19-27) */
     int32_t max_leaf_size; /* LinearBVH::maxLeafSize() (LinearBVH.h:135-137) */
     float time_step;       /* Solver::timeStep() (Solver.h:101) */
     int32_t device;        /* CUDA device ordinal */
@@ -137,7 +143,10 @@ int nb_get_phase_times(nb_ctx *ctx, nb_phase_times *out);
 
 /* Parity taps on the last tree built (synchronise). Any output pointer may be NULL.
  *   num_nodes     node count of the linear BVH (preorder)
- *   record_floats floats per node record (12 for order 1, 16 for order 2); see nb_tree_record
+ *   record_floats floats per node record (12 for order 1, 16 for order 2; 32 for the dual solver:
+ *                 box min xyz + body count (int bits), box max xyz + diagonal length, centre of
+ *                 mass + mass, link (2 ints, 2 zero), quadrupole (6), octupole (10));
+ *                 see nb_tree_record
  *   sorted_codes  n Morton codes in sorted order (MortonSort.h:46-73)
  *   sorted_ids    n caller indices of the sorted bodies (the Morton sort's permutation)
  *   records       num_nodes * record_floats floats

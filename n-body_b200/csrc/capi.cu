@@ -57,6 +57,9 @@ struct nb_ctx {
     TreeWorkspace tw;
     NodeArrays nodes;
     TraverseWorkspace trav;
+    DualNodes dnodes;          // dual solver: octupole node arrays
+    DualWorkspace dws;         // dual solver: starting nodes, per-block arenas and task stacks
+    int64_t dual_cap = 0;      // body capacity the dual buffers were sized for
     BBoxAccum *bbox = nullptr;
     unsigned long long *counts = nullptr;
     uint32_t *err = nullptr;
@@ -89,6 +92,7 @@ struct nb_ctx {
     bool have_tree = false;
     bool have_acc = false;
     bool acc_is_bh = false;
+    bool acc_is_dual = false;
 
     bool timing = false;
     std::vector<cudaEvent_t> event_pool;
@@ -121,7 +125,10 @@ int pay_float4s(int order) { return order == 1 ? NodeLayout<1>::PAY : NodeLayout
 int rec_floats(int order) { return 8 + 4 * pay_float4s(order); }
 
 void refresh_names(nb_ctx *ctx) {
-    if (ctx->cfg.solver == NB_SOLVER_NAIVE) {
+    if (ctx->cfg.solver == NB_SOLVER_DUAL_LINEAR_BVH) {
+        ctx->id_str = "implicit-linear-bvh-fmm-8p";
+        ctx->name_str = "Implicit Linear-BVH Fast Multipole Method (Octupole)";
+    } else if (ctx->cfg.solver == NB_SOLVER_NAIVE) {
         ctx->id_str = "naive";
         ctx->name_str = "Naive";
     } else if (ctx->cfg.order == 1) {
@@ -135,10 +142,14 @@ void refresh_names(nb_ctx *ctx) {
 
 int validate(nb_ctx *ctx, const nb_config *cfg) {
     if (!cfg) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "config is NULL");
-    if (cfg->solver != NB_SOLVER_LINEAR_BVH && cfg->solver != NB_SOLVER_NAIVE)
+    if (cfg->solver != NB_SOLVER_LINEAR_BVH && cfg->solver != NB_SOLVER_NAIVE &&
+        cfg->solver != NB_SOLVER_DUAL_LINEAR_BVH)
         return fail(ctx, NB_ERR_INVALID_ARGUMENT, "unknown solver");
-    if (cfg->order < 1 || cfg->order > kMaxOrder)
+    if (cfg->solver == NB_SOLVER_DUAL_LINEAR_BVH) {
+        if (cfg->order != 3) return fail(ctx, NB_ERR_UNSUPPORTED, "the dual-tree solver runs at order 3 (octupole)");
+    } else if (cfg->order < 1 || cfg->order > kMaxOrder) {
         return fail(ctx, NB_ERR_UNSUPPORTED, "order must be 1 (centre of mass) or 2 (quadrupole)");
+    }
     if (cfg->max_leaf_size < 1) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "max_leaf_size must be >= 1");
     if (!(cfg->theta >= 0.f)) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "theta must be >= 0");
     if (!(cfg->epsilon >= 0.f)) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "epsilon must be >= 0");
@@ -162,7 +173,42 @@ void drop_graph(nb_ctx *ctx) {
     ctx->graph2 = nullptr;
 }
 
+void free_dual(nb_ctx *ctx) {
+    dev_free(ctx->tw.sq2); dev_free(ctx->tw.sq3);
+    dev_free(ctx->dnodes.bmin); dev_free(ctx->dnodes.bmax); dev_free(ctx->dnodes.com); dev_free(ctx->dnodes.q);
+    dev_free(ctx->dnodes.link);
+    ctx->dnodes.capacity = 0;
+    dev_free(ctx->dws.roots); dev_free(ctx->dws.num_roots); dev_free(ctx->dws.arena); dev_free(ctx->dws.tasks);
+    ctx->dws.arena_words = 0;
+    ctx->dual_cap = 0;
+}
+
+// Buffers of the dual solver, sized for the current body capacity (allocated before any capture).
+int ensure_dual(nb_ctx *ctx) {
+    if (ctx->cfg.solver != NB_SOLVER_DUAL_LINEAR_BVH || ctx->cap == 0) return NB_OK;
+    if (ctx->dual_cap == ctx->cap) return NB_OK;
+    free_dual(ctx);
+    const int64_t c = ctx->cap;
+    const size_t slots = (size_t) (2 * c);
+    NB_TRY(dev_alloc(&ctx->tw.sq2, slots), "alloc octupole summaries");
+    NB_TRY(dev_alloc(&ctx->tw.sq3, slots), "alloc octupole summaries");
+    NB_TRY(dev_alloc(&ctx->dnodes.bmin, slots), "alloc dual nodes");
+    NB_TRY(dev_alloc(&ctx->dnodes.bmax, slots), "alloc dual nodes");
+    NB_TRY(dev_alloc(&ctx->dnodes.com, slots), "alloc dual nodes");
+    NB_TRY(dev_alloc(&ctx->dnodes.q, 4 * slots), "alloc dual nodes");
+    NB_TRY(dev_alloc(&ctx->dnodes.link, slots), "alloc dual nodes");
+    ctx->dnodes.capacity = (int64_t) slots;
+    NB_TRY(dev_alloc(&ctx->dws.roots, kDualRoots), "alloc dual roots");
+    NB_TRY(dev_alloc(&ctx->dws.num_roots, 1), "alloc dual roots");
+    ctx->dws.arena_words = dual_arena_words(c);
+    NB_TRY(dev_alloc(&ctx->dws.arena, (size_t) kDualRoots * (size_t) ctx->dws.arena_words), "alloc dual arena");
+    NB_TRY(dev_alloc(&ctx->dws.tasks, (size_t) kDualRoots * kDualTasks * 6), "alloc dual tasks");
+    ctx->dual_cap = c;
+    return NB_OK;
+}
+
 void free_buffers(nb_ctx *ctx) {
+    free_dual(ctx);
     dev_free(ctx->pos); dev_free(ctx->vel); dev_free(ctx->acc); dev_free(ctx->pos2); dev_free(ctx->vel2);
     dev_free(ctx->id); dev_free(ctx->id2); dev_free(ctx->keys); dev_free(ctx->vals);
     dev_free(ctx->sw.keys_alt); dev_free(ctx->sw.vals_alt); dev_free(ctx->sw.lookback);
@@ -211,7 +257,7 @@ int ensure_capacity(nb_ctx *ctx, int64_t n) {
     NB_TRY(dev_alloc(&ctx->nodes.pay, (size_t) node_cap * NodeLayout<2>::PAY), "alloc tree nodes");
     ctx->nodes.capacity = node_cap;
     ctx->cap = c;
-    return NB_OK;
+    return ensure_dual(ctx);
 }
 
 cudaEvent_t take_event(nb_ctx *ctx) {
@@ -265,10 +311,12 @@ void collect_times(nb_ctx *ctx) {
 // Kernel launches of one force pass + drift (for the launch count the bench reports).
 int64_t launches_per_pass(const nb_ctx *ctx, bool with_bbox, bool with_drift) {
     if (ctx->cfg.solver == NB_SOLVER_NAIVE) return 1 + (with_drift ? 1 : 0);
+    // the dual path adds loadBalancedBreak to the same pipeline
     // morton(1) + scan(1) + 8 sort passes + gather(1) + karras(1) + summarize(1) + emit(1)
     // + root-leaf(1) + traverse(1)
     int64_t k = 1 + 1 + 8 + 1 + 1 + 1 + 1 + 1 + 1;
     if (ctx->n <= 1) k -= 3;  // no Karras internal nodes
+    if (ctx->cfg.solver == NB_SOLVER_DUAL_LINEAR_BVH) k += 1;
     return k + (with_bbox ? 1 : 0) + (with_drift ? 1 : 0);
 }
 
@@ -326,6 +374,7 @@ int force_pass(nb_ctx *ctx, Marks &mk) {
     const int64_t n = ctx->n;
     cudaStream_t s = ctx->stream;
     cudaMemsetAsync(ctx->counts, 0, 4 * sizeof(unsigned long long), s);
+    ctx->acc_is_dual = false;
     const bool need_bbox = !ctx->bbox_valid;
     mk.mark(kBBox);
     if (ctx->cfg.solver == NB_SOLVER_NAIVE) {
@@ -351,9 +400,21 @@ int force_pass(nb_ctx *ctx, Marks &mk) {
     std::swap(ctx->vel, ctx->vel2);
     std::swap(ctx->id, ctx->id2);
     mk.mark(kBuild);
+    ctx->sorted_codes = ctx->keys;
+    if (ctx->cfg.solver == NB_SOLVER_DUAL_LINEAR_BVH) {
+        if (ctx->dual_cap != ctx->cap) return fail(ctx, NB_ERR_CUDA, "dual-tree buffers missing");
+        launch_build_dual_tree(ctx->keys, ctx->pos, n, ctx->cfg.max_leaf_size, ctx->tw, ctx->dnodes, ctx->err, s);
+        mk.mark(kTraverse);
+        launch_dual_traverse(ctx->dnodes, ctx->tw.num_nodes, ctx->pos, n, ctx->cfg.G, ctx->cfg.epsilon,
+                             ctx->cfg.theta, ctx->acc, ctx->counts, ctx->dws, ctx->err, s);
+        ctx->have_tree = true;
+        ctx->acc_is_bh = true;
+        ctx->acc_is_dual = true;
+        if (ctx->timing) ctx->times.launches += launches_per_pass(ctx, need_bbox, false);
+        return check_cuda(ctx, cudaGetLastError(), "dual-tree force pass");
+    }
     launch_build_tree(ctx->keys, ctx->pos, n, ctx->cfg.max_leaf_size, ctx->cfg.order, ctx->cfg.theta, ctx->tw,
                       ctx->nodes, ctx->err, s);
-    ctx->sorted_codes = ctx->keys;
     mk.mark(kTraverse);
     launch_bh_traverse(ctx->cfg.order, ctx->nodes, ctx->tw.num_nodes, ctx->pos, n, ctx->pos, n, ctx->cfg.G,
                        ctx->cfg.epsilon, ctx->acc, ctx->counts, ctx->trav, ctx->err, s);
@@ -374,6 +435,7 @@ int device_status(nb_ctx *ctx) {
     if (e & kErrTreeDepth) return fail(ctx, NB_ERR_DEVICE_CHECK, "tree walk exceeded the maximum depth");
     if (e & kErrStackOverflow) return fail(ctx, NB_ERR_DEVICE_CHECK, "traversal stack overflow");
     if (e & kErrTraverseLimit) return fail(ctx, NB_ERR_DEVICE_CHECK, "traversal met an invalid tree link");
+    if (e & kErrDualArena) return fail(ctx, NB_ERR_DEVICE_CHECK, "dual-tree list or task storage exhausted");
     return NB_OK;
 }
 
@@ -471,11 +533,13 @@ int nb_set_config(nb_ctx *ctx, const nb_config *cfg) {
     int rc = validate(ctx, cfg);
     if (rc != NB_OK) return rc;
     if (cfg->device != ctx->cfg.device) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "the device cannot change");
+    if (cfg->solver == NB_SOLVER_DUAL_LINEAR_BVH && ctx->num_inst > 0)
+        return fail(ctx, NB_ERR_UNSUPPORTED, "the dual-tree solver runs one instance");
     ctx->cfg = *cfg;
     ctx->have_tree = false;
     drop_graph(ctx);
     refresh_names(ctx);
-    return NB_OK;
+    return ensure_dual(ctx);
 }
 
 int nb_get_config(const nb_ctx *ctx, nb_config *cfg) {
@@ -691,6 +755,7 @@ int nb_get_counts(nb_ctx *ctx, nb_counts *out) {
     NB_TRY(cudaMemcpyAsync(c, ctx->counts, sizeof(c), cudaMemcpyDeviceToHost, ctx->stream), "read counts");
     rc = device_status(ctx);
     if (rc != NB_OK) return rc;
+    // device counters: {particle-particle, node-particle, particle-node, node-node}
     if (ctx->acc_is_bh) {
         out->particle_particle = c[0];
         out->node_particle = c[1];
@@ -698,8 +763,8 @@ int nb_get_counts(nb_ctx *ctx, nb_counts *out) {
         out->particle_particle = (uint64_t) ctx->n * (uint64_t) ctx->n;
         out->node_particle = 0;
     }
-    out->particle_node = 0;
-    out->node_node = 0;
+    out->particle_node = ctx->acc_is_dual ? c[2] : 0;
+    out->node_node = ctx->acc_is_dual ? c[3] : 0;
     return NB_OK;
 }
 
@@ -732,7 +797,8 @@ int nb_get_tree(nb_ctx *ctx, int64_t *num_nodes, int32_t *record_floats, uint64_
     NB_TRY(cudaMemcpyAsync(box, ctx->bbox, sizeof(box), cudaMemcpyDeviceToHost, ctx->stream), "read bbox");
     rc = device_status(ctx);
     if (rc != NB_OK) return rc;
-    const int rf = rec_floats(ctx->cfg.order);
+    const bool dual = ctx->acc_is_dual;
+    const int rf = dual ? 32 : rec_floats(ctx->cfg.order);
     if (num_nodes) *num_nodes = nn;
     if (record_floats) *record_floats = rf;
     if (bbox) {
@@ -747,7 +813,29 @@ int nb_get_tree(nb_ctx *ctx, int64_t *num_nodes, int32_t *record_floats, uint64_
                "codes");
     if (sorted_ids && n > 0)
         NB_TRY(cudaMemcpyAsync(sorted_ids, ctx->id, (size_t) n * 4, cudaMemcpyDeviceToHost, ctx->stream), "ids");
-    if (records && nn > 0) {
+    if (records && nn > 0 && dual) {
+        std::vector<float4> a((size_t) nn), b((size_t) nn), c((size_t) nn), q((size_t) nn * 4);
+        std::vector<int2> link((size_t) nn);
+        const size_t f4 = (size_t) nn * sizeof(float4);
+        NB_TRY(cudaMemcpyAsync(a.data(), ctx->dnodes.bmin, f4, cudaMemcpyDeviceToHost, ctx->stream), "records");
+        NB_TRY(cudaMemcpyAsync(b.data(), ctx->dnodes.bmax, f4, cudaMemcpyDeviceToHost, ctx->stream), "records");
+        NB_TRY(cudaMemcpyAsync(c.data(), ctx->dnodes.com, f4, cudaMemcpyDeviceToHost, ctx->stream), "records");
+        NB_TRY(cudaMemcpyAsync(q.data(), ctx->dnodes.q, 4 * f4, cudaMemcpyDeviceToHost, ctx->stream), "records");
+        NB_TRY(cudaMemcpyAsync(link.data(), ctx->dnodes.link, (size_t) nn * sizeof(int2), cudaMemcpyDeviceToHost,
+                               ctx->stream), "records");
+        rc = device_status(ctx);
+        if (rc != NB_OK) return rc;
+        for (int64_t k = 0; k < nn; ++k) {
+            float *r = records + k * rf;
+            std::memcpy(r, &a[k], 16);
+            std::memcpy(r + 4, &b[k], 16);
+            std::memcpy(r + 8, &c[k], 16);
+            std::memcpy(r + 12, &link[k], 8);
+            r[14] = 0.f;
+            r[15] = 0.f;
+            std::memcpy(r + 16, &q[4 * k], 64);
+        }
+    } else if (records && nn > 0) {
         const int pf = pay_float4s(ctx->cfg.order);
         std::vector<float4> mac((size_t) nn), pay((size_t) nn * pf);
         std::vector<int2> link((size_t) nn);
@@ -892,6 +980,8 @@ int nb_set_instances(nb_ctx *ctx, int32_t count, const int64_t *sizes, const flo
                      const float *velocity) {
     int rc = begin(ctx);
     if (rc != NB_OK) return rc;
+    if (ctx->cfg.solver == NB_SOLVER_DUAL_LINEAR_BVH)
+        return fail(ctx, NB_ERR_UNSUPPORTED, "the dual-tree solver runs one instance");
     int64_t n = 0;
     rc = check_instances(ctx, count, sizes, thetas, &n);
     if (rc != NB_OK) return rc;

@@ -1,0 +1,733 @@
+// Implicit-field dual-tree traversal on the device: the reference's
+// MultipoleImplicitLinearBVHFMMSolver<3> (octupole node moments, local field of order 4) under the
+// DiagonalOverSeparation criterion.
+//
+// Decisions follow the reference, evaluated with the same IEEE operations, so the set of
+// interactions (and the interaction counts) equals the reference's:
+//   ImplicitDualTraversalSolver::updateAccelerations   ImplicitDualTraversalSolver.h:42-69
+//   Tree::loadBalancedBreak(256)                       Tree.h:84-107
+//   balancedLockstepDualTreeImplicitField              balancedLockstepDualTreeImplicitField.h:14-46
+//   lockstepDualTreeImplicitField                      lockstepDualTreeImplicitField.h:21-168
+//   passiveTreeImplicitField                           passiveTreeImplicitField.h:13-78
+//   activeTree (point form of the criterion)           activeTree.h:24-79
+//   DiagonalOverSeparation                             DiagonalOverSeparation.h:17-49
+//   separation                                         BoundingBox.h:84-94 (std::pow(float, int) is a
+//                                                      double pow, so the sum and root are in double)
+//   M2L / P2L / M2P / L2L / L2P                        Gravity.h:239-259, 282-306, 352-392;
+//                                                      MultipoleAcceleration.h:33-84
+//
+// Work organisation. One thread block per starting passive node (the <= 256 nodes of
+// loadBalancedBreak, found on the device). Each block runs the reference's recursion as a
+// depth-first stack of tasks (lock-step tasks and passive-tree tasks) whose lists and local fields
+// live in a per-block arena of global memory; every step of a task is block-parallel:
+//   - classifying an active-node or active-body list: one entry per thread, stable block-wide
+//     compaction (ballots and warp counts), so list order is deterministic;
+//   - M2L / P2L into the task's local field: per-thread partial fields, fixed-order block reduction;
+//   - near field at a passive leaf: the (body, active subtree) activeTree walks or (body, close
+//     body) pairs spread over the block, partial sums reduced per body in a fixed order.
+// Results are deterministic run to run. The floating-point accumulation order differs from the
+// reference's serial recursion; the interactions evaluated are the same.
+#include <algorithm>
+#include <cfloat>
+
+#include "nb_internal.cuh"
+#include "stensor.cuh"
+
+namespace nbg {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kTaskInts = 6;  // type, passive node, list offset, list length, field offset, arena top
+constexpr int kLockstep = 0, kPassive = 1;
+constexpr int kWalkStack = kMaxTreeDepth + 2;
+constexpr int F = st::kFieldFloats;
+
+// Dual-tree node as stored (nb_internal.cuh, DualNodes). Internal nodes keep ~first body in link.y.
+struct DNode {
+    float mn[3], mx[3], diag;
+    int size;
+    float com[3], M;
+    int link0, link1;
+    __device__ bool leaf() const { return link1 >= 0; }
+    __device__ int first() const { return link1 >= 0 ? link0 : -1 - link1; }
+};
+
+__device__ __forceinline__ DNode load_node(const DualNodes &N, int k) {
+    DNode d;
+    const float4 a = __ldg(N.bmin + k), b = __ldg(N.bmax + k), c = __ldg(N.com + k);
+    const int2 l = __ldg(N.link + k);
+    d.mn[0] = a.x; d.mn[1] = a.y; d.mn[2] = a.z; d.size = __float_as_int(a.w);
+    d.mx[0] = b.x; d.mx[1] = b.y; d.mx[2] = b.z; d.diag = b.w;
+    d.com[0] = c.x; d.com[1] = c.y; d.com[2] = c.z; d.M = c.w;
+    d.link0 = l.x; d.link1 = l.y;
+    return d;
+}
+
+// BoundingBox::center: (max + min) / 2
+__device__ __forceinline__ void center(const DNode &n, float c[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) c[k] = fdiv(fadd(n.mx[k], n.mn[k]), 2.0f);
+}
+
+__device__ __forceinline__ float max0(float x) { return (x < 0.f) ? 0.f : x; }
+// glm::length: sqrt((x*x + y*y) + z*z)
+__device__ __forceinline__ float len3(float a, float b, float c) {
+    return __fsqrt_rn(fadd(fadd(fmul(a, a), fmul(b, b)), fmul(c, c)));
+}
+// (float) sqrt(pow(|u|, 2) + pow(|v|, 2)) with the pow, sum and root in double
+__device__ __forceinline__ float sep_from(float lu, float lv) {
+    const double du = (double) lu, dv = (double) lv;
+    return __double2float_rn(__dsqrt_rn(__dadd_rn(__dmul_rn(du, du), __dmul_rn(dv, dv))));
+}
+__device__ __forceinline__ float sep_point(const DNode &n, const float p[3]) {
+    const float lu = len3(max0(fsub(n.mn[0], p[0])), max0(fsub(n.mn[1], p[1])), max0(fsub(n.mn[2], p[2])));
+    const float lv = len3(max0(fsub(p[0], n.mx[0])), max0(fsub(p[1], n.mx[1])), max0(fsub(p[2], n.mx[2])));
+    return sep_from(lu, lv);
+}
+__device__ __forceinline__ float sep_box(const DNode &a, const DNode &b) {
+    const float lu = len3(max0(fsub(a.mn[0], b.mx[0])), max0(fsub(a.mn[1], b.mx[1])), max0(fsub(a.mn[2], b.mx[2])));
+    const float lv = len3(max0(fsub(b.mn[0], a.mx[0])), max0(fsub(b.mn[1], a.mx[1])), max0(fsub(b.mn[2], a.mx[2])));
+    return sep_from(lu, lv);
+}
+
+// DiagonalOverSeparation, (active node, point): approximate the node for the point
+__device__ __forceinline__ bool approx_for_point(const DNode &a, const float p[3], float theta) {
+    return fdiv(a.diag, sep_point(a, p)) < theta && a.size > 32;
+}
+// (point, passive node): the active point is far from the passive node
+__device__ __forceinline__ bool point_is_far(const float p[3], const DNode &P, float theta) {
+    return fdiv(fmul(3.0f, P.diag), sep_point(P, p)) < theta;
+}
+// (active node, passive node): 0 = approximate, else DescendActive (1) | DescendPassive (2)
+__device__ __forceinline__ int node_node(const DNode &A, const DNode &P, float theta) {
+    if (fdiv(fadd(A.diag, P.diag), sep_box(A, P)) < theta && A.size > 32) return 0;
+    int r = 0;
+    if (A.diag <= fmul(P.diag, 2.0f)) r |= 2;
+    if (P.diag <= fmul(A.diag, 2.0f)) r |= 1;
+    return r;
+}
+
+struct Ctx {
+    DualNodes nodes;
+    const float4 *bodies;
+    float G, eps, theta;
+    int nn, n;  // node and body counts
+    // Preorder links only point forward: a child's index exceeds its parent's and the left child's
+    // (parent + 1); a leaf's bodies lie in [0, n). A link that breaks this is not followed (error
+    // bit kErrTraverseLimit), so every descent terminates and stays in bounds.
+    __device__ bool right_ok(int k, int right) const { return right > k + 1 && right < nn; }
+    __device__ bool left_ok(int k) const { return k + 1 < nn; }
+    __device__ bool range_ok(int first, int end) const { return 0 <= first && first <= end && end <= n; }
+};
+
+__device__ __forceinline__ void load_q(const DualNodes &N, int k, float q2[6], float q3[10]) {
+    const float4 *q = N.q + (int64_t) k * 4;
+    const float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
+    q2[0] = a.x; q2[1] = a.y; q2[2] = a.z; q2[3] = a.w; q2[4] = b.x; q2[5] = b.y;
+    q3[0] = b.z; q3[1] = b.w; q3[2] = c.x; q3[3] = c.y; q3[4] = c.z; q3[5] = c.w;
+    q3[6] = d.x; q3[7] = d.y; q3[8] = d.z; q3[9] = d.w;
+}
+
+__device__ __forceinline__ float soft_r(const float R[3], float eps) {
+    return sqrtf(fmaf(R[0], R[0], fmaf(R[1], R[1], fmaf(R[2], R[2], eps))));
+}
+
+// Gravity::particleParticle (Gravity.h:199-209), added into a
+__device__ __forceinline__ void pair(const Ctx &x, float4 b, const float p[3], float a[3]) {
+    const float R[3] = {p[0] - b.x, p[1] - b.y, p[2] - b.z};
+    if (R[0] == 0.f && R[1] == 0.f && R[2] == 0.f) return;
+    const float r = soft_r(R, x.eps);
+    const float s = b.w * x.G / (r * (r * r));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) a[i] = fmaf(-R[i], s, a[i]);
+}
+
+// Gravity::nodeParticle for MultipoleMassSummary<3> (Gravity.h:239-259), added into a
+__device__ void node_particle3(const Ctx &x, int k, const DNode &n, const float p[3], float a[3]) {
+    const float R[3] = {p[0] - n.com[0], p[1] - n.com[1], p[2] - n.com[2]};
+    if (R[0] == 0.f && R[1] == 0.f && R[2] == 0.f) return;
+    const float r = soft_r(R, x.eps);
+    const st::Coef c(r);
+    float q2[6], q3[10], d3[10], d4[15], v3[3], v4[3];
+    load_q(x.nodes, k, q2, q3);
+    st::D3(R, c, d3);
+    st::D4(R, c, d4);
+    st::t3_dot_t2(d3, q2, v3);
+    st::t4_dot_t3(d4, q3, v4);
+    const float mono = -n.M / (r * (r * r));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) a[i] += x.G * (R[i] * mono + v3[i] / 2.0f - v4[i] / 6.0f);
+}
+
+// Gravity::nodeNode for MultipoleMassSummary<3> -> MultipoleAccelerationSummary<4> (M2L,
+// Gravity.h:352-392), added into the local field f about pc. As in the reference, the moment
+// terms carry no factor G.
+__device__ void m2l(const Ctx &x, int k, const DNode &n, const float pc[3], float *f) {
+    const float R[3] = {pc[0] - n.com[0], pc[1] - n.com[1], pc[2] - n.com[2]};
+    if (R[0] == 0.f && R[1] == 0.f && R[2] == 0.f) return;
+    const float r = soft_r(R, x.eps);
+    const st::Coef c(r);
+    float q2[6], q3[10], d2[6], d3[10], d4[15], v3[3], v4[3], t2q[6];
+    load_q(x.nodes, k, q2, q3);
+    st::D2(R, c, d2);
+    st::D3(R, c, d3);
+    st::D4(R, c, d4);
+    st::t3_dot_t2(d3, q2, v3);
+    st::t4_dot_t3(d4, q3, v4);
+    st::t4_dot_t2(d4, q2, t2q);
+    const float mg = n.M * x.G;
+    const float mono = mg / (r * (r * r));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) f[i] += -R[i] * mono + v3[i] / 2.0f + v4[i] / 6.0f;
+#pragma unroll
+    for (int a = 0; a < 6; ++a) f[3 + a] += d2[a] * mg - t2q[a] * 0.5f;
+#pragma unroll
+    for (int a = 0; a < 10; ++a) f[9 + a] += d3[a] * mg * 0.5f;
+#pragma unroll
+    for (int a = 0; a < 15; ++a) f[19 + a] += d4[a] * mg * (1.0f / 6.0f);
+}
+
+// Gravity::particleNode into MultipoleAccelerationSummary<4> (P2L, Gravity.h:282-306)
+__device__ void p2l(const Ctx &x, float4 b, const float pc[3], float *f) {
+    const float R[3] = {pc[0] - b.x, pc[1] - b.y, pc[2] - b.z};
+    if (R[0] == 0.f && R[1] == 0.f && R[2] == 0.f) return;
+    const float r = soft_r(R, x.eps);
+    const st::Coef c(r);
+    float d2[6], d3[10], d4[15];
+    st::D2(R, c, d2);
+    st::D3(R, c, d3);
+    st::D4(R, c, d4);
+    const float mg = b.w * x.G;
+    const float inv3 = 1.0f / (r * (r * r));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) f[i] -= R[i] * inv3 * mg;
+#pragma unroll
+    for (int a = 0; a < 6; ++a) f[3 + a] += d2[a] * mg;
+#pragma unroll
+    for (int a = 0; a < 10; ++a) f[9 + a] += d3[a] * mg * 0.5f;
+#pragma unroll
+    for (int a = 0; a < 15; ++a) f[19 + a] += d4[a] * mg * (1.0f / 6.0f);
+}
+
+// activeTree from node `root` for the point p (activeTree.h:24-79): left subtree first.
+__device__ void active_tree(const Ctx &x, int root, const float p[3], float a[3], unsigned long long &npp,
+                            unsigned long long &nnp, uint32_t *err) {
+    int stk[kWalkStack];
+    int sp = 0;
+    stk[sp++] = root;
+    while (sp > 0) {
+        const int k = stk[--sp];
+        const DNode n = load_node(x.nodes, k);
+        if (approx_for_point(n, p, x.theta)) {
+            node_particle3(x, k, n, p, a);
+            ++nnp;
+        } else if (n.leaf()) {
+            if (!x.range_ok(n.link0, n.link1)) {
+                atomicOr(err, (uint32_t) kErrTraverseLimit);
+                continue;
+            }
+            for (int j = n.link0; j < n.link1; ++j) pair(x, __ldg(x.bodies + j), p, a);
+            npp += (unsigned long long) (n.link1 - n.link0);
+        } else {
+            if (sp + 2 > kWalkStack) {
+                atomicOr(err, (uint32_t) kErrTreeDepth);
+                return;
+            }
+            if (!x.left_ok(k) || !x.right_ok(k, n.link0)) {
+                atomicOr(err, (uint32_t) kErrTraverseLimit);
+                continue;
+            }
+            stk[sp++] = n.link0;  // right child, visited second
+            stk[sp++] = k + 1;    // left child
+        }
+    }
+}
+
+struct Scan3 {
+    int wcnt[3][kWarps];
+    int base[3];
+};
+
+// Stable block-wide rank of a class label (0..2, or -1 for none) in thread order; returns the
+// element's position within its class, the running bases in s.base carrying across calls.
+// Every thread of the block must call it.
+__device__ int stable_rank(int cls, Scan3 &s) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned m0 = __ballot_sync(0xffffffffu, cls == 0);
+    const unsigned m1 = __ballot_sync(0xffffffffu, cls == 1);
+    const unsigned m2 = __ballot_sync(0xffffffffu, cls == 2);
+    if (lane == 0) {
+        s.wcnt[0][warp] = __popc(m0);
+        s.wcnt[1][warp] = __popc(m1);
+        s.wcnt[2][warp] = __popc(m2);
+    }
+    __syncthreads();
+    int pos = -1;
+    if (cls >= 0) {
+        const unsigned mine = cls == 0 ? m0 : (cls == 1 ? m1 : m2);
+        int off = s.base[cls];
+        for (int w = 0; w < warp; ++w) off += s.wcnt[cls][w];
+        pos = off + __popc(mine & ((1u << lane) - 1u));
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        int t = 0;
+        for (int w = 0; w < kWarps; ++w) t += s.wcnt[threadIdx.x][w];
+        s.base[threadIdx.x] += t;
+    }
+    __syncthreads();
+    return pos;
+}
+
+// Block-wide exclusive prefix sum of v; every thread gets the block total.
+__device__ int block_exclusive_scan(int v, int *s_w, int &total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) s_w[warp] = x;
+    __syncthreads();
+    int off = 0, tot = 0;
+    for (int w = 0; w < kWarps; ++w) {
+        if (w < warp) off += s_w[w];
+        tot += s_w[w];
+    }
+    __syncthreads();
+    total = tot;
+    return off + x - v;
+}
+
+// Adds the per-thread partial fields into the block's shared field (fixed order: lanes by
+// butterfly, then warps in index order).
+__device__ void block_add_field(const float part[F], float *s_field, float (*s_red)[F]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int a = 0; a < F; ++a) {
+        float v = part[a];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) s_red[warp][a] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < F) {
+        float s = 0.f;
+        for (int w = 0; w < kWarps; ++w) s += s_red[w][threadIdx.x];
+        s_field[threadIdx.x] += s;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void push_task(int *t, int type, int node, int list, int len, int field, int top) {
+    t[0] = type; t[1] = node; t[2] = list; t[3] = len; t[4] = field; t[5] = top;
+}
+
+__global__ void __launch_bounds__(kThreads) dual_kernel(DualNodes nodes, const int *__restrict__ num_nodes,
+                                                        const float4 *__restrict__ bodies, int n, float G,
+                                                        float eps, float theta, float4 *__restrict__ acc,
+                                                        unsigned long long *__restrict__ counts,
+                                                        const int *__restrict__ roots, const int *__restrict__ num_roots,
+                                                        int *__restrict__ arena_all, int arena_words,
+                                                        int *__restrict__ tasks_all, uint32_t *__restrict__ err) {
+    __shared__ float s_field[F];
+    __shared__ float s_child[2][F];
+    __shared__ float s_red[kWarps][F];
+    __shared__ float s_part[kThreads][3];
+    __shared__ int s_task[kTaskInts];
+    __shared__ Scan3 s_scan;
+    __shared__ int s_w[kWarps];
+    __shared__ int s_ntask, s_fail;
+
+    if ((int) blockIdx.x >= *num_roots) return;  // uniform across the block
+    const int tid = threadIdx.x;
+    const Ctx x{nodes, bodies, G, eps, theta, *num_nodes, n};
+    int *arena = arena_all + (int64_t) blockIdx.x * arena_words;
+    float *farena = reinterpret_cast<float *>(arena);
+    int *tasks = tasks_all + (int64_t) blockIdx.x * kDualTasks * kTaskInts;
+    unsigned long long npp = 0, nnp = 0, npn = 0, nnn = 0;
+    const int root = roots[blockIdx.x];
+    if (root < 0 || root >= x.nn || x.nn <= 0) {
+        if (tid == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
+        return;
+    }
+    const DNode Rt = load_node(nodes, root);
+
+    // ---- balancedLockstepDualTreeImplicitField: breadth-first over the active tree from its root;
+    // a node joins the starting list unless the criterion says "descend the active node" only and
+    // it is not a leaf, in which case its children join the next level ----
+    const int eq_cap = arena_words / 4;
+    int cur = eq_cap, curlen = 1;
+    if (tid == 0) {
+        arena[cur] = 0;
+        s_fail = 0;
+    }
+    if (tid < 3) s_scan.base[tid] = 0;
+    __syncthreads();
+    while (curlen > 0) {
+        const int nxt = cur + curlen;
+        for (int i0 = 0; i0 < curlen; i0 += kThreads) {
+            const int i = i0 + tid;
+            int a = -1, cls = -1, right = -1;
+            if (i < curlen) {
+                a = arena[cur + i];
+                const DNode A = load_node(nodes, a);
+                const int rec = node_node(A, Rt, theta);
+                cls = (rec != 1 || A.leaf()) ? 0 : 1;
+                right = A.link0;
+                if (cls == 1 && !(x.left_ok(a) && x.right_ok(a, right))) {
+                    atomicOr(err, (uint32_t) kErrTraverseLimit);
+                    cls = -1;
+                }
+            }
+            const int pos = stable_rank(cls, s_scan);
+            if (cls == 0) {
+                if (pos < eq_cap) arena[pos] = a;
+                else s_fail = 1;
+            } else if (cls == 1) {
+                if ((int64_t) nxt + 2 * (int64_t) pos + 1 < arena_words) {
+                    arena[nxt + 2 * pos] = a + 1;
+                    arena[nxt + 2 * pos + 1] = right;
+                } else {
+                    s_fail = 1;
+                }
+            }
+        }
+        __syncthreads();
+        const int nextlen = 2 * s_scan.base[1];
+        const bool failed = s_fail != 0;
+        __syncthreads();
+        if (tid == 1) s_scan.base[1] = 0;
+        cur = nxt;
+        curlen = failed ? 0 : nextlen;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const int eq = min(s_scan.base[0], eq_cap);
+        push_task(tasks, kLockstep, root, 0, eq, -1, eq);
+        s_ntask = 1;
+        if (s_fail) atomicOr(err, (uint32_t) kErrDualArena);
+    }
+
+    // ---- depth-first task loop ----
+    for (;;) {
+        __syncthreads();
+        const int nt = s_ntask;
+        if (nt == 0) break;
+        __syncthreads();
+        if (tid == 0) {
+            const int *t = tasks + (nt - 1) * kTaskInts;
+            for (int k = 0; k < kTaskInts; ++k) s_task[k] = t[k];
+            s_ntask = nt - 1;
+        }
+        if (tid < 3) s_scan.base[tid] = 0;
+        __syncthreads();
+        const int type = s_task[0], pk = s_task[1], loff = s_task[2], len = s_task[3], foff = s_task[4];
+        const int scratch = s_task[5];
+        const DNode P = load_node(nodes, pk);
+        float pc[3];
+        center(P, pc);
+        const int pfirst = P.first(), pend = pfirst + P.size;
+        if (!x.range_ok(pfirst, pend) || (!P.leaf() && !(x.left_ok(pk) && x.right_ok(pk, P.link0)))) {
+            if (tid == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
+            continue;
+        }
+        if (tid < F) s_field[tid] = foff >= 0 ? farena[foff + tid] : 0.f;
+        __syncthreads();
+
+        if (type == kLockstep && len == 0) {
+            // no active nodes remain: evaluate the local field at every body of the passive node
+            for (int b = pfirst + tid; b < pend; b += kThreads) {
+                const float4 q = __ldg(bodies + b);
+                const float o[3] = {fsub(q.x, pc[0]), fsub(q.y, pc[1]), fsub(q.z, pc[2])};
+                float a[3];
+                st::field_at(s_field, o, a);
+                float4 v = acc[b];
+                v.x += a[0]; v.y += a[1]; v.z += a[2];
+                acc[b] = v;
+            }
+            continue;
+        }
+
+        // arena needed by this task above `scratch`: the three class lists, the deeper list and two
+        // child fields (the leaf-body list is checked once its length is known)
+        const int64_t need = 3 * (int64_t) len + (type == kLockstep ? 2 * (int64_t) len : 0) + 2 * F;
+        if ((int64_t) scratch + need >= arena_words) {
+            if (tid == 0) atomicOr(err, (uint32_t) kErrDualArena);
+            continue;
+        }
+        const int *list = arena + loff;
+        int *c1 = arena + scratch + len, *c2 = c1 + len;
+        int *c0 = arena + scratch;  // scratch for leaf-body offsets (far entries are not stored)
+
+        // ---- classify the list: far entries go into the local field now ----
+        float part[F];
+#pragma unroll
+        for (int a = 0; a < F; ++a) part[a] = 0.f;
+        for (int i0 = 0; i0 < len; i0 += kThreads) {
+            const int i = i0 + tid;
+            int cls = -1, e = -1;
+            if (i < len) {
+                e = list[i];
+                if (type == kLockstep) {
+                    const DNode A = load_node(nodes, e);
+                    if (node_node(A, P, theta) == 0) {
+                        m2l(x, e, A, pc, part);
+                        ++nnn;
+                        cls = 0;
+                    } else if (A.leaf()) {
+                        cls = x.range_ok(A.link0, A.link1) ? 1 : -1;
+                    } else {
+                        cls = (x.left_ok(e) && x.right_ok(e, A.link0)) ? 2 : -1;
+                    }
+                    if (cls < 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
+                } else {
+                    const float4 q = __ldg(bodies + e);
+                    const float pe[3] = {q.x, q.y, q.z};
+                    if (point_is_far(pe, P, theta)) {
+                        p2l(x, q, pc, part);
+                        ++npn;
+                        cls = 0;
+                    } else {
+                        cls = 1;
+                    }
+                }
+            }
+            const int pos = stable_rank(cls, s_scan);
+            if (cls == 1) c1[pos] = e;
+            else if (cls == 2) c2[pos] = e;
+        }
+        const int nleaf = s_scan.base[1], nnon = s_scan.base[2];
+        block_add_field(part, s_field, s_red);
+
+        if (P.leaf()) {
+            // ---- passive leaf: near field (activeTree walks or close-body pairs), then L2P ----
+            const int nnear = (type == kLockstep) ? nleaf + nnon : nleaf;
+            for (int b0 = pfirst; b0 < pend; b0 += kThreads) {
+                const int nb = min(kThreads, pend - b0);
+                const int groups = kThreads / nb;
+                const int bi = tid % nb, g = tid / nb;
+                float v[3] = {0.f, 0.f, 0.f};
+                if (g < groups) {
+                    const float4 q = __ldg(bodies + b0 + bi);
+                    const float p[3] = {q.x, q.y, q.z};
+                    for (int r = g; r < nnear; r += groups) {
+                        if (type == kLockstep) {
+                            active_tree(x, r < nleaf ? c1[r] : c2[r - nleaf], p, v, npp, nnp, err);
+                        } else {
+                            pair(x, __ldg(bodies + c1[r]), p, v);
+                            ++npp;
+                        }
+                    }
+                }
+                s_part[tid][0] = v[0];
+                s_part[tid][1] = v[1];
+                s_part[tid][2] = v[2];
+                __syncthreads();
+                if (tid < nb) {
+                    float s[3] = {0.f, 0.f, 0.f};
+                    for (int k = 0; k < groups; ++k) {
+                        s[0] += s_part[k * nb + tid][0];
+                        s[1] += s_part[k * nb + tid][1];
+                        s[2] += s_part[k * nb + tid][2];
+                    }
+                    const float4 q = __ldg(bodies + b0 + tid);
+                    const float o[3] = {fsub(q.x, pc[0]), fsub(q.y, pc[1]), fsub(q.z, pc[2])};
+                    float a[3];
+                    st::field_at(s_field, o, a);
+                    float4 w = acc[b0 + tid];
+                    w.x += s[0] + a[0];
+                    w.y += s[1] + a[1];
+                    w.z += s[2] + a[2];
+                    acc[b0 + tid] = w;
+                }
+                __syncthreads();
+            }
+            continue;
+        }
+
+        // ---- internal passive node: translate the field to both children ----
+        const int left = pk + 1, right = P.link0;
+        if (tid == 0 || tid == 32) {
+            const DNode C = load_node(nodes, tid == 0 ? left : right);
+            float cc[3];
+            center(C, cc);
+            const float o[3] = {fsub(cc[0], pc[0]), fsub(cc[1], pc[1]), fsub(cc[2], pc[2])};
+            st::field_translated(s_field, o, s_child[tid == 0 ? 0 : 1]);
+        }
+        __syncthreads();
+        const int top = scratch + 3 * len;
+        if (type == kPassive) {
+            // children see the close bodies with their translated fields; left runs first
+            const int fr = top, fl = top + F;
+            for (int a = tid; a < F; a += kThreads) {
+                farena[fr + a] = s_child[1][a];
+                farena[fl + a] = s_child[0][a];
+            }
+            if (tid == 0) {
+                if (nt - 1 + 2 <= kDualTasks) {
+                    int *t = tasks + (nt - 1) * kTaskInts;
+                    push_task(t, kPassive, right, scratch + len, nleaf, fr, fr + F);
+                    push_task(t + kTaskInts, kPassive, left, scratch + len, nleaf, fl, fl + F);
+                    s_ntask = nt + 1;
+                } else {
+                    atomicOr(err, (uint32_t) kErrDualArena);
+                }
+            }
+            continue;
+        }
+
+        // lock-step at an internal passive node: the children of the non-leaf active nodes form the
+        // deeper list shared by both passive children; the bodies of the leaf active nodes go
+        // through passiveTree over this passive node first (with an empty field)
+        const int dp = top;
+        for (int i = tid; i < nnon; i += kThreads) {
+            const int a = c2[i];
+            arena[dp + 2 * i] = a + 1;
+            arena[dp + 2 * i + 1] = __ldg(nodes.link + a).x;
+        }
+        const int fr = dp + 2 * nnon, fl = fr + F, lb = fl + F;
+        for (int a = tid; a < F; a += kThreads) {
+            farena[fr + a] = s_child[1][a];
+            farena[fl + a] = s_child[0][a];
+        }
+        int total = 0;
+        for (int i0 = 0; i0 < nleaf; i0 += kThreads) {
+            const int i = i0 + tid;
+            int sz = 0;
+            if (i < nleaf) {
+                const int2 l = __ldg(nodes.link + c1[i]);
+                sz = l.y - l.x;
+            }
+            int chunk = 0;
+            const int off = block_exclusive_scan(sz, s_w, chunk);
+            if (i < nleaf) c0[i] = total + off;
+            total += chunk;
+        }
+        const bool fits = (int64_t) lb + total < arena_words;
+        if (fits) {
+            for (int i = tid; i < nleaf; i += kThreads) {
+                const int2 l = __ldg(nodes.link + c1[i]);
+                int *dst = arena + lb + c0[i];
+                for (int b = l.x; b < l.y; ++b) dst[b - l.x] = b;
+            }
+        }
+        if (tid == 0) {
+            const int pushes = 2 + (total > 0 ? 1 : 0);
+            if (!fits || nt - 1 + pushes > kDualTasks) {
+                atomicOr(err, (uint32_t) kErrDualArena);
+            } else {
+                int *t = tasks + (nt - 1) * kTaskInts;
+                push_task(t, kLockstep, right, dp, 2 * nnon, fr, fr + F);
+                push_task(t + kTaskInts, kLockstep, left, dp, 2 * nnon, fl, fl + F);
+                if (total > 0) push_task(t + 2 * kTaskInts, kPassive, pk, lb, total, -1, lb + total);
+                s_ntask = nt - 1 + pushes;
+            }
+        }
+    }
+
+    // interaction counts in the order {particle-particle, node-particle, particle-node, node-node}
+    const unsigned long long c[4] = {npp, nnp, npn, nnn};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        unsigned long long v = c[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((tid & 31) == 0 && v) atomicAdd(counts + k, v);
+    }
+}
+
+// Tree::loadBalancedBreak(256) (Tree.h:84-107): split the node with the most bodies until 256
+// starting nodes exist or the largest is a leaf. The heap steps restate libstdc++'s
+// std::pop_heap / std::push_heap (__adjust_heap, __push_heap) so that ties between equal sizes
+// resolve as on the host. One thread; (size, node) pairs in shared memory.
+__global__ void load_balanced_break_kernel(DualNodes nodes, const int *__restrict__ num_nodes, int *__restrict__ roots,
+                                           int *__restrict__ num_roots, uint32_t *__restrict__ err) {
+    __shared__ int hs[kDualRoots + 2], hn[kDualRoots + 2];
+    if (threadIdx.x != 0) return;
+    const int nn = *num_nodes;
+    if (nn <= 0) {
+        *num_roots = 0;
+        return;
+    }
+    auto push_up = [&](int hole, int top, int vs, int vn) {
+        int parent = (hole - 1) / 2;
+        while (hole > top && hs[parent] < vs) {
+            hs[hole] = hs[parent];
+            hn[hole] = hn[parent];
+            hole = parent;
+            parent = (hole - 1) / 2;
+        }
+        hs[hole] = vs;
+        hn[hole] = vn;
+    };
+    auto pop_heap = [&](int len) {
+        if (len <= 1) return;
+        const int L = len - 1;
+        const int vs = hs[L], vn = hn[L];
+        hs[L] = hs[0];
+        hn[L] = hn[0];
+        int hole = 0, child = 0;
+        while (child < (L - 1) / 2) {
+            child = 2 * (child + 1);
+            if (hs[child] < hs[child - 1]) child--;
+            hs[hole] = hs[child];
+            hn[hole] = hn[child];
+            hole = child;
+        }
+        if ((L & 1) == 0 && child == (L - 2) / 2) {
+            child = 2 * (child + 1);
+            hs[hole] = hs[child - 1];
+            hn[hole] = hn[child - 1];
+            hole = child - 1;
+        }
+        push_up(hole, 0, vs, vn);
+    };
+    auto size_of = [&](int k) { return __float_as_int(__ldg(nodes.bmin + k).w); };
+    int len = 1;
+    hs[0] = size_of(0);
+    hn[0] = 0;
+    while (len < kDualRoots) {
+        pop_heap(len);
+        const int k = hn[len - 1];
+        const int2 l = __ldg(nodes.link + k);
+        if (l.y >= 0) break;  // the largest node is a leaf
+        if (!(k + 1 < nn && l.x > k + 1 && l.x < nn)) {
+            atomicOr(err, (uint32_t) kErrTraverseLimit);
+            break;
+        }
+        len -= 1;
+        for (int c: {k + 1, l.x}) {
+            hs[len] = size_of(c);
+            hn[len] = c;
+            len += 1;
+            push_up(len - 1, 0, hs[len - 1], hn[len - 1]);
+        }
+    }
+    for (int i = 0; i < len; ++i) roots[i] = hn[i];
+    *num_roots = len;
+}
+
+}  // namespace
+
+void launch_dual_traverse(const DualNodes &nodes, const int *num_nodes, const float4 *bodies, int64_t n, float G,
+                          float eps, float theta, float4 *acc, unsigned long long *counts, DualWorkspace &ws,
+                          uint32_t *err, cudaStream_t s) {
+    if (n <= 0) return;
+    cudaMemsetAsync(acc, 0, (size_t) n * sizeof(float4), s);
+    load_balanced_break_kernel<<<1, 32, 0, s>>>(nodes, num_nodes, ws.roots, ws.num_roots, err);
+    dual_kernel<<<kDualRoots, kThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta, acc, counts,
+                                                ws.roots, ws.num_roots, ws.arena, (int) ws.arena_words, ws.tasks,
+                                                err);
+}
+
+int64_t dual_arena_words(int64_t n) {
+    // lists along one root-to-leaf path of the passive tree; grows with the body count
+    const int64_t w = 64 * n + (int64_t(1) << 16);
+    return std::min<int64_t>(std::max<int64_t>(w, int64_t(1) << 16), int64_t(1) << 23);
+}
+
+}  // namespace nbg

@@ -89,6 +89,7 @@ template<int ORDER>
 struct Summ {
     float bmin[3], bmax[3], com[3], M;
     float q[6];
+    float q3[ORDER >= 3 ? 10 : 1];
 };
 
 template<int ORDER>
@@ -98,7 +99,11 @@ __device__ __forceinline__ void store_slot(const TreeWorkspace &tw, int slot, co
     tw.scom[slot] = make_float4(s.com[0], s.com[1], s.com[2], s.M);
     if constexpr (ORDER >= 2) {
         tw.sq0[slot] = make_float4(s.q[0], s.q[1], s.q[2], s.q[3]);
-        tw.sq1[slot] = make_float4(s.q[4], s.q[5], 0.f, 0.f);
+        tw.sq1[slot] = make_float4(s.q[4], s.q[5], ORDER >= 3 ? s.q3[0] : 0.f, ORDER >= 3 ? s.q3[1] : 0.f);
+    }
+    if constexpr (ORDER >= 3) {
+        tw.sq2[slot] = make_float4(s.q3[2], s.q3[3], s.q3[4], s.q3[5]);
+        tw.sq3[slot] = make_float4(s.q3[6], s.q3[7], s.q3[8], s.q3[9]);
     }
 }
 
@@ -113,6 +118,12 @@ __device__ __forceinline__ Summ<ORDER> load_slot(const TreeWorkspace &tw, int sl
     if constexpr (ORDER >= 2) {
         float4 q0 = __ldcg(tw.sq0 + slot), q1 = __ldcg(tw.sq1 + slot);
         s.q[0] = q0.x; s.q[1] = q0.y; s.q[2] = q0.z; s.q[3] = q0.w; s.q[4] = q1.x; s.q[5] = q1.y;
+        if constexpr (ORDER >= 3) {
+            float4 q2 = __ldcg(tw.sq2 + slot), q3 = __ldcg(tw.sq3 + slot);
+            s.q3[0] = q1.z; s.q3[1] = q1.w;
+            s.q3[2] = q2.x; s.q3[3] = q2.y; s.q3[4] = q2.z; s.q3[5] = q2.w;
+            s.q3[6] = q3.x; s.q3[7] = q3.y; s.q3[8] = q3.z; s.q3[9] = q3.w;
+        }
     }
     return s;
 }
@@ -125,6 +136,41 @@ __device__ __forceinline__ void offset_quadrupole(float ox, float oy, float oz, 
     q[3] = fmul(fmul(oy, oy), m);
     q[4] = fmul(fmul(oy, oz), m);
     q[5] = fmul(fmul(oz, oz), m);
+}
+
+// Unique-slot dimensions of the order-3 packed tensor (XXX, XXY, XXZ, XYY, XYZ, XZZ, YYY, YYZ,
+// YZZ, ZZZ) and the order-2 slot of a sorted pair, as in SymmetricTensor3.h:372-395.
+__device__ __forceinline__ int slot2(int a, int b) { return a == 0 ? b : 3 + (a == 2) + (b == 2); }
+__device__ __forceinline__ void dims3(int L, int d[3]) {
+    const int t[10][3] = {{0, 0, 0}, {0, 0, 1}, {0, 0, 2}, {0, 1, 1}, {0, 1, 2},
+                          {0, 2, 2}, {1, 1, 1}, {1, 1, 2}, {1, 2, 2}, {2, 2, 2}};
+    d[0] = t[L][0]; d[1] = t[L][1]; d[2] = t[L][2];
+}
+__device__ __forceinline__ int slot2u(int a, int b) { return a <= b ? slot2(a, b) : slot2(b, a); }
+
+// Octupole term of one offset: outerProduct(outerProduct(d, d), d) (MultipoleMoment.h:46-62),
+// times the mass; t2 is the unscaled packed d (x) d.
+__device__ __forceinline__ void offset_octupole(const float t2[6], const float d[3], float m, float q3[10]) {
+#pragma unroll
+    for (int L = 0; L < 10; ++L) {
+        int dd[3];
+        dims3(L, dd);
+        q3[L] = fmul(fmul(t2[slot2(dd[0], dd[1])], d[dd[2]]), m);
+    }
+}
+
+// sumOfOuterProducts(T2, d) at each order-3 slot: right fold over the three left rotations of
+// the index (SymmetricTensor3.h:235-244, 483-488).
+__device__ __forceinline__ void sum_outer3(const float t2[6], const float d[3], float out[10]) {
+#pragma unroll
+    for (int L = 0; L < 10; ++L) {
+        int a[3];
+        dims3(L, a);
+        const float e0 = fmul(t2[slot2u(a[0], a[1])], d[a[2]]);
+        const float e1 = fmul(t2[slot2u(a[1], a[2])], d[a[0]]);
+        const float e2 = fmul(t2[slot2u(a[2], a[0])], d[a[1]]);
+        out[L] = fadd(e0, fadd(e1, e2));
+    }
 }
 
 template<int ORDER>
@@ -141,26 +187,40 @@ __device__ Summ<ORDER> leaf_summary(const float4 *__restrict__ bodies, int b, in
     cx = fdiv(cx, M); cy = fdiv(cy, M); cz = fdiv(cz, M);
     s.com[0] = cx; s.com[1] = cy; s.com[2] = cz; s.M = M;
     if constexpr (ORDER >= 2) {
-        float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        auto term = [&](int i, float q[6]) {
+        // moments of order 2 (and 3) of each body about the centre of mass, times its mass
+        constexpr int NQ = ORDER >= 3 ? 16 : 6;
+        float acc[NQ];
+#pragma unroll
+        for (int k = 0; k < NQ; ++k) acc[k] = 0.f;
+        auto term = [&](int i, float q[NQ]) {
             const float4 p = bodies[i];
-            offset_quadrupole(fsub(p.x, cx), fsub(p.y, cy), fsub(p.z, cz), p.w, q);
+            const float d[3] = {fsub(p.x, cx), fsub(p.y, cy), fsub(p.z, cz)};
+            offset_quadrupole(d[0], d[1], d[2], p.w, q);
+            if constexpr (ORDER >= 3) {
+                const float t2[6] = {fmul(d[0], d[0]), fmul(d[0], d[1]), fmul(d[0], d[2]),
+                                     fmul(d[1], d[1]), fmul(d[1], d[2]), fmul(d[2], d[2])};
+                offset_octupole(t2, d, p.w, q + 6);
+            }
         };
         int i = b;
         for (; e + 1 - i >= 4; i += 4) {
-            float f0[6], f1[6], f2[6], f3[6];
+            float f0[NQ], f1[NQ], f2[NQ], f3[NQ];
             term(i, f0); term(i + 1, f1); term(i + 2, f2); term(i + 3, f3);
 #pragma unroll
-            for (int k = 0; k < 6; ++k) acc[k] = fadd(acc[k], fadd(fadd(f0[k], f1[k]), fadd(f2[k], f3[k])));
+            for (int k = 0; k < NQ; ++k) acc[k] = fadd(acc[k], fadd(fadd(f0[k], f1[k]), fadd(f2[k], f3[k])));
         }
         for (; i <= e; ++i) {
-            float f[6];
+            float f[NQ];
             term(i, f);
 #pragma unroll
-            for (int k = 0; k < 6; ++k) acc[k] = fadd(acc[k], f[k]);
+            for (int k = 0; k < NQ; ++k) acc[k] = fadd(acc[k], f[k]);
         }
 #pragma unroll
         for (int k = 0; k < 6; ++k) s.q[k] = acc[k];
+        if constexpr (ORDER >= 3) {
+#pragma unroll
+            for (int k = 0; k < 10; ++k) s.q3[k] = acc[6 + k];
+        }
     }
     float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
     for (int i = b; i <= e; ++i) {
@@ -189,6 +249,26 @@ __device__ Summ<ORDER> internal_summary(const Summ<ORDER> &a, const Summ<ORDER> 
         offset_quadrupole(fsub(b.com[0], c[0]), fsub(b.com[1], c[1]), fsub(b.com[2], c[2]), b.M, qb);
 #pragma unroll
         for (int k = 0; k < 6; ++k) s.q[k] = fadd(fadd(0.f, fadd(qa[k], a.q[k])), fadd(qb[k], b.q[k]));
+        if constexpr (ORDER >= 3) {
+            // per child: (moment of the offset) * mass + child moment, plus sumOfOuterProducts(child
+            // quadrupole, offset) (MultipoleMassSummary.h:63-73)
+            float m3[2][10];
+            const Summ<ORDER> *cs[2] = {&a, &b};
+#pragma unroll
+            for (int ci = 0; ci < 2; ++ci) {
+                const Summ<ORDER> &ch = *cs[ci];
+                const float d[3] = {fsub(ch.com[0], c[0]), fsub(ch.com[1], c[1]), fsub(ch.com[2], c[2])};
+                const float t2[6] = {fmul(d[0], d[0]), fmul(d[0], d[1]), fmul(d[0], d[2]),
+                                     fmul(d[1], d[1]), fmul(d[1], d[2]), fmul(d[2], d[2])};
+                float o3[10], sop[10];
+                offset_octupole(t2, d, ch.M, o3);
+                sum_outer3(ch.q, d, sop);
+#pragma unroll
+                for (int k = 0; k < 10; ++k) m3[ci][k] = fadd(fadd(o3[k], ch.q3[k]), sop[k]);
+            }
+#pragma unroll
+            for (int k = 0; k < 10; ++k) s.q3[k] = fadd(fadd(0.f, m3[0][k]), m3[1][k]);
+        }
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -326,6 +406,66 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(int n, TreeWorkspace tw,
     if (i == 0) *tw.num_nodes = tw.cnt[i];
 }
 
+// Dual-tree node arrays (order 3 summaries): bounding box, centre of mass and mass, packed
+// quadrupole and octupole, links.
+__device__ void write_dual_record(const DualNodes &nodes, int pre, const Summ<3> &s, int first, int last,
+                                  int link0, int link1, uint32_t *err) {
+    if (pre < 0 || pre >= nodes.capacity) {
+        atomicOr(err, (uint32_t) kErrNodeOverflow);
+        return;
+    }
+    // diagonal length as BoundingBox::diagonalLength: sqrt((dx*dx + dy*dy) + dz*dz), IEEE operations
+    const float dx = fsub(s.bmax[0], s.bmin[0]), dy = fsub(s.bmax[1], s.bmin[1]), dz = fsub(s.bmax[2], s.bmin[2]);
+    const float diag = __fsqrt_rn(fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz)));
+    nodes.bmin[pre] = make_float4(s.bmin[0], s.bmin[1], s.bmin[2], __int_as_float(last - first + 1));
+    nodes.bmax[pre] = make_float4(s.bmax[0], s.bmax[1], s.bmax[2], diag);
+    nodes.com[pre] = make_float4(s.com[0], s.com[1], s.com[2], s.M);
+    float4 *q = nodes.q + (int64_t) pre * 4;
+    q[0] = make_float4(s.q[0], s.q[1], s.q[2], s.q[3]);
+    q[1] = make_float4(s.q[4], s.q[5], s.q3[0], s.q3[1]);
+    q[2] = make_float4(s.q3[2], s.q3[3], s.q3[4], s.q3[5]);
+    q[3] = make_float4(s.q3[6], s.q3[7], s.q3[8], s.q3[9]);
+    nodes.link[pre] = make_int2(link0, link1);
+}
+
+__global__ void __launch_bounds__(kThreads) emit_dual_kernel(int n, TreeWorkspace tw, DualNodes nodes, uint32_t *err) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1 || !tw.splittable[i]) return;
+    int pre = 0;
+    int depth = 0;
+    for (int u = i; u != 0; ++depth) {
+        const int p = tw.parent[u];
+        if (depth >= kMaxTreeDepth || p < 0 || p >= n - 1) {
+            atomicOr(err, (uint32_t) kErrTreeDepth);
+            return;
+        }
+        pre += 1;
+        if (tw.right[p] == u) pre += tw.cnt[slot_of(tw.left[p], n)];
+        u = p;
+    }
+    const int lc = tw.left[i], rc = tw.right[i];
+    const int lslot = slot_of(lc, n);
+    const int right_pre = pre + 1 + tw.cnt[lslot];
+    const int2 ri = tw.range[i];
+    write_dual_record(nodes, pre, load_slot<3>(tw, i), ri.x, ri.y, right_pre, -1 - ri.x, err);
+    if (is_final_leaf(tw.splittable, lc)) {
+        int2 r = lc < 0 ? make_int2(~lc, ~lc) : tw.range[lc];
+        write_dual_record(nodes, pre + 1, load_slot<3>(tw, lslot), r.x, r.y, r.x, r.y + 1, err);
+    }
+    if (is_final_leaf(tw.splittable, rc)) {
+        int2 r = rc < 0 ? make_int2(~rc, ~rc) : tw.range[rc];
+        write_dual_record(nodes, right_pre, load_slot<3>(tw, slot_of(rc, n)), r.x, r.y, r.x, r.y + 1, err);
+    }
+    if (i == 0) *tw.num_nodes = tw.cnt[i];
+}
+
+__global__ void root_leaf_dual_kernel(const float4 *__restrict__ bodies, int n, TreeWorkspace tw, DualNodes nodes,
+                                      uint32_t *err) {
+    if (n > 1 && tw.splittable[0]) return;
+    write_dual_record(nodes, 0, leaf_summary<3>(bodies, 0, n - 1), 0, n - 1, 0, n, err);
+    *tw.num_nodes = 1;
+}
+
 // The whole tree is one leaf when n == 1, or when the root is not splittable (n <= maxLeafSize
 // or every code equal).
 template<int ORDER>
@@ -338,6 +478,25 @@ __global__ void root_leaf_kernel(const float4 *__restrict__ bodies, int n, TreeW
 }
 
 }  // namespace
+
+void launch_build_dual_tree(const uint64_t *sorted_codes, const float4 *bodies, int64_t n64, int leaf, TreeWorkspace &tw,
+                            const DualNodes &nodes, uint32_t *err, cudaStream_t s) {
+    const int n = (int) n64;
+    if (n <= 0) {
+        cudaMemsetAsync(tw.num_nodes, 0, sizeof(int), s);
+        return;
+    }
+    const int internal = n - 1;
+    const int blocks = internal > 0 ? (internal + kThreads - 1) / kThreads : 1;
+    if (internal > 0) {
+        karras_kernel<<<blocks, kThreads, 0, s>>>(sorted_codes, nullptr, n, leaf, tw.range, tw.left, tw.right,
+                                                  tw.parent, tw.splittable);
+        cudaMemsetAsync(tw.visit, 0, (size_t) internal * sizeof(int), s);
+        summarize_kernel<3><<<blocks, kThreads, 0, s>>>(bodies, n, tw, err);
+        emit_dual_kernel<<<blocks, kThreads, 0, s>>>(n, tw, nodes, err);
+    }
+    root_leaf_dual_kernel<<<1, 1, 0, s>>>(bodies, n, tw, nodes, err);
+}
 
 void launch_build_tree(const uint64_t *sorted_codes, const float4 *bodies, int64_t n64, int leaf, int order,
                        float theta, TreeWorkspace &tw, const NodeArrays &nodes, uint32_t *err, cudaStream_t s,

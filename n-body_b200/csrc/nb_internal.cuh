@@ -108,6 +108,7 @@ enum DeviceError : uint32_t {
     kErrNodeOverflow = 1u << 2,      // more tree nodes than the node buffer holds
     kErrStackOverflow = 1u << 3,     // traversal stack full (a push was dropped)
     kErrTraverseLimit = 1u << 4,     // traversal met an invalid link or exceeded its round limit
+    kErrDualArena = 1u << 5,         // dual-tree list or task storage exhausted
 };
 
 // ---- launchers (stream-ordered; defined in the .cu files) ----
@@ -159,6 +160,7 @@ struct TreeWorkspace {
     int *visit = nullptr;           // n-1 arrival counters
     float4 *sbmin = nullptr, *sbmax = nullptr, *scom = nullptr;  // 2n-1 summary slots
     float4 *sq0 = nullptr, *sq1 = nullptr;                        // quadrupole slots (order >= 2)
+    float4 *sq2 = nullptr, *sq3 = nullptr;                        // octupole slots (order 3)
     int *cnt = nullptr;             // subtree node count per slot
     int *num_nodes = nullptr;       // device scalar: final node count
     int64_t capacity = 0;
@@ -166,6 +168,34 @@ struct TreeWorkspace {
 void launch_build_tree(const uint64_t *sorted_codes, const float4 *bodies, int64_t n, int leaf, int order, float theta,
                        TreeWorkspace &tw, const NodeArrays &nodes, uint32_t *err, cudaStream_t s,
                        const BatchSegments &seg = BatchSegments());
+
+// Dual-tree node arrays (preorder): bmin = (min.xyz, body count as int bits), bmax = (max.xyz,
+// diagonal length as BoundingBox::diagonalLength computes it),
+// com = (centre of mass, mass), q = 4 float4 per node: Q2 (6) then Q3 (10);
+// link = (first body, end body) at a leaf, (right child, -1 - first body) at an internal node.
+struct DualNodes {
+    float4 *bmin = nullptr, *bmax = nullptr, *com = nullptr, *q = nullptr;
+    int2 *link = nullptr;
+    int64_t capacity = 0;
+};
+void launch_build_dual_tree(const uint64_t *sorted_codes, const float4 *bodies, int64_t n, int leaf, TreeWorkspace &tw,
+                            const DualNodes &nodes, uint32_t *err, cudaStream_t s);
+
+// dualtree.cu
+constexpr int kDualRoots = 256;   // starting passive nodes (Tree::loadBalancedBreak(256))
+constexpr int kDualTasks = 4096;  // task records per block
+struct DualWorkspace {
+    int *roots = nullptr;           // starting passive nodes (at most kDualRoots)
+    int *num_roots = nullptr;
+    int *arena = nullptr;           // per block: arena_words words of lists and local fields
+    int *tasks = nullptr;           // per block: kDualTasks task records of 6 ints
+    int64_t arena_words = 0;
+};
+// Arena words per block for n bodies.
+int64_t dual_arena_words(int64_t n);
+void launch_dual_traverse(const DualNodes &nodes, const int *num_nodes, const float4 *bodies, int64_t n, float G,
+                          float eps, float theta, float4 *acc, unsigned long long *counts, DualWorkspace &ws,
+                          uint32_t *err, cudaStream_t s);
 
 // traverse.cu
 struct TraverseWorkspace {

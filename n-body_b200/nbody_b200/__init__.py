@@ -37,6 +37,7 @@ _STATUS = {
 
 SOLVER_LINEAR_BVH = 0
 SOLVER_NAIVE = 1
+SOLVER_DUAL_LINEAR_BVH = 2
 
 
 class NBodyError(RuntimeError):
@@ -397,6 +398,20 @@ class NaiveSolver(Solver):
     _solver_kind = SOLVER_NAIVE
 
 
+class MultipoleImplicitLinearBVHFMMSolver(Solver):
+    """MultipoleImplicitLinearBVHFMMSolver<Order> (ImplicitLinearBVHFMMSolver.h:15-38): dual-tree
+    traversal of the linear BVH against itself under DiagonalOverSeparation, with implicit local
+    fields of order Order + 1. Order 3 (octupole, "implicit-linear-bvh-fmm-8p") runs on the GPU."""
+
+    _solver_kind = SOLVER_DUAL_LINEAR_BVH
+    _order = 3
+    _default_theta = 0.5  # ThetaDescentCriterion's default (DescentCriterionType.h:53)
+
+
+class OctupoleImplicitLinearBVHFMMSolver(MultipoleImplicitLinearBVHFMMSolver):
+    _order = 3
+
+
 class Server:
     """Continuous-batching server of independent simulations (nb_server_*)."""
 
@@ -487,6 +502,25 @@ def decode_records(records: np.ndarray, order: int) -> dict:
     if order == 2:
         out["quadrupole"] = np.ascontiguousarray(r[:, 12:18])
     return out
+
+
+def decode_dual_records(records: np.ndarray) -> dict:
+    """Split the dual solver's node records (32 floats per node) into named fields: bounding box,
+    body count, diagonal length, centre of mass and mass, link (2 int32: leaf = body range,
+    internal = right child's preorder index and -1 - first body), quadrupole (6) and octupole (10)
+    in the reference's packed layout."""
+    r = np.ascontiguousarray(records, np.float32)
+    return {
+        "bmin": r[:, 0:3],
+        "size": np.ascontiguousarray(r[:, 3]).view(np.int32),
+        "bmax": r[:, 4:7],
+        "diag": r[:, 7],
+        "com": r[:, 8:11],
+        "mass": r[:, 11],
+        "link": np.ascontiguousarray(r[:, 12:14]).view(np.int32),
+        "quadrupole": np.ascontiguousarray(r[:, 16:22]),
+        "octupole": np.ascontiguousarray(r[:, 22:32]),
+    }
 
 
 from . import scenarios  # noqa: E402  (host-side scenario generators)

@@ -32,6 +32,7 @@
 
 #include <omp.h>
 
+#include "dualtree.h"
 #include "physics.h"
 
 using namespace oracle;
@@ -598,6 +599,68 @@ void or_tensor2_times_vector(const float *t2, const float *v, float *out) {
     for (int i = 0; i < 6; ++i) t.v[i] = t2[i];
     vec3 r = contract_down(t, {v[0], v[1], v[2]});
     out[0] = r.x; out[1] = r.y; out[2] = r.z;
+}
+
+}  // extern "C"
+
+namespace {
+template<int Order>
+int64_t dual_accelerations(int64_t n, const float *pm, float G, float eps, float theta, int32_t leaf, float *acc,
+                           uint64_t *counts, int32_t threads) {
+    float box[6];
+    or_bbox(n, pm, box);
+    std::vector<uint64_t> codes((size_t) n), sorted((size_t) n);
+    std::vector<uint32_t> perm((size_t) n);
+    or_morton(n, pm, box, codes.data());
+    sort_codes(n, codes.data(), perm.data());
+    std::vector<float> pms((size_t) n * 4);
+    for (int64_t k = 0; k < n; ++k) {
+        sorted[k] = codes[perm[k]];
+        std::memcpy(&pms[4 * k], pm + 4 * (int64_t) perm[k], 16);
+    }
+    Tree t;
+    t.begin.reserve(2 * n);
+    build_node(t, sorted.data(), 0, (int32_t) n, leaf);
+    std::vector<Summary<Order>> s = summarize_tree<Order>(t, pms.data());
+    const int64_t nn = (int64_t) t.begin.size();
+    std::vector<dual::Node<Order>> nodes((size_t) nn);
+    for (int64_t k = 0; k < nn; ++k) {
+        auto &d = nodes[k];
+        d.begin = t.begin[k]; d.end = t.end[k]; d.left = t.left[k]; d.right = t.right[k];
+        d.box = {s[k].bmin, s[k].bmax};
+        d.com = s[k].com; d.mass = s[k].mass; d.mp = s[k].mp;
+    }
+    std::vector<float> accs((size_t) n * 4, 0.f);
+    std::vector<int32_t> roots = dual::load_balanced_break<Order>(nodes, 256);
+    uint64_t tot[4] = {0, 0, 0, 0};
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel
+    {
+        uint64_t local[4] = {0, 0, 0, 0};
+        dual::DualSolver<Order> solver{nodes, pms.data(), accs.data(), Gravity{G, eps}, dual::Criterion{theta}, local};
+#pragma omp for schedule(dynamic, 1)
+        for (int64_t r = 0; r < (int64_t) roots.size(); ++r) solver.balanced(roots[r]);
+#pragma omp critical
+        for (int k = 0; k < 4; ++k) tot[k] += local[k];
+    }
+    for (int64_t k = 0; k < n; ++k) std::memcpy(acc + 4 * (int64_t) perm[k], &accs[4 * k], 16);
+    if (counts) for (int k = 0; k < 4; ++k) counts[k] = tot[k];
+    return nn;
+}
+}  // namespace
+
+extern "C" {
+
+// MultipoleImplicitLinearBVHFMMSolver<order> accelerations (order 1..3; the local field has order
+// order+1), in input order. counts = {particle-particle, node-particle, particle-node, node-node}.
+int64_t or_dual_accelerations(int64_t n, const float *pm, float G, float eps, float theta, int32_t leaf, int32_t order,
+                              float *acc, uint64_t *counts, int32_t threads) {
+    if (n <= 0) return 0;
+    switch (order) {
+        case 2: return dual_accelerations<2>(n, pm, G, eps, theta, leaf, acc, counts, threads);
+        case 3: return dual_accelerations<3>(n, pm, G, eps, theta, leaf, acc, counts, threads);
+        default: return -1;
+    }
 }
 
 int32_t or_max_threads(void) { return omp_get_max_threads(); }

@@ -58,6 +58,7 @@ def lib() -> C.CDLL:
             "or_particle_node": (C.c_int, [i32, f32, f32, _f32p, f32, _f32p, _f32p]),
             "or_field_at": (C.c_int, [i32, _f32p, _f32p, _f32p]),
             "or_field_translated": (C.c_int, [i32, _f32p, _f32p, _f32p]),
+            "or_dual_accelerations": (i64, [i64, _f32p, f32, f32, f32, i32, i32, _f32p, _u64p, i32]),
             "or_tensor_linear_index": (i32, [i32, _i32p]),
             "or_tensor_dimensional_index": (C.c_int, [i32, i32, _i32p]),
             "or_tensor_lexicographic_index": (C.c_int, [i32, i32, _i32p]),
@@ -140,6 +141,17 @@ def bh_targets(pm, targets, G=1.0, eps=1e-5, theta=0.5, leaf=16, order=1, thread
     acc = np.zeros((len(targets), 4), np.float32)
     counts = np.zeros(2, np.uint64)
     nn = lib().or_bh_targets(len(pm), pm, len(targets), targets, G, eps, theta, leaf, order, acc, counts, threads)
+    assert nn >= 0
+    return acc, counts
+
+
+def dual_accelerations(pm, G=1.0, eps=1e-5, theta=0.4, leaf=64, order=3, threads=0):
+    """MultipoleImplicitLinearBVHFMMSolver<order> (dual-tree, implicit local field of order+1):
+    accelerations in input order and the (pp, np, pn, nn) interaction counts."""
+    pm = _bodies(pm)
+    acc = np.zeros((len(pm), 4), np.float32)
+    counts = np.zeros(4, np.uint64)
+    nn = lib().or_dual_accelerations(len(pm), pm, G, eps, theta, leaf, order, acc, counts, threads)
     assert nn >= 0
     return acc, counts
 
