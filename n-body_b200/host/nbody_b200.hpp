@@ -1,0 +1,283 @@
+// C++ host interface of the B200 force path: the reference's Solver / Gravity / Simulation
+// surface (NBody::Solver<Rule>, src/NBody/Simulation/Solver.h:26-187; NBody::Physics::Gravity,
+// src/NBody/Physics/Rules/Gravity.h:187-410; NBody::Simulation, src/NBody/Simulation/Simulation.h)
+// over the C ABI in include/nbody_gpu.h. Header-only; link with libnbody_b200.so.
+//
+// Differences from the reference, by design:
+//   - Simulation holds plain arrays (positions, velocities, masses, accelerations in particle
+//     order) instead of an EnTT registry; the reference's views map onto them one to one.
+//   - Errors raise nbody_b200::Error (the reference asserts or logs, MultiSolver.h:86, 104-105).
+//   - step() keeps the bodies on the device between calls and copies them back once per call;
+//     step(n) runs n steps on the device with a single copy back (the device-resident fast path).
+//   - There is no CPU fallback: constructing a solver without an sm_100 device throws.
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/nbody_gpu.h"
+
+namespace nbody_b200 {
+
+class Error : public std::runtime_error {
+public:
+    Error(int status, const std::string &what) : std::runtime_error(what), _status(status) {}
+    int status() const { return _status; }
+
+private:
+    int _status;
+};
+
+struct vec3 {
+    float x = 0.f, y = 0.f, z = 0.f;
+    friend bool operator==(const vec3 &a, const vec3 &b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
+};
+
+// Gravity rule: G and the softening epsilon added to r^2 (Gravity.h:195, 207, 407-409).
+class Gravity {
+public:
+    explicit Gravity(float G = 1.0f, float epsilon = 0.00001f) : _G(G), _epsilon(epsilon) {}
+    float &g() { return _G; }
+    const float &g() const { return _G; }
+    float &epsilon() { return _epsilon; }
+    const float &epsilon() const { return _epsilon; }
+
+private:
+    float _G, _epsilon;
+};
+
+// The bodies of a simulation in particle order. Particles without an acceleration component in
+// the reference (inactive as passive) are not modelled: every particle is active and passive.
+class Simulation {
+public:
+    std::vector<vec3> position, velocity, acceleration;
+    std::vector<float> mass;
+
+    std::size_t particleCount() const { return position.size(); }
+
+    std::size_t newParticle(vec3 p, vec3 v, float m) {
+        position.push_back(p);
+        velocity.push_back(v);
+        mass.push_back(m);
+        acceleration.push_back({});
+        return position.size() - 1;
+    }
+
+    void clear() {
+        position.clear();
+        velocity.clear();
+        acceleration.clear();
+        mass.clear();
+    }
+
+    // 4 floats per body, as the C ABI takes them
+    std::vector<float> packedPositionMass() const {
+        std::vector<float> out(4 * particleCount());
+        for (std::size_t i = 0; i < particleCount(); ++i) {
+            out[4 * i] = position[i].x;
+            out[4 * i + 1] = position[i].y;
+            out[4 * i + 2] = position[i].z;
+            out[4 * i + 3] = mass[i];
+        }
+        return out;
+    }
+    std::vector<float> packedVelocity() const {
+        std::vector<float> out(4 * particleCount(), 0.f);
+        for (std::size_t i = 0; i < particleCount(); ++i) {
+            out[4 * i] = velocity[i].x;
+            out[4 * i + 1] = velocity[i].y;
+            out[4 * i + 2] = velocity[i].z;
+        }
+        return out;
+    }
+    void unpackPositionMass(const std::vector<float> &pm) {
+        for (std::size_t i = 0; i < particleCount(); ++i) {
+            position[i] = {pm[4 * i], pm[4 * i + 1], pm[4 * i + 2]};
+            mass[i] = pm[4 * i + 3];
+        }
+    }
+    void unpackVelocity(const std::vector<float> &v) {
+        for (std::size_t i = 0; i < particleCount(); ++i) velocity[i] = {v[4 * i], v[4 * i + 1], v[4 * i + 2]};
+    }
+    void unpackAcceleration(const std::vector<float> &a) {
+        for (std::size_t i = 0; i < particleCount(); ++i) acceleration[i] = {a[4 * i], a[4 * i + 1], a[4 * i + 2]};
+    }
+};
+
+// Interaction counts (SimpleTrackingRule's convention, SimpleTrackingRule.h:29-51).
+struct InteractionCounts {
+    uint64_t particleParticle = 0, particleNode = 0, nodeParticle = 0, nodeNode = 0;
+};
+
+// Solver<Rule> (Solver.h:26-187) over one device context. The subclasses fix the algorithm.
+class Solver {
+public:
+    Solver(const Solver &) = delete;
+    Solver &operator=(const Solver &) = delete;
+    virtual ~Solver() {
+        if (_ctx) nb_destroy(_ctx);
+    }
+
+    // Solver::id / name (Solver.h:89-91), as the reference formats them
+    std::string id() const { return nb_solver_id(_ctx); }
+    std::string name() const { return nb_solver_name(_ctx); }
+
+    // ActiveTreeSolver::theta (ActiveTreeSolver.h:78-80) / DiagonalOverSeparation::theta
+    float theta() const { return config().theta; }
+    void setTheta(float t) { update([&](nb_config &c) { c.theta = t; }); }
+    // LinearBVH::maxLeafSize (LinearBVH.h:135-137)
+    int maxLeafSize() const { return config().max_leaf_size; }
+    void setMaxLeafSize(int l) { update([&](nb_config &c) { c.max_leaf_size = l; }); }
+    // Solver::timeStep (Solver.h:101); per solver here rather than a static
+    float timeStep() const { return config().time_step; }
+    void setTimeStep(float dt) { update([&](nb_config &c) { c.time_step = dt; }); }
+
+    Simulation &simulation() { return _sim; }
+    Gravity &rule() { return _rule; }
+
+    // Solver::updateAccelerations (ActiveTreeSolver.h:33-72 / ImplicitDualTraversalSolver.h:42-69):
+    // accelerations of the simulation's current bodies, written to simulation().acceleration.
+    void updateAccelerations() {
+        upload();
+        std::vector<float> acc(4 * _sim.particleCount());
+        check(nb_update_accelerations(_ctx, acc.empty() ? nullptr : acc.data()));
+        _sim.unpackAcceleration(acc);
+    }
+
+    // Solver::step (Solver.h:103-113): accelerations, then v += a dt and x += v dt.
+    // step(n) runs n steps on the device and copies the bodies back once.
+    void step(int n = 1) {
+        upload();
+        check(nb_step(_ctx, n));
+        download();
+    }
+
+    InteractionCounts counts() const {
+        nb_counts c{};
+        check(nb_get_counts(_ctx, &c));
+        return {c.particle_particle, c.particle_node, c.node_particle, c.node_node};
+    }
+
+    // Forces the next call to copy the simulation's bodies to the device (call after editing them).
+    void invalidate() { _uploaded_count = SIZE_MAX; }
+
+    nb_ctx *handle() const { return _ctx; }
+
+protected:
+    Solver(Simulation &sim, Gravity &rule, int32_t solver, int32_t order, float theta)
+        : _sim(sim), _rule(rule) {
+        nb_config c;
+        nb_config_default(&c);
+        c.solver = solver;
+        c.order = order;
+        c.theta = theta;
+        c.G = rule.g();
+        c.epsilon = rule.epsilon();
+        int rc = nb_create(&c, &_ctx);
+        if (rc != NB_OK) throw Error(rc, "nb_create failed: no usable sm_100 device or invalid configuration");
+    }
+
+private:
+    template<typename F>
+    void update(F &&f) {
+        nb_config c = config();
+        f(c);
+        check(nb_set_config(_ctx, &c));
+    }
+    nb_config config() const {
+        nb_config c{};
+        check(nb_get_config(_ctx, &c));
+        return c;
+    }
+    void check(int rc) const {
+        if (rc != NB_OK) throw Error(rc, nb_last_error(_ctx));
+    }
+    // The rule's constants and the bodies go to the device when they changed on the host.
+    void upload() {
+        nb_config c = config();
+        if (c.G != _rule.g() || c.epsilon != _rule.epsilon()) {
+            c.G = _rule.g();
+            c.epsilon = _rule.epsilon();
+            check(nb_set_config(_ctx, &c));
+        }
+        if (_uploaded_count == _sim.particleCount() && !changed()) return;
+        std::vector<float> pm = _sim.packedPositionMass(), v = _sim.packedVelocity();
+        check(nb_set_bodies(_ctx, (int64_t) _sim.particleCount(), pm.empty() ? nullptr : pm.data(),
+                            v.empty() ? nullptr : v.data()));
+        _uploaded_count = _sim.particleCount();
+        _shadow_pm = std::move(pm);
+        _shadow_v = std::move(v);
+    }
+    void download() {
+        const std::size_t n = _sim.particleCount();
+        std::vector<float> pm(4 * n), v(4 * n), a(4 * n);
+        check(nb_get_bodies(_ctx, n ? pm.data() : nullptr, n ? v.data() : nullptr));
+        check(nb_get_accelerations(_ctx, n ? a.data() : nullptr));
+        _sim.unpackPositionMass(pm);
+        _sim.unpackVelocity(v);
+        _sim.unpackAcceleration(a);
+        _shadow_pm = std::move(pm);
+        _shadow_v = std::move(v);
+    }
+    // Host edits since the last transfer (positions, masses or velocities)
+    bool changed() const { return _sim.packedPositionMass() != _shadow_pm || _sim.packedVelocity() != _shadow_v; }
+
+    Simulation &_sim;
+    Gravity &_rule;
+    nb_ctx *_ctx = nullptr;
+    std::size_t _uploaded_count = SIZE_MAX;
+    std::vector<float> _shadow_pm, _shadow_v;
+};
+
+// LinearBVHSolver (LinearBVHSolver.h:18-31): centre-of-mass summaries, "linear-bvh"
+class LinearBVHSolver : public Solver {
+public:
+    LinearBVHSolver(Simulation &sim, Gravity &rule) : Solver(sim, rule, NB_SOLVER_LINEAR_BVH, 1, 0.3f) {}
+};
+
+// MultipoleLinearBVHSolver<Order> (LinearBVHSolver.h:33-44); order 2 runs on the GPU
+template<int Order>
+class MultipoleLinearBVHSolver : public Solver {
+    static_assert(Order == 2, "the device path implements the quadrupole (order 2) linear BVH");
+
+public:
+    MultipoleLinearBVHSolver(Simulation &sim, Gravity &rule) : Solver(sim, rule, NB_SOLVER_LINEAR_BVH, Order, 0.3f) {}
+};
+using QuadrupoleLinearBVHSolver = MultipoleLinearBVHSolver<2>;
+
+// NaiveSolver (NaiveSolver.h:12-53): FP32 direct sum, "naive"
+class NaiveSolver : public Solver {
+public:
+    NaiveSolver(Simulation &sim, Gravity &rule) : Solver(sim, rule, NB_SOLVER_NAIVE, 1, 0.3f) {}
+};
+
+// MultipoleImplicitLinearBVHFMMSolver<Order> (ImplicitLinearBVHFMMSolver.h:15-38); order 3 runs on the GPU
+template<int Order>
+class MultipoleImplicitLinearBVHFMMSolver : public Solver {
+    static_assert(Order == 3, "the device dual-tree path implements octupole moments (order 3)");
+
+public:
+    // theta defaults to ThetaDescentCriterion's 0.5 (DescentCriterionType.h:53)
+    MultipoleImplicitLinearBVHFMMSolver(Simulation &sim, Gravity &rule)
+        : Solver(sim, rule, NB_SOLVER_DUAL_LINEAR_BVH, Order, 0.5f) {}
+};
+using OctupoleImplicitLinearBVHFMMSolver = MultipoleImplicitLinearBVHFMMSolver<3>;
+
+// MultiSolver::select (MultiSolver.h:79-87): a solver by its id.
+inline std::unique_ptr<Solver> makeSolver(const std::string &id, Simulation &sim, Gravity &rule) {
+    if (id == "linear-bvh") return std::make_unique<LinearBVHSolver>(sim, rule);
+    if (id == "linear-bvh-4p") return std::make_unique<QuadrupoleLinearBVHSolver>(sim, rule);
+    if (id == "naive") return std::make_unique<NaiveSolver>(sim, rule);
+    if (id == "implicit-linear-bvh-fmm-8p") return std::make_unique<OctupoleImplicitLinearBVHFMMSolver>(sim, rule);
+    throw Error(NB_ERR_INVALID_ARGUMENT, "unknown solver id: " + id);
+}
+
+inline std::vector<std::string> solverIds() {
+    return {"linear-bvh", "linear-bvh-4p", "naive", "implicit-linear-bvh-fmm-8p"};
+}
+
+}  // namespace nbody_b200

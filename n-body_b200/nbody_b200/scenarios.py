@@ -116,3 +116,50 @@ def softening_to_epsilon(softening_length: float) -> float:
     """A configured softening length e enters the reference's Gravity as epsilon = e^2, since
     Gravity adds epsilon to r^2 (Gravity.h:207)."""
     return float(np.float32(softening_length) * np.float32(softening_length))
+
+
+def write_json(path: str, bodies, velocities=None, G: float | None = None, accelerations=None) -> None:
+    """A scenario in the reference's JSON schema (NBody::to_json, Simulation.cpp:154-185):
+    {"G": G (optional), "particles": [{"position", "velocity", "mass", "acceleration"}]}.
+    Floats are written with 9 significant digits, which read back to the same float32."""
+    import json
+
+    pm = np.asarray(bodies, np.float32)
+    vel = np.zeros_like(pm) if velocities is None else np.asarray(velocities, np.float32)
+    acc = None if accelerations is None else np.asarray(accelerations, np.float32)
+
+    def v3(a):
+        return {"x": float(a[0]), "y": float(a[1]), "z": float(a[2])}
+
+    parts = []
+    for i in range(len(pm)):
+        p = {"position": v3(pm[i]), "velocity": v3(vel[i]), "mass": float(pm[i, 3])}
+        if acc is not None:
+            p["acceleration"] = v3(acc[i])
+        parts.append(p)
+    root = {"particles": parts}
+    if G is not None:
+        root = {"G": float(np.float32(G)), **root}
+    with open(path, "w") as f:
+        json.dump(root, f)
+
+
+def read_json(path: str):
+    """(bodies, velocities, accelerations, G or None) of a JSON scenario (NBody::from_json,
+    Simulation.cpp:187-228): missing vectors read as zero, a missing mass as 0."""
+    import json
+
+    with open(path) as f:
+        root = json.load(f)
+    parts = root["particles"]
+    n = len(parts)
+    pm = np.zeros((n, 4), np.float32)
+    vel = np.zeros((n, 4), np.float32)
+    acc = np.zeros((n, 4), np.float32)
+    for i, p in enumerate(parts):
+        for key, arr in (("position", pm), ("velocity", vel), ("acceleration", acc)):
+            if key in p:
+                arr[i, :3] = (p[key]["x"], p[key]["y"], p[key]["z"])
+        pm[i, 3] = p.get("mass", 0.0)
+    G = root.get("G")
+    return pm, vel, acc, (None if G is None else float(G))

@@ -1,0 +1,54 @@
+"""The C++ host layer (n-body_b200/host/nbody_b200.hpp) through its command-line runner, on a GPU.
+
+The C++ Solver classes drive the same C ABI as the Python binding, so a scenario stepped by
+nbody_cli must end bit-identical to the same steps through the binding, with the same
+interaction counts.
+"""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import REPO
+
+pytestmark = pytest.mark.gpu
+
+CLI = os.path.join(REPO, "n-body_b200", "lib", "nbody_cli")
+
+
+def run(*args):
+    r = subprocess.run([CLI, *args], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    return r
+
+
+@pytest.mark.parametrize("solver_id,cls,theta,leaf,steps", [
+    ("linear-bvh", "LinearBVHSolver", 0.5, 16, 3),
+    ("linear-bvh-4p", "QuadrupoleLinearBVHSolver", 0.5, 16, 4),
+    ("naive", "NaiveSolver", 0.5, 16, 2),
+    ("implicit-linear-bvh-fmm-8p", "OctupoleImplicitLinearBVHFMMSolver", 0.4, 64, 2),
+])
+def test_cli_matches_binding(tmp_path, nb, solver_id, cls, theta, leaf, steps):
+    pm, vel = nb.scenarios.plummer(6000, seed=17)
+    src = tmp_path / "in.json"
+    nb.scenarios.write_json(str(src), pm, vel, G=1.5)
+    out = tmp_path / "out.json"
+    r = run("-s", solver_id, "-i", str(steps), "-t", "0.001", "--theta", str(theta), "--max-leaf-size", str(leaf),
+            "--epsilon", "0.0001", "-o", str(out), "--counts", str(src))
+    counts = json.loads(r.stdout.strip().splitlines()[-1])
+    assert counts["solver"] == solver_id
+    p_cli, v_cli, a_cli, G = nb.scenarios.read_json(str(out))
+    assert G == np.float32(1.5)
+    with getattr(nb, cls)(bodies=pm, velocities=vel, rule=nb.Gravity(1.5, 1e-4), theta=theta, max_leaf_size=leaf,
+                          time_step=1e-3) as s:
+        s.step(steps)
+        p_ref, v_ref = s.bodies()
+        a_ref = s.accelerations()
+        c_ref = s.counts()
+    assert np.array_equal(p_cli, p_ref)
+    assert np.array_equal(v_cli[:, :3], v_ref[:, :3])
+    assert np.array_equal(a_cli[:, :3], a_ref[:, :3])
+    for k in ("particle_particle", "particle_node", "node_particle", "node_node"):
+        assert counts[k] == c_ref[k], k
