@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--duration", type=float, default=20.0, help="serving: seconds of arrivals per run")
     ap.add_argument("--rate", type=float, default=40.0, help="serving: arrivals per second (open loop)")
     ap.add_argument("--instances", type=int, default=256)
+    ap.add_argument("--shard-targets", action="store_true",
+                    help="N>1: one instance sharded over the ranks' targets with an NCCL all-gather of "
+                         "positions and velocities per step (strong scaling) instead of one instance per rank")
     return ap.parse_args()
 
 
@@ -252,7 +255,11 @@ def run_ours(args):
     # A dedicated (non-default) stream shared by the solver, the L2 flush and the timing events.
     stream = torch.cuda.Stream(device)
     with torch.cuda.stream(stream):
-        line = _run_ours_on_stream(args, torch, nb, pm, vel, eps, stream, world, rank, device)
+        if args.shard_targets and world > 1:
+            pm, vel = scenarios.plummer(args.n, seed=SEED)  # one instance, the same on every rank
+            line = _run_sharded_on_stream(args, torch, nb, pm, vel, eps, stream, world, rank, device)
+        else:
+            line = _run_ours_on_stream(args, torch, nb, pm, vel, eps, stream, world, rank, device)
     if world > 1:
         torch.distributed.destroy_process_group()
     if rank == 0:
@@ -367,6 +374,73 @@ def _run_ours_on_stream(args, torch, nb, pm, vel, eps, stream, world, rank, devi
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(pm, eps)
     return line
+
+
+def _run_sharded_on_stream(args, torch, nb, pm, vel, eps, stream, world, rank, device):
+    """One instance of args.n bodies advanced by all ranks: each evaluates its slice of the
+    Morton-ordered targets, then an NCCL in-place all-gather of positions and velocities."""
+    solver = nb.QuadrupoleLinearBVHSolver(rule=nb.Gravity(1.0, eps), theta=THETA, max_leaf_size=LEAF,
+                                          time_step=DT, device=device)
+    solver.set_stream(stream.cuda_stream)
+    solver.set_shard(rank, world)
+    solver.set_bodies(pm, vel)
+    stepper = nb.ShardedStepper(solver)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    for _ in range(max(args.warmup, 3)):
+        flush_l2(flush)
+        stepper.step(1)
+    torch.cuda.synchronize(device)
+    solver.enable_timing(True)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    torch.distributed.barrier()
+    torch.cuda.synchronize(device)
+    with Clocks(device) as clk:
+        for k in range(args.steps):
+            flush_l2(flush)
+            starts[k].record(stream)
+            stepper.step(1)
+            ends[k].record(stream)
+        torch.cuda.synchronize(device)
+    torch.distributed.barrier()
+    step_ms = float(sum(a.elapsed_time(b) for a, b in zip(starts, ends)))
+    phases = solver.phase_times()
+    solver.enable_timing(False)
+    lib = nb.lib()
+    h_pm = torch.from_numpy(pm.copy()).pin_memory()
+    h_vel = torch.from_numpy(vel.copy()).pin_memory()
+    out_pm = torch.empty_like(h_pm).pin_memory()
+    out_vel = torch.empty_like(h_vel).pin_memory()
+    torch.distributed.barrier()
+    e2e_s = 0.0
+    for _ in range(args.e2e_steps):
+        t0 = time.perf_counter()
+        solver._check(lib.nb_set_bodies(solver.handle, args.n, h_pm.data_ptr(), h_vel.data_ptr()))
+        stepper.step(1)
+        solver._check(lib.nb_get_bodies(solver.handle, out_pm.data_ptr(), out_vel.data_ptr()))
+        e2e_s += time.perf_counter() - t0
+    t = torch.tensor([step_ms, e2e_s], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    t_max, e2e_max = float(t[0]), float(t[1])
+    solver.close()
+    passes = max(int(phases["passes"]), 1)
+    chunk, _, _ = nb.shard_range(args.n, rank, world)
+    return {
+        "metric": METRIC, "value": args.n * args.steps / (t_max / 1000.0), "unit": "body-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Plummer sphere)",
+        "config": dict(workload_config(args), parallelism=f"target-sharded over {world} ranks, "
+                                                         "NCCL in-place all-gather of positions and velocities"),
+        "e2e": {"value": args.n * args.e2e_steps / e2e_max, "unit": "body-steps/s",
+                "h2d_bytes_per_step": 32 * args.n, "d2h_bytes_per_step": 32 * args.n, "steps": args.e2e_steps},
+        "allgather_bytes_per_step": 2 * 16 * chunk * world,
+        "phases_ms_per_step": {k: phases[k] / passes for k in
+                               ("bbox_ms", "morton_ms", "sort_ms", "gather_ms", "build_ms", "traverse_ms",
+                                "integrate_ms")},
+        "gpu_launches": int(phases["launches"]),
+        "clocks": clk.summary(),
+    }
 
 
 def measured_hbm():

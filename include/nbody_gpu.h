@@ -172,6 +172,23 @@ int nb_get_instance_roots(nb_ctx *ctx, int32_t *roots);
  * timing, when enabled, runs the steps uncaptured). */
 int nb_enable_graphs(nb_ctx *ctx, int enable);
 
+/* Target sharding of one instance over `world` processes, one GPU each (SURVEY multi-GPU row:
+ * the path shards over targets, every rank needs all sources). Every rank holds the same state.
+ * A force pass still sorts and builds over all bodies, but evaluates accelerations, and nb_step
+ * applies the kick-drift, only for this rank's slice of the Morton-ordered bodies:
+ *   chunk = ceil(n / world) rounded up to a multiple of 32, slice = [rank * chunk, (rank+1) * chunk) ∩ [0, n).
+ * After each nb_step(ctx, 1) the caller all-gathers the chunks of positions and velocities in place
+ * (recv = the buffers of nb_shard_buffers, rank r's chunk at offset r * chunk; an NCCL in-place
+ * all-gather) and calls nb_shard_gathered. Sharded contexts step once per nb_step call;
+ * accelerations are valid for the own slice only. Call nb_set_shard before nb_set_bodies, so the
+ * buffers get room for world * chunk bodies. Not for batches or the dual-tree solver. */
+int nb_shard_range(int64_t n, int32_t rank, int32_t world, int64_t *chunk, int64_t *first, int64_t *count);
+int nb_set_shard(nb_ctx *ctx, int32_t rank, int32_t world);
+/* Current state buffers (Morton slot order, float4 per body; they alternate between passes, so
+ * query them after every step) and their capacity in bodies. */
+int nb_shard_buffers(nb_ctx *ctx, void **d_pos_mass, void **d_velocity, int64_t *capacity);
+int nb_shard_gathered(nb_ctx *ctx);
+
 /* Serving: continuous batching of independent simulations on one device (no reference
  * counterpart beyond Solver::step per simulation). A request is a body set with its own theta and
  * step count. nb_server_tick retires finished requests (copying their final bodies out), admits

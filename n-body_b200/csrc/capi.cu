@@ -88,6 +88,9 @@ struct nb_ctx {
     float4 *graph_pos = nullptr;   // the body buffer the captured pair starts from
     int64_t steps_since_set = 0;   // plain or captured steps since the body set was replaced
 
+    // target sharding of one instance over `shard_world` processes (1: not sharded)
+    int32_t shard_rank = 0, shard_world = 1;
+
     bool bbox_valid = false;  // bbox already holds the box of the current positions
     bool have_tree = false;
     bool have_acc = false;
@@ -123,6 +126,17 @@ int check_cuda(nb_ctx *c, cudaError_t e, const char *what) {
 // Exported record: mac (4 floats), link (2 ints + 2 zero), payload (4 floats per PAY entry).
 int pay_float4s(int order) { return order == 1 ? NodeLayout<1>::PAY : NodeLayout<2>::PAY; }
 int rec_floats(int order) { return 8 + 4 * pay_float4s(order); }
+
+// Slice of Morton-ordered bodies owned by `rank`: chunks of ceil(n / world) rounded up to whole
+// 32-target traversal groups; the last chunks may be short or empty.
+void shard_slice(int64_t n, int32_t rank, int32_t world, int64_t *chunk, int64_t *first, int64_t *count) {
+    int64_t c = world > 0 ? (n + world - 1) / world : n;
+    c = (c + 31) / 32 * 32;
+    const int64_t f = std::min<int64_t>(n, (int64_t) rank * c);
+    *chunk = c;
+    *first = f;
+    *count = std::min<int64_t>(n, f + c) - f;
+}
 
 void refresh_names(nb_ctx *ctx) {
     if (ctx->cfg.solver == NB_SOLVER_DUAL_LINEAR_BVH) {
@@ -377,9 +391,11 @@ int force_pass(nb_ctx *ctx, Marks &mk) {
     ctx->acc_is_dual = false;
     const bool need_bbox = !ctx->bbox_valid;
     mk.mark(kBBox);
+    int64_t chunk = n, first = 0, count = n;
+    shard_slice(n, ctx->shard_rank, ctx->shard_world, &chunk, &first, &count);
     if (ctx->cfg.solver == NB_SOLVER_NAIVE) {
         mk.mark(kMorton); mk.mark(kSort); mk.mark(kGather); mk.mark(kBuild); mk.mark(kTraverse);
-        launch_direct_f32(ctx->pos, n, ctx->pos, n, ctx->cfg.G, ctx->cfg.epsilon, ctx->acc, s);
+        launch_direct_f32(ctx->pos, n, ctx->pos + first, count, ctx->cfg.G, ctx->cfg.epsilon, ctx->acc + first, s);
         ctx->have_tree = false;
         ctx->acc_is_bh = false;
         if (ctx->timing) ctx->times.launches += 1;
@@ -416,8 +432,9 @@ int force_pass(nb_ctx *ctx, Marks &mk) {
     launch_build_tree(ctx->keys, ctx->pos, n, ctx->cfg.max_leaf_size, ctx->cfg.order, ctx->cfg.theta, ctx->tw,
                       ctx->nodes, ctx->err, s);
     mk.mark(kTraverse);
-    launch_bh_traverse(ctx->cfg.order, ctx->nodes, ctx->tw.num_nodes, ctx->pos, n, ctx->pos, n, ctx->cfg.G,
-                       ctx->cfg.epsilon, ctx->acc, ctx->counts, ctx->trav, ctx->err, s);
+    // a sharded context evaluates only its slice of the Morton-ordered targets
+    launch_bh_traverse(ctx->cfg.order, ctx->nodes, ctx->tw.num_nodes, ctx->pos, n, ctx->pos + first, count,
+                       ctx->cfg.G, ctx->cfg.epsilon, ctx->acc + first, ctx->counts, ctx->trav, ctx->err, s);
     ctx->have_tree = true;
     ctx->acc_is_bh = true;
     if (ctx->timing) ctx->times.launches += launches_per_pass(ctx, need_bbox, false);
@@ -533,8 +550,8 @@ int nb_set_config(nb_ctx *ctx, const nb_config *cfg) {
     int rc = validate(ctx, cfg);
     if (rc != NB_OK) return rc;
     if (cfg->device != ctx->cfg.device) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "the device cannot change");
-    if (cfg->solver == NB_SOLVER_DUAL_LINEAR_BVH && ctx->num_inst > 0)
-        return fail(ctx, NB_ERR_UNSUPPORTED, "the dual-tree solver runs one instance");
+    if (cfg->solver == NB_SOLVER_DUAL_LINEAR_BVH && (ctx->num_inst > 0 || ctx->shard_world > 1))
+        return fail(ctx, NB_ERR_UNSUPPORTED, "the dual-tree solver runs one unsharded instance");
     ctx->cfg = *cfg;
     ctx->have_tree = false;
     drop_graph(ctx);
@@ -563,7 +580,10 @@ static int set_bodies_impl(nb_ctx *ctx, int64_t n, const void *pm, const void *v
     if (rc != NB_OK) return rc;
     if (n < 0 || n > kMaxBodies) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "body count out of range");
     if (n > 0 && !pm) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "positions are NULL");
-    rc = ensure_capacity(ctx, n);
+    int64_t chunk = n, first = 0, count = n;
+    shard_slice(n, ctx->shard_rank, ctx->shard_world, &chunk, &first, &count);
+    // a sharded context all-gathers whole chunks in place: room for world * chunk bodies
+    rc = ensure_capacity(ctx, std::max<int64_t>(n, chunk * ctx->shard_world));
     if (rc != NB_OK) return rc;
     free_batch(ctx);
     drop_graph(ctx);
@@ -672,10 +692,13 @@ static int one_step(nb_ctx *ctx) {
         rc = force_pass(ctx, mk);
         if (rc != NB_OK) return rc;
         mk.mark(kIntegrate);
-        const bool reduce_box = ctx->cfg.solver != NB_SOLVER_NAIVE && ctx->num_inst == 0;
+        // a sharded context drifts only its slice; the box is recomputed after the all-gather
+        const bool reduce_box = ctx->cfg.solver != NB_SOLVER_NAIVE && ctx->num_inst == 0 && ctx->shard_world == 1;
+        int64_t chunk = ctx->n, first = 0, count = ctx->n;
+        shard_slice(ctx->n, ctx->shard_rank, ctx->shard_world, &chunk, &first, &count);
         if (reduce_box) launch_bbox_reset(ctx->bbox, ctx->stream);
-        launch_kick_drift(ctx->pos, ctx->vel, ctx->acc, ctx->n, ctx->cfg.time_step, reduce_box ? ctx->bbox : nullptr,
-                          ctx->stream);
+        launch_kick_drift(ctx->pos + first, ctx->vel + first, ctx->acc + first, count, ctx->cfg.time_step,
+                          reduce_box ? ctx->bbox : nullptr, ctx->stream);
         ctx->bbox_valid = reduce_box;
         if (ctx->timing) ctx->times.launches += 1;
         rc = check_cuda(ctx, cudaGetLastError(), "kick-drift");
@@ -723,6 +746,8 @@ int nb_step(nb_ctx *ctx, int32_t steps) {
     int rc = begin(ctx);
     if (rc != NB_OK) return rc;
     if (steps < 0) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "negative step count");
+    if (ctx->shard_world > 1 && steps > 1)
+        return fail(ctx, NB_ERR_INVALID_ARGUMENT, "a sharded context steps once per call (all-gather between steps)");
     int32_t k = 0;
     while (k < steps) {
         const bool pair = ctx->use_graphs && !ctx->timing && ctx->n > 0 && steps - k >= 2 && ctx->steps_since_set > 0;
@@ -982,6 +1007,8 @@ int nb_set_instances(nb_ctx *ctx, int32_t count, const int64_t *sizes, const flo
     if (rc != NB_OK) return rc;
     if (ctx->cfg.solver == NB_SOLVER_DUAL_LINEAR_BVH)
         return fail(ctx, NB_ERR_UNSUPPORTED, "the dual-tree solver runs one instance");
+    if (ctx->shard_world > 1)
+        return fail(ctx, NB_ERR_UNSUPPORTED, "batched instances are not sharded (run independent batches per rank)");
     int64_t n = 0;
     rc = check_instances(ctx, count, sizes, thetas, &n);
     if (rc != NB_OK) return rc;
@@ -1009,6 +1036,46 @@ int nb_enable_graphs(nb_ctx *ctx, int enable) {
     if (!ctx) return NB_ERR_INVALID_ARGUMENT;
     ctx->use_graphs = enable != 0;
     if (!ctx->use_graphs) drop_graph(ctx);
+    return NB_OK;
+}
+
+int nb_shard_range(int64_t n, int32_t rank, int32_t world, int64_t *chunk, int64_t *first, int64_t *count) {
+    if (n < 0 || world < 1 || rank < 0 || rank >= world || !chunk || !first || !count)
+        return NB_ERR_INVALID_ARGUMENT;
+    shard_slice(n, rank, world, chunk, first, count);
+    return NB_OK;
+}
+
+int nb_set_shard(nb_ctx *ctx, int32_t rank, int32_t world) {
+    if (!ctx) return NB_ERR_INVALID_ARGUMENT;
+    if (world < 1 || world > 4096 || rank < 0 || rank >= world)
+        return fail(ctx, NB_ERR_INVALID_ARGUMENT, "shard rank out of range");
+    if (world > 1 && ctx->cfg.solver == NB_SOLVER_DUAL_LINEAR_BVH)
+        return fail(ctx, NB_ERR_UNSUPPORTED, "the dual-tree solver is not sharded");
+    if (world > 1 && ctx->num_inst > 0)
+        return fail(ctx, NB_ERR_UNSUPPORTED, "batched instances are not sharded");
+    int64_t chunk = 0, first = 0, count = 0;
+    shard_slice(ctx->n, rank, world, &chunk, &first, &count);
+    if (ctx->n > 0 && chunk * world > ctx->cap)
+        return fail(ctx, NB_ERR_INVALID_ARGUMENT, "call nb_set_shard before nb_set_bodies (buffers lack gather room)");
+    ctx->shard_rank = rank;
+    ctx->shard_world = world;
+    ctx->bbox_valid = false;
+    drop_graph(ctx);
+    return NB_OK;
+}
+
+int nb_shard_buffers(nb_ctx *ctx, void **d_pos_mass, void **d_velocity, int64_t *capacity) {
+    if (!ctx) return NB_ERR_INVALID_ARGUMENT;
+    if (d_pos_mass) *d_pos_mass = ctx->pos;
+    if (d_velocity) *d_velocity = ctx->vel;
+    if (capacity) *capacity = ctx->cap;
+    return NB_OK;
+}
+
+int nb_shard_gathered(nb_ctx *ctx) {
+    if (!ctx) return NB_ERR_INVALID_ARGUMENT;
+    ctx->bbox_valid = false;
     return NB_OK;
 }
 

@@ -145,6 +145,10 @@ SIGNATURES = {
     "nb_server_status": (C.c_int, [_vp, _i64, C.POINTER(_i32), C.POINTER(_i32)]),
     "nb_server_take_result": (C.c_int, [_vp, _i64, _vp, _vp]),
     "nb_server_get_stats": (C.c_int, [_vp, C.POINTER(ServerStats)]),
+    "nb_shard_range": (C.c_int, [_i64, _i32, _i32, C.POINTER(_i64), C.POINTER(_i64), C.POINTER(_i64)]),
+    "nb_set_shard": (C.c_int, [_vp, _i32, _i32]),
+    "nb_shard_buffers": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_i64)]),
+    "nb_shard_gathered": (C.c_int, [_vp]),
     "nb_host_alloc": (_vp, [C.c_size_t]),
     "nb_host_free": (None, [_vp]),
 }
@@ -168,6 +172,22 @@ def lib() -> C.CDLL:
             fn.argtypes = args
         _lib = L
     return _lib
+
+
+def shard_range(n: int, rank: int, world: int):
+    """(chunk, first, count) of `rank`'s slice of n Morton-ordered bodies (nb_shard_range)."""
+    chunk, first, count = C.c_int64(), C.c_int64(), C.c_int64()
+    rc = lib().nb_shard_range(n, rank, world, C.byref(chunk), C.byref(first), C.byref(count))
+    if rc != NB_OK:
+        raise NBodyError(rc, "invalid shard range")
+    return chunk.value, first.value, count.value
+
+
+class _DeviceArray:
+    """A raw device buffer of float4 bodies, exposed through __cuda_array_interface__."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n, 4), "typestr": "<f4", "data": (ptr, False), "version": 2}
 
 
 def default_config() -> Config:
@@ -372,6 +392,29 @@ class Solver:
                                       _ptr(bbox)))
         return {"num_nodes": nn.value, "codes": codes, "ids": ids, "records": recs[: nn.value], "bbox": bbox}
 
+    # -- target sharding over ranks (nb_set_shard; see ShardedStepper) --
+    def set_shard(self, rank: int, world: int):
+        self._check(lib().nb_set_shard(self._ctx, rank, world))
+
+    def shard_buffers(self):
+        pos, vel, cap = C.c_void_p(), C.c_void_p(), C.c_int64()
+        self._check(lib().nb_shard_buffers(self._ctx, C.byref(pos), C.byref(vel), C.byref(cap)))
+        return pos.value, vel.value, cap.value
+
+    def shard_tensors(self, rows: int):
+        """torch views (rows, 4) of the current position and velocity buffers (device memory)."""
+        import torch
+
+        pos, vel, cap = self.shard_buffers()
+        if rows > cap:
+            raise ValueError("rows exceed the buffer capacity")
+        dev = torch.device("cuda", self.config().device)
+        return (torch.as_tensor(_DeviceArray(pos, rows), device=dev),
+                torch.as_tensor(_DeviceArray(vel, rows), device=dev))
+
+    def shard_gathered(self):
+        self._check(lib().nb_shard_gathered(self._ctx))
+
     def direct_device(self, n, d_bodies, nt, d_targets, d_acc, precision=32):
         self._check(lib().nb_direct_device(self._ctx, n, d_bodies, nt, d_targets, d_acc, precision))
 
@@ -523,4 +566,5 @@ def decode_dual_records(records: np.ndarray) -> dict:
     }
 
 
-from . import scenarios  # noqa: E402  (host-side scenario generators)
+from . import scenarios  # noqa: E402
+from .sharded import ShardedStepper  # noqa: E402  (host-side scenario generators)
