@@ -60,6 +60,7 @@ struct nb_ctx {
     DualNodes dnodes;          // dual solver: octupole node arrays
     DualWorkspace dws;         // dual solver: starting nodes, per-block arenas and task stacks
     int64_t dual_cap = 0;      // body capacity the dual buffers were sized for
+    unsigned long long *host_scratch = nullptr;  // pinned: near-pool counters and the error word
     BBoxAccum *bbox = nullptr;
     unsigned long long *counts = nullptr;
     uint32_t *err = nullptr;
@@ -190,10 +191,13 @@ void drop_graph(nb_ctx *ctx) {
 void free_dual(nb_ctx *ctx) {
     dev_free(ctx->tw.sq2); dev_free(ctx->tw.sq3);
     dev_free(ctx->dnodes.bmin); dev_free(ctx->dnodes.bmax); dev_free(ctx->dnodes.com); dev_free(ctx->dnodes.q);
-    dev_free(ctx->dnodes.link);
+    dev_free(ctx->dnodes.link); dev_free(ctx->dnodes.thr);
     ctx->dnodes.capacity = 0;
     dev_free(ctx->dws.roots); dev_free(ctx->dws.num_roots); dev_free(ctx->dws.arena); dev_free(ctx->dws.tasks);
     ctx->dws.arena_words = 0;
+    NearPool &np = ctx->dws.near;
+    dev_free(np.head); dev_free(np.items); dev_free(np.words); dev_free(np.units); dev_free(np.counters);
+    np.head_cap = np.item_cap = np.word_cap = np.unit_cap = 0;
     ctx->dual_cap = 0;
 }
 
@@ -211,12 +215,23 @@ int ensure_dual(nb_ctx *ctx) {
     NB_TRY(dev_alloc(&ctx->dnodes.com, slots), "alloc dual nodes");
     NB_TRY(dev_alloc(&ctx->dnodes.q, 4 * slots), "alloc dual nodes");
     NB_TRY(dev_alloc(&ctx->dnodes.link, slots), "alloc dual nodes");
+    NB_TRY(dev_alloc(&ctx->dnodes.thr, slots), "alloc dual nodes");
     ctx->dnodes.capacity = (int64_t) slots;
     NB_TRY(dev_alloc(&ctx->dws.roots, kDualRoots), "alloc dual roots");
     NB_TRY(dev_alloc(&ctx->dws.num_roots, 1), "alloc dual roots");
     ctx->dws.arena_words = dual_arena_words(c);
     NB_TRY(dev_alloc(&ctx->dws.arena, (size_t) kDualRoots * (size_t) ctx->dws.arena_words), "alloc dual arena");
     NB_TRY(dev_alloc(&ctx->dws.tasks, (size_t) kDualRoots * kDualTasks * 6), "alloc dual tasks");
+    NearPool &np = ctx->dws.near;
+    np.head_cap = (int64_t) slots;
+    dual_near_sizes(c, &np.item_cap, &np.word_cap);
+    np.unit_cap = c + 64;
+    NB_TRY(dev_alloc(&np.head, (size_t) np.head_cap), "alloc near-field pool");
+    NB_TRY(dev_alloc(&np.items, (size_t) np.item_cap), "alloc near-field pool");
+    NB_TRY(dev_alloc(&np.words, (size_t) np.word_cap), "alloc near-field pool");
+    NB_TRY(dev_alloc(&np.units, (size_t) np.unit_cap), "alloc near-field pool");
+    NB_TRY(dev_alloc(&np.counters, 4), "alloc near-field pool");
+    if (ctx->dws.near_blocks == 0) ctx->dws.near_blocks = dual_near_blocks(ctx->cfg.device);
     ctx->dual_cap = c;
     return NB_OK;
 }
@@ -330,8 +345,48 @@ int64_t launches_per_pass(const nb_ctx *ctx, bool with_bbox, bool with_drift) {
     // + root-leaf(1) + traverse(1)
     int64_t k = 1 + 1 + 8 + 1 + 1 + 1 + 1 + 1 + 1;
     if (ctx->n <= 1) k -= 3;  // no Karras internal nodes
-    if (ctx->cfg.solver == NB_SOLVER_DUAL_LINEAR_BVH) k += 1;
+    if (ctx->cfg.solver == NB_SOLVER_DUAL_LINEAR_BVH) k += 2;  // loadBalancedBreak and the near-field kernel
     return k + (with_bbox ? 1 : 0) + (with_drift ? 1 : 0);
+}
+
+// The dual-tree traversal and near field. The near-field pool and the per-block arenas are sized
+// from the body count; when a pass finds them too small (error bits kErrNearPool / kErrDualArena),
+// the host grows them to the sizes the pass asked for and runs the traversal again.
+int dual_traverse(nb_ctx *ctx, int64_t n, cudaStream_t s) {
+    NearPool &np = ctx->dws.near;
+    for (int attempt = 0;; ++attempt) {
+        launch_dual_traverse(ctx->dnodes, ctx->tw.num_nodes, ctx->pos, n, ctx->cfg.G, ctx->cfg.epsilon,
+                             ctx->cfg.theta, ctx->acc, ctx->counts, ctx->dws, ctx->err, s);
+        unsigned long long *h = ctx->host_scratch;
+        NB_TRY(cudaMemcpyAsync(h, np.counters, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
+               "read near-field pool");
+        NB_TRY(cudaMemcpyAsync(h + 4, ctx->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "read status");
+        NB_TRY(cudaStreamSynchronize(s), "dual-tree traversal");
+        uint32_t e = 0;
+        std::memcpy(&e, h + 4, sizeof(uint32_t));
+        const bool pool = (e & kErrNearPool) != 0, arena = (e & kErrDualArena) != 0;
+        if ((!pool && !arena) || attempt == 3) return NB_OK;
+        if (pool) {
+            const int64_t items = (int64_t) h[0], words = (int64_t) h[1];
+            dev_free(np.items);
+            dev_free(np.words);
+            np.item_cap = std::max<int64_t>(np.item_cap, items + items / 4 + 1024);
+            np.word_cap = std::min<int64_t>(std::max<int64_t>(np.word_cap, words + words / 4 + 4096),
+                                            (int64_t(1) << 31) - 1);
+            NB_TRY(dev_alloc(&np.items, (size_t) np.item_cap), "grow near-field pool");
+            NB_TRY(dev_alloc(&np.words, (size_t) np.word_cap), "grow near-field pool");
+        }
+        if (arena) {
+            dev_free(ctx->dws.arena);
+            ctx->dws.arena_words = std::min<int64_t>(2 * ctx->dws.arena_words, int64_t(1) << 28);
+            NB_TRY(dev_alloc(&ctx->dws.arena, (size_t) kDualRoots * (size_t) ctx->dws.arena_words),
+                   "grow dual arena");
+        }
+        e &= ~(uint32_t) (kErrNearPool | kErrDualArena);
+        std::memcpy(h + 4, &e, sizeof(uint32_t));
+        NB_TRY(cudaMemcpyAsync(ctx->err, h + 4, sizeof(uint32_t), cudaMemcpyHostToDevice, s), "reset status");
+        NB_TRY(cudaMemsetAsync(ctx->counts, 0, 4 * sizeof(unsigned long long), s), "reset counts");
+    }
 }
 
 // Force pass over a batch of instances: per-instance boxes and codes, a global code sort followed
@@ -419,10 +474,11 @@ int force_pass(nb_ctx *ctx, Marks &mk) {
     ctx->sorted_codes = ctx->keys;
     if (ctx->cfg.solver == NB_SOLVER_DUAL_LINEAR_BVH) {
         if (ctx->dual_cap != ctx->cap) return fail(ctx, NB_ERR_CUDA, "dual-tree buffers missing");
-        launch_build_dual_tree(ctx->keys, ctx->pos, n, ctx->cfg.max_leaf_size, ctx->tw, ctx->dnodes, ctx->err, s);
+        launch_build_dual_tree(ctx->keys, ctx->pos, n, ctx->cfg.max_leaf_size, ctx->cfg.theta, ctx->tw, ctx->dnodes,
+                               ctx->err, s);
         mk.mark(kTraverse);
-        launch_dual_traverse(ctx->dnodes, ctx->tw.num_nodes, ctx->pos, n, ctx->cfg.G, ctx->cfg.epsilon,
-                             ctx->cfg.theta, ctx->acc, ctx->counts, ctx->dws, ctx->err, s);
+        const int rc = dual_traverse(ctx, n, s);
+        if (rc != NB_OK) return rc;
         ctx->have_tree = true;
         ctx->acc_is_bh = true;
         ctx->acc_is_dual = true;
@@ -453,6 +509,7 @@ int device_status(nb_ctx *ctx) {
     if (e & kErrStackOverflow) return fail(ctx, NB_ERR_DEVICE_CHECK, "traversal stack overflow");
     if (e & kErrTraverseLimit) return fail(ctx, NB_ERR_DEVICE_CHECK, "traversal met an invalid tree link");
     if (e & kErrDualArena) return fail(ctx, NB_ERR_DEVICE_CHECK, "dual-tree list or task storage exhausted");
+    if (e & kErrNearPool) return fail(ctx, NB_ERR_DEVICE_CHECK, "dual-tree near-field pool exhausted");
     return NB_OK;
 }
 
@@ -508,6 +565,10 @@ int nb_create(const nb_config *cfg, nb_ctx **out) {
         nb_destroy(ctx);
         return NB_ERR_OUT_OF_MEMORY;
     }
+    if (cudaMallocHost((void **) &ctx->host_scratch, 8 * sizeof(unsigned long long)) != cudaSuccess) {
+        nb_destroy(ctx);
+        return NB_ERR_OUT_OF_MEMORY;
+    }
     ctx->trav.warps = traverse_resident_warps(cfg->device);
     if (dev_alloc(&ctx->trav.stack, (size_t) ctx->trav.warps * kTraverseStack) != cudaSuccess ||
         dev_alloc(&ctx->trav.group_counter, 1) != cudaSuccess) {
@@ -532,6 +593,7 @@ int nb_destroy(nb_ctx *ctx) {
     dev_free(ctx->bbox); dev_free(ctx->counts); dev_free(ctx->err); dev_free(ctx->sw.hist);
     dev_free(ctx->sw.offsets); dev_free(ctx->sw.tile_counter); dev_free(ctx->tw.num_nodes); dev_free(ctx->acc64);
     dev_free(ctx->trav.stack); dev_free(ctx->trav.group_counter);
+    if (ctx->host_scratch) cudaFreeHost(ctx->host_scratch);
     for (auto &ev: ctx->pending) ctx->event_pool.insert(ctx->event_pool.end(), ev.begin(), ev.end());
     for (auto e: ctx->event_pool) cudaEventDestroy(e);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -750,7 +812,9 @@ int nb_step(nb_ctx *ctx, int32_t steps) {
         return fail(ctx, NB_ERR_INVALID_ARGUMENT, "a sharded context steps once per call (all-gather between steps)");
     int32_t k = 0;
     while (k < steps) {
-        const bool pair = ctx->use_graphs && !ctx->timing && ctx->n > 0 && steps - k >= 2 && ctx->steps_since_set > 0;
+        // the dual-tree pass reads its pool usage back on the host, so it is never captured
+        const bool pair = ctx->use_graphs && !ctx->timing && ctx->n > 0 && steps - k >= 2 && ctx->steps_since_set > 0 &&
+                          ctx->cfg.solver != NB_SOLVER_DUAL_LINEAR_BVH;
         // The captured pair reads and writes the buffers it was recorded with; each plain force
         // pass swaps the ping-pong buffers, so replay only when the bodies sit where it expects.
         if (pair && (!ctx->graph2 || ctx->pos == ctx->graph_pos)) {

@@ -16,17 +16,27 @@
 //   M2L / P2L / M2P / L2L / L2P                        Gravity.h:239-259, 282-306, 352-392;
 //                                                      MultipoleAcceleration.h:33-84
 //
-// Work organisation. One thread block per starting passive node (the <= 256 nodes of
-// loadBalancedBreak, found on the device). Each block runs the reference's recursion as a
-// depth-first stack of tasks (lock-step tasks and passive-tree tasks) whose lists and local fields
-// live in a per-block arena of global memory; every step of a task is block-parallel:
-//   - classifying an active-node or active-body list: one entry per thread, stable block-wide
-//     compaction (ballots and warp counts), so list order is deterministic;
-//   - M2L / P2L into the task's local field: per-thread partial fields, fixed-order block reduction;
-//   - near field at a passive leaf: the (body, active subtree) activeTree walks or (body, close
-//     body) pairs spread over the block, partial sums reduced per body in a fixed order.
-// Results are deterministic run to run. The floating-point accumulation order differs from the
-// reference's serial recursion; the interactions evaluated are the same.
+// Work organisation, two kernels:
+//   dual_kernel  one thread block per starting passive node (the <= 256 nodes of
+//                loadBalancedBreak, found on the device). Each block runs the reference's
+//                recursion as a depth-first stack of tasks (lock-step and passive-tree tasks)
+//                whose lists and local fields live in a per-block arena of global memory. Every
+//                step is block-parallel: lists are classified one entry per thread with a stable
+//                block-wide compaction (ballots and warp counts); the far entries' M2L / P2L terms
+//                are then evaluated uniformly, one per thread, and reduced into the task's local
+//                field in a fixed order; L2L translates it to the children; at a passive leaf the
+//                block applies L2P. The leaf's near field is not evaluated here: the block appends
+//                it to the leaf's item list (the activeTree roots of a lock-step leaf, or the close
+//                bodies of a passive-tree leaf) in a global pool.
+//   near_kernel  a persistent grid over all SMs. Each warp takes 32 targets of one passive leaf
+//                and runs the leaf's items in list order: close bodies as pair tiles staged in
+//                shared memory; activeTree roots as a warp walk with one lane per target and a
+//                lane mask per stack entry, pairs at opened leaves as shared-memory tiles, and
+//                M2P terms queued per lane and evaluated target-major.
+// The near field, about nine tenths of the work, is thereby balanced over the whole GPU, and the
+// uneven passive subtrees only bound the much shorter traversal. Every sum has a fixed order, so
+// results are deterministic run to run; the accumulation order differs from the reference's
+// serial recursion, the interactions evaluated are the same.
 #include <algorithm>
 #include <cfloat>
 
@@ -41,7 +51,6 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kTaskInts = 6;  // type, passive node, list offset, list length, field offset, arena top
 constexpr int kLockstep = 0, kPassive = 1;
-constexpr int kWalkStack = kMaxTreeDepth + 2;
 constexpr int F = st::kFieldFloats;
 
 // Dual-tree node as stored (nb_internal.cuh, DualNodes). Internal nodes keep ~first body in link.y.
@@ -76,15 +85,14 @@ __device__ __forceinline__ float max0(float x) { return (x < 0.f) ? 0.f : x; }
 __device__ __forceinline__ float len3(float a, float b, float c) {
     return __fsqrt_rn(fadd(fadd(fmul(a, a), fmul(b, b)), fmul(c, c)));
 }
-// (float) sqrt(pow(|u|, 2) + pow(|v|, 2)) with the pow, sum and root in double
+// (float) sqrt(pow(|u|, 2) + pow(|v|, 2)) with the pow, sum and root in double. When one length
+// is zero the result is the other one exactly (a float's square is exact in double, and so is the
+// root of an exact square), which is the common case and needs no double arithmetic.
 __device__ __forceinline__ float sep_from(float lu, float lv) {
+    if (lv == 0.f) return lu;
+    if (lu == 0.f) return lv;
     const double du = (double) lu, dv = (double) lv;
     return __double2float_rn(__dsqrt_rn(__dadd_rn(__dmul_rn(du, du), __dmul_rn(dv, dv))));
-}
-__device__ __forceinline__ float sep_point(const DNode &n, const float p[3]) {
-    const float lu = len3(max0(fsub(n.mn[0], p[0])), max0(fsub(n.mn[1], p[1])), max0(fsub(n.mn[2], p[2])));
-    const float lv = len3(max0(fsub(p[0], n.mx[0])), max0(fsub(p[1], n.mx[1])), max0(fsub(p[2], n.mx[2])));
-    return sep_from(lu, lv);
 }
 __device__ __forceinline__ float sep_box(const DNode &a, const DNode &b) {
     const float lu = len3(max0(fsub(a.mn[0], b.mx[0])), max0(fsub(a.mn[1], b.mx[1])), max0(fsub(a.mn[2], b.mx[2])));
@@ -92,17 +100,30 @@ __device__ __forceinline__ float sep_box(const DNode &a, const DNode &b) {
     return sep_from(lu, lv);
 }
 
-// DiagonalOverSeparation, (active node, point): approximate the node for the point
-__device__ __forceinline__ bool approx_for_point(const DNode &a, const float p[3], float theta) {
-    return fdiv(a.diag, sep_point(a, p)) < theta && a.size > 32;
+// sep(node, p) >= B, exactly, with the node's thresholds (B, S): when one of the two separation
+// vectors is zero, sep is RN(sqrt(|v|^2)) and the test is |v|^2 >= S; otherwise the double path.
+__device__ __forceinline__ bool sep_at_least(const DNode &n, const float p[3], float B, float S) {
+    const float ux = max0(fsub(n.mn[0], p[0])), uy = max0(fsub(n.mn[1], p[1])), uz = max0(fsub(n.mn[2], p[2]));
+    const float vx = max0(fsub(p[0], n.mx[0])), vy = max0(fsub(p[1], n.mx[1])), vz = max0(fsub(p[2], n.mx[2]));
+    const float su = fadd(fadd(fmul(ux, ux), fmul(uy, uy)), fmul(uz, uz));
+    const float sv = fadd(fadd(fmul(vx, vx), fmul(vy, vy)), fmul(vz, vz));
+    if (sv == 0.f) return su >= S;
+    if (su == 0.f) return sv >= S;
+    return sep_from(__fsqrt_rn(su), __fsqrt_rn(sv)) >= B;
 }
-// (point, passive node): the active point is far from the passive node
-__device__ __forceinline__ bool point_is_far(const float p[3], const DNode &P, float theta) {
-    return fdiv(fmul(3.0f, P.diag), sep_point(P, p)) < theta;
+
+// DiagonalOverSeparation (DiagonalOverSeparation.h:29-49), (active node, point): approximate the
+// node for the point, RN(diag / sep) < theta and more than 32 bodies. thr = node thresholds.
+__device__ __forceinline__ bool approx_for_point(const DNode &a, float4 thr, const float p[3]) {
+    return a.size > 32 && sep_at_least(a, p, thr.x, thr.y);
+}
+// (point, passive node): the active point is far from the passive node, RN(3 diag / sep) < theta
+__device__ __forceinline__ bool point_is_far(const float p[3], const DNode &P, float4 thr) {
+    return sep_at_least(P, p, thr.z, thr.w);
 }
 // (active node, passive node): 0 = approximate, else DescendActive (1) | DescendPassive (2)
 __device__ __forceinline__ int node_node(const DNode &A, const DNode &P, float theta) {
-    if (fdiv(fadd(A.diag, P.diag), sep_box(A, P)) < theta && A.size > 32) return 0;
+    if (A.size > 32 && fdiv(fadd(A.diag, P.diag), sep_box(A, P)) < theta) return 0;
     int r = 0;
     if (A.diag <= fmul(P.diag, 2.0f)) r |= 2;
     if (P.diag <= fmul(A.diag, 2.0f)) r |= 1;
@@ -130,16 +151,17 @@ __device__ __forceinline__ void load_q(const DualNodes &N, int k, float q2[6], f
     q3[6] = d.x; q3[7] = d.y; q3[8] = d.z; q3[9] = d.w;
 }
 
-__device__ __forceinline__ float soft_r(const float R[3], float eps) {
-    return sqrtf(fmaf(R[0], R[0], fmaf(R[1], R[1], fmaf(R[2], R[2], eps))));
+// 1 / sqrt(|R|^2 + eps) (the reference's r is sqrt(|R|^2 + eps), Gravity.h:207)
+__device__ __forceinline__ float soft_inv_r(const float R[3], float eps) {
+    return rsqrtf(fmaf(R[0], R[0], fmaf(R[1], R[1], fmaf(R[2], R[2], eps))));
 }
 
 // Gravity::particleParticle (Gravity.h:199-209), added into a
 __device__ __forceinline__ void pair(const Ctx &x, float4 b, const float p[3], float a[3]) {
     const float R[3] = {p[0] - b.x, p[1] - b.y, p[2] - b.z};
     if (R[0] == 0.f && R[1] == 0.f && R[2] == 0.f) return;
-    const float r = soft_r(R, x.eps);
-    const float s = b.w * x.G / (r * (r * r));
+    const float inv = soft_inv_r(R, x.eps);
+    const float s = (b.w * x.G) * (inv * inv * inv);
 #pragma unroll
     for (int i = 0; i < 3; ++i) a[i] = fmaf(-R[i], s, a[i]);
 }
@@ -148,15 +170,15 @@ __device__ __forceinline__ void pair(const Ctx &x, float4 b, const float p[3], f
 __device__ void node_particle3(const Ctx &x, int k, const DNode &n, const float p[3], float a[3]) {
     const float R[3] = {p[0] - n.com[0], p[1] - n.com[1], p[2] - n.com[2]};
     if (R[0] == 0.f && R[1] == 0.f && R[2] == 0.f) return;
-    const float r = soft_r(R, x.eps);
-    const st::Coef c(r);
+    const float inv = soft_inv_r(R, x.eps);
+    const st::Coef c = st::Coef::from_inverse(inv);
     float q2[6], q3[10], d3[10], d4[15], v3[3], v4[3];
     load_q(x.nodes, k, q2, q3);
     st::D3(R, c, d3);
     st::D4(R, c, d4);
     st::t3_dot_t2(d3, q2, v3);
     st::t4_dot_t3(d4, q3, v4);
-    const float mono = -n.M / (r * (r * r));
+    const float mono = -n.M * (inv * inv * inv);
 #pragma unroll
     for (int i = 0; i < 3; ++i) a[i] += x.G * (R[i] * mono + v3[i] / 2.0f - v4[i] / 6.0f);
 }
@@ -167,8 +189,8 @@ __device__ void node_particle3(const Ctx &x, int k, const DNode &n, const float 
 __device__ void m2l(const Ctx &x, int k, const DNode &n, const float pc[3], float *f) {
     const float R[3] = {pc[0] - n.com[0], pc[1] - n.com[1], pc[2] - n.com[2]};
     if (R[0] == 0.f && R[1] == 0.f && R[2] == 0.f) return;
-    const float r = soft_r(R, x.eps);
-    const st::Coef c(r);
+    const float inv = soft_inv_r(R, x.eps);
+    const st::Coef c = st::Coef::from_inverse(inv);
     float q2[6], q3[10], d2[6], d3[10], d4[15], v3[3], v4[3], t2q[6];
     load_q(x.nodes, k, q2, q3);
     st::D2(R, c, d2);
@@ -178,7 +200,7 @@ __device__ void m2l(const Ctx &x, int k, const DNode &n, const float pc[3], floa
     st::t4_dot_t3(d4, q3, v4);
     st::t4_dot_t2(d4, q2, t2q);
     const float mg = n.M * x.G;
-    const float mono = mg / (r * (r * r));
+    const float mono = mg * (inv * inv * inv);
 #pragma unroll
     for (int i = 0; i < 3; ++i) f[i] += -R[i] * mono + v3[i] / 2.0f + v4[i] / 6.0f;
 #pragma unroll
@@ -193,14 +215,14 @@ __device__ void m2l(const Ctx &x, int k, const DNode &n, const float pc[3], floa
 __device__ void p2l(const Ctx &x, float4 b, const float pc[3], float *f) {
     const float R[3] = {pc[0] - b.x, pc[1] - b.y, pc[2] - b.z};
     if (R[0] == 0.f && R[1] == 0.f && R[2] == 0.f) return;
-    const float r = soft_r(R, x.eps);
-    const st::Coef c(r);
+    const float inv = soft_inv_r(R, x.eps);
+    const st::Coef c = st::Coef::from_inverse(inv);
     float d2[6], d3[10], d4[15];
     st::D2(R, c, d2);
     st::D3(R, c, d3);
     st::D4(R, c, d4);
     const float mg = b.w * x.G;
-    const float inv3 = 1.0f / (r * (r * r));
+    const float inv3 = inv * inv * inv;
 #pragma unroll
     for (int i = 0; i < 3; ++i) f[i] -= R[i] * inv3 * mg;
 #pragma unroll
@@ -209,40 +231,6 @@ __device__ void p2l(const Ctx &x, float4 b, const float pc[3], float *f) {
     for (int a = 0; a < 10; ++a) f[9 + a] += d3[a] * mg * 0.5f;
 #pragma unroll
     for (int a = 0; a < 15; ++a) f[19 + a] += d4[a] * mg * (1.0f / 6.0f);
-}
-
-// activeTree from node `root` for the point p (activeTree.h:24-79): left subtree first.
-__device__ void active_tree(const Ctx &x, int root, const float p[3], float a[3], unsigned long long &npp,
-                            unsigned long long &nnp, uint32_t *err) {
-    int stk[kWalkStack];
-    int sp = 0;
-    stk[sp++] = root;
-    while (sp > 0) {
-        const int k = stk[--sp];
-        const DNode n = load_node(x.nodes, k);
-        if (approx_for_point(n, p, x.theta)) {
-            node_particle3(x, k, n, p, a);
-            ++nnp;
-        } else if (n.leaf()) {
-            if (!x.range_ok(n.link0, n.link1)) {
-                atomicOr(err, (uint32_t) kErrTraverseLimit);
-                continue;
-            }
-            for (int j = n.link0; j < n.link1; ++j) pair(x, __ldg(x.bodies + j), p, a);
-            npp += (unsigned long long) (n.link1 - n.link0);
-        } else {
-            if (sp + 2 > kWalkStack) {
-                atomicOr(err, (uint32_t) kErrTreeDepth);
-                return;
-            }
-            if (!x.left_ok(k) || !x.right_ok(k, n.link0)) {
-                atomicOr(err, (uint32_t) kErrTraverseLimit);
-                continue;
-            }
-            stk[sp++] = n.link0;  // right child, visited second
-            stk[sp++] = k + 1;    // left child
-        }
-    }
 }
 
 struct Scan3 {
@@ -322,6 +310,48 @@ __device__ void block_add_field(const float part[F], float *s_field, float (*s_r
     __syncthreads();
 }
 
+constexpr int kItemRoots = 0, kItemBodies = 1;
+
+// Appends a near-field item for passive leaf `leaf` (bodies [first, first + size)): the payload is
+// a[0..na) then b[0..nb) (activeTree roots), or for close bodies the runs of consecutive indices as
+// (first index, length) pairs. The owning block is the only writer of the leaf's list head, so the
+// list order is the block's task order. The first item of a leaf also registers its 32-target
+// units for the near kernel. Called by every thread of the block.
+__device__ void append_item(const NearPool &pool, int leaf, int first, int size, int kind, const int *a, int na,
+                            const int *b, int nb, uint32_t *err, int *s_slot) {
+    const int count = na + nb;
+    if (count == 0) return;  // uniform
+    if (threadIdx.x == 0) {
+        int slot = -1;
+        const unsigned long long it = atomicAdd(&pool.counters[0], 1ull);
+        const unsigned long long off = atomicAdd(&pool.counters[1], (unsigned long long) count);
+        bool ok = it < (unsigned long long) pool.item_cap && off + count <= (unsigned long long) pool.word_cap &&
+                  leaf < pool.head_cap;
+        const int old = ok ? pool.head[leaf] : -1;
+        if (ok && old < 0) {
+            const int nunits = (size + 31) / 32;
+            const unsigned long long u = atomicAdd(&pool.counters[2], (unsigned long long) nunits);
+            ok = u + nunits <= (unsigned long long) pool.unit_cap;
+            if (ok)
+                for (int j = 0; j < nunits; ++j) pool.units[u + j] = make_int2(leaf, first + 32 * j);
+        }
+        if (ok) {
+            pool.items[it] = make_int4(old, kind, (int) off, count);
+            pool.head[leaf] = (int) it;
+            slot = (int) off;
+        } else {
+            atomicOr(err, (uint32_t) kErrNearPool);
+        }
+        *s_slot = slot;
+    }
+    __syncthreads();
+    const int off = *s_slot;
+    if (off >= 0) {
+        for (int i = threadIdx.x; i < na; i += kThreads) pool.words[off + i] = a[i];
+        for (int i = threadIdx.x; i < nb; i += kThreads) pool.words[off + na + i] = b[i];
+    }
+}
+
 __device__ __forceinline__ void push_task(int *t, int type, int node, int list, int len, int field, int top) {
     t[0] = type; t[1] = node; t[2] = list; t[3] = len; t[4] = field; t[5] = top;
 }
@@ -332,15 +362,15 @@ __global__ void __launch_bounds__(kThreads) dual_kernel(DualNodes nodes, const i
                                                         unsigned long long *__restrict__ counts,
                                                         const int *__restrict__ roots, const int *__restrict__ num_roots,
                                                         int *__restrict__ arena_all, int arena_words,
-                                                        int *__restrict__ tasks_all, uint32_t *__restrict__ err) {
+                                                        int *__restrict__ tasks_all, NearPool pool,
+                                                        uint32_t *__restrict__ err) {
     __shared__ float s_field[F];
     __shared__ float s_child[2][F];
     __shared__ float s_red[kWarps][F];
-    __shared__ float s_part[kThreads][3];
     __shared__ int s_task[kTaskInts];
     __shared__ Scan3 s_scan;
     __shared__ int s_w[kWarps];
-    __shared__ int s_ntask, s_fail;
+    __shared__ int s_ntask, s_fail, s_slot;
 
     if ((int) blockIdx.x >= *num_roots) return;  // uniform across the block
     const int tid = threadIdx.x;
@@ -348,7 +378,7 @@ __global__ void __launch_bounds__(kThreads) dual_kernel(DualNodes nodes, const i
     int *arena = arena_all + (int64_t) blockIdx.x * arena_words;
     float *farena = reinterpret_cast<float *>(arena);
     int *tasks = tasks_all + (int64_t) blockIdx.x * kDualTasks * kTaskInts;
-    unsigned long long npp = 0, nnp = 0, npn = 0, nnn = 0;
+    unsigned long long npn = 0, nnn = 0;
     const int root = roots[blockIdx.x];
     if (root < 0 || root >= x.nn || x.nn <= 0) {
         if (tid == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
@@ -428,6 +458,7 @@ __global__ void __launch_bounds__(kThreads) dual_kernel(DualNodes nodes, const i
         const int type = s_task[0], pk = s_task[1], loff = s_task[2], len = s_task[3], foff = s_task[4];
         const int scratch = s_task[5];
         const DNode P = load_node(nodes, pk);
+        const float4 pthr = __ldg(nodes.thr + pk);
         float pc[3];
         center(P, pc);
         const int pfirst = P.first(), pend = pfirst + P.size;
@@ -452,9 +483,9 @@ __global__ void __launch_bounds__(kThreads) dual_kernel(DualNodes nodes, const i
             continue;
         }
 
-        // arena needed by this task above `scratch`: the three class lists, the deeper list and two
-        // child fields (the leaf-body list is checked once its length is known)
-        const int64_t need = 3 * (int64_t) len + (type == kLockstep ? 2 * (int64_t) len : 0) + 2 * F;
+        // arena needed by this task above `scratch`: the three class lists, the deeper list (or the
+        // close-body runs) and two child fields (the leaf-body list is checked once its length is known)
+        const int64_t need = 5 * (int64_t) len + 2 * F;
         if ((int64_t) scratch + need >= arena_words) {
             if (tid == 0) atomicOr(err, (uint32_t) kErrDualArena);
             continue;
@@ -463,10 +494,7 @@ __global__ void __launch_bounds__(kThreads) dual_kernel(DualNodes nodes, const i
         int *c1 = arena + scratch + len, *c2 = c1 + len;
         int *c0 = arena + scratch;  // scratch for leaf-body offsets (far entries are not stored)
 
-        // ---- classify the list: far entries go into the local field now ----
-        float part[F];
-#pragma unroll
-        for (int a = 0; a < F; ++a) part[a] = 0.f;
+        // ---- classify the list (stable compaction): far c0, leaf / close c1, non-leaf c2 ----
         for (int i0 = 0; i0 < len; i0 += kThreads) {
             const int i = i0 + tid;
             int cls = -1, e = -1;
@@ -474,77 +502,74 @@ __global__ void __launch_bounds__(kThreads) dual_kernel(DualNodes nodes, const i
                 e = list[i];
                 if (type == kLockstep) {
                     const DNode A = load_node(nodes, e);
-                    if (node_node(A, P, theta) == 0) {
-                        m2l(x, e, A, pc, part);
-                        ++nnn;
-                        cls = 0;
-                    } else if (A.leaf()) {
-                        cls = x.range_ok(A.link0, A.link1) ? 1 : -1;
-                    } else {
-                        cls = (x.left_ok(e) && x.right_ok(e, A.link0)) ? 2 : -1;
-                    }
+                    if (node_node(A, P, theta) == 0) cls = 0;
+                    else if (A.leaf()) cls = x.range_ok(A.link0, A.link1) ? 1 : -1;
+                    else cls = (x.left_ok(e) && x.right_ok(e, A.link0)) ? 2 : -1;
                     if (cls < 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
                 } else {
                     const float4 q = __ldg(bodies + e);
                     const float pe[3] = {q.x, q.y, q.z};
-                    if (point_is_far(pe, P, theta)) {
-                        p2l(x, q, pc, part);
-                        ++npn;
-                        cls = 0;
-                    } else {
-                        cls = 1;
-                    }
+                    cls = point_is_far(pe, P, pthr) ? 0 : 1;
                 }
             }
             const int pos = stable_rank(cls, s_scan);
-            if (cls == 1) c1[pos] = e;
+            if (cls == 0) c0[pos] = e;
+            else if (cls == 1) c1[pos] = e;
             else if (cls == 2) c2[pos] = e;
         }
-        const int nleaf = s_scan.base[1], nnon = s_scan.base[2];
+        __syncthreads();  // the compacted lists are read by other threads below
+        const int nfar = s_scan.base[0], nleaf = s_scan.base[1], nnon = s_scan.base[2];
+
+        // ---- far entries into the local field: M2L (lock-step) or P2L (passive tree) ----
+        float part[F];
+#pragma unroll
+        for (int a = 0; a < F; ++a) part[a] = 0.f;
+        for (int i = tid; i < nfar; i += kThreads) {
+            const int e = c0[i];
+            if (type == kLockstep) {
+                m2l(x, e, load_node(nodes, e), pc, part);
+                ++nnn;
+            } else {
+                p2l(x, __ldg(bodies + e), pc, part);
+                ++npn;
+            }
+        }
         block_add_field(part, s_field, s_red);
 
         if (P.leaf()) {
-            // ---- passive leaf: near field (activeTree walks or close-body pairs), then L2P ----
-            const int nnear = (type == kLockstep) ? nleaf + nnon : nleaf;
-            for (int b0 = pfirst; b0 < pend; b0 += kThreads) {
-                const int nb = min(kThreads, pend - b0);
-                const int groups = kThreads / nb;
-                const int bi = tid % nb, g = tid / nb;
-                float v[3] = {0.f, 0.f, 0.f};
-                if (g < groups) {
-                    const float4 q = __ldg(bodies + b0 + bi);
-                    const float p[3] = {q.x, q.y, q.z};
-                    for (int r = g; r < nnear; r += groups) {
-                        if (type == kLockstep) {
-                            active_tree(x, r < nleaf ? c1[r] : c2[r - nleaf], p, v, npp, nnp, err);
-                        } else {
-                            pair(x, __ldg(bodies + c1[r]), p, v);
-                            ++npp;
-                        }
-                    }
-                }
-                s_part[tid][0] = v[0];
-                s_part[tid][1] = v[1];
-                s_part[tid][2] = v[2];
-                __syncthreads();
-                if (tid < nb) {
-                    float s[3] = {0.f, 0.f, 0.f};
-                    for (int k = 0; k < groups; ++k) {
-                        s[0] += s_part[k * nb + tid][0];
-                        s[1] += s_part[k * nb + tid][1];
-                        s[2] += s_part[k * nb + tid][2];
-                    }
-                    const float4 q = __ldg(bodies + b0 + tid);
-                    const float o[3] = {fsub(q.x, pc[0]), fsub(q.y, pc[1]), fsub(q.z, pc[2])};
-                    float a[3];
-                    st::field_at(s_field, o, a);
-                    float4 w = acc[b0 + tid];
-                    w.x += s[0] + a[0];
-                    w.y += s[1] + a[1];
-                    w.z += s[2] + a[2];
-                    acc[b0 + tid] = w;
+            // ---- passive leaf: L2P of this task's field; the near field goes to the leaf's items ----
+            for (int b = pfirst + tid; b < pend; b += kThreads) {
+                const float4 q = __ldg(bodies + b);
+                const float o[3] = {fsub(q.x, pc[0]), fsub(q.y, pc[1]), fsub(q.z, pc[2])};
+                float a[3];
+                st::field_at(s_field, o, a);
+                float4 w = acc[b];
+                w.x += a[0];
+                w.y += a[1];
+                w.z += a[2];
+                acc[b] = w;
+            }
+            if (type == kLockstep) {
+                append_item(pool, pk, pfirst, P.size, kItemRoots, c1, nleaf, c2, nnon, err, &s_slot);
+            } else {
+                // close bodies as runs of consecutive indices: run starts in c0 (free once the far
+                // terms are summed), then (first body, length) pairs in c2 (room for 2 len words)
+                for (int i0 = 0; i0 < nleaf; i0 += kThreads) {
+                    const int i = i0 + tid;
+                    const bool start = i < nleaf && (i == 0 || c1[i] != c1[i - 1] + 1);
+                    const int pos = stable_rank(start ? 0 : -1, s_scan);
+                    if (start) c0[pos - nfar] = i;  // base[0] already counted the far entries
                 }
                 __syncthreads();
+                const int runs = s_scan.base[0] - nfar;
+                for (int r = tid; r < runs; r += kThreads) {
+                    const int i = c0[r];
+                    const int next = r + 1 < runs ? c0[r + 1] : nleaf;
+                    c2[2 * r] = c1[i];
+                    c2[2 * r + 1] = next - i;
+                }
+                __syncthreads();
+                append_item(pool, pk, pfirst, P.size, kItemBodies, c2, 2 * runs, c2, 0, err, &s_slot);
             }
             continue;
         }
@@ -629,14 +654,14 @@ __global__ void __launch_bounds__(kThreads) dual_kernel(DualNodes nodes, const i
         }
     }
 
-    // interaction counts in the order {particle-particle, node-particle, particle-node, node-node}
-    const unsigned long long c[4] = {npp, nnp, npn, nnn};
+    // interaction counts {particle-node, node-node} (the near kernel counts the other two)
+    const unsigned long long c[2] = {npn, nnn};
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < 2; ++k) {
         unsigned long long v = c[k];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if ((tid & 31) == 0 && v) atomicAdd(counts + k, v);
+        if ((tid & 31) == 0 && v) atomicAdd(counts + 2 + k, v);
     }
 }
 
@@ -711,6 +736,201 @@ __global__ void load_balanced_break_kernel(DualNodes nodes, const int *__restric
     *num_roots = len;
 }
 
+
+// ---------------------------------------------------------------------------------------------
+// Near field of the passive leaves (second kernel).
+
+constexpr int kNearThreads = 256;
+constexpr int kNearWarps = kNearThreads / 32;
+constexpr int kNearStack = kMaxTreeDepth + 4;  // (node, lane mask) entries of one warp's walk
+constexpr int kPriv = 16;                      // queued M2P nodes per lane
+
+struct NearWarp {
+    int2 stack[kNearStack];
+    int priv[kPriv][32];  // [slot][lane]
+    float4 tile[32];      // staged source bodies
+};
+
+// Pairs of the warp's targets (lanes in `mine`) with sources src(0..m): the warp stages 32 at a
+// time in shared memory and every lane reads them back as broadcasts.
+template<typename Src>
+__device__ __forceinline__ void pair_tile(const Ctx &x, NearWarp &w, int m, Src src, bool mine, const float p[3],
+                                          float a[3]) {
+    const int lane = threadIdx.x & 31;
+    for (int j0 = 0; j0 < m; j0 += 32) {
+        const int c = min(32, m - j0);
+        w.tile[lane] = lane < c ? src(j0 + lane) : make_float4(0.f, 0.f, 0.f, 0.f);
+        __syncwarp();
+        if (mine) {
+            int k = 0;
+            for (; k + 4 <= c; k += 4) {
+                pair(x, w.tile[k], p, a);
+                pair(x, w.tile[k + 1], p, a);
+                pair(x, w.tile[k + 2], p, a);
+                pair(x, w.tile[k + 3], p, a);
+            }
+            for (; k < c; ++k) pair(x, w.tile[k], p, a);
+        }
+        __syncwarp();
+    }
+}
+
+// M2P terms queued by each lane, evaluated target-major (each lane its own queue).
+__device__ __noinline__ void flush_priv(const Ctx &x, NearWarp &w, int len, const float p[3], float a[3]) {
+    const int lane = threadIdx.x & 31;
+    const int maxlen = __reduce_max_sync(0xffffffffu, (unsigned) len);
+    for (int i = 0; i < maxlen; ++i) {
+        if (i < len) {
+            const int k = w.priv[i][lane];
+            node_particle3(x, k, load_node(x.nodes, k), p, a);
+        }
+    }
+    __syncwarp();
+}
+
+// activeTree (activeTree.h:24-79) from `root` for the warp's targets (lanes in `vmask`): one stack
+// entry per node with the mask of lanes that still descend. Approximated nodes are queued per lane.
+__device__ void warp_walk(const Ctx &x, NearWarp &w, int root, unsigned vmask, const float p[3], float a[3], int &plen,
+                          unsigned long long &npp, unsigned long long &nnp, uint32_t *err) {
+    const int lane = threadIdx.x & 31;
+    int sp = 1;
+    if (lane == 0) w.stack[0] = make_int2(root, (int) vmask);
+    __syncwarp();
+    while (sp > 0) {
+        --sp;
+        const int2 e = w.stack[sp];
+        __syncwarp();
+        const int k = e.x;
+        const unsigned m = (unsigned) e.y;
+        const DNode nd = load_node(x.nodes, k);
+        const bool in = (m >> lane) & 1u;
+        const bool ap = in && approx_for_point(nd, __ldg(x.nodes.thr + k), p);
+        if (ap) {
+            w.priv[plen][lane] = k;
+            ++plen;
+            ++nnp;
+        }
+        if (__any_sync(0xffffffffu, plen == kPriv)) {
+            __syncwarp();
+            flush_priv(x, w, plen, p, a);
+            plen = 0;
+        }
+        const unsigned need = m & ~__ballot_sync(0xffffffffu, ap);
+        if (need == 0) continue;
+        if (nd.leaf()) {
+            if (!x.range_ok(nd.link0, nd.link1)) {
+                if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
+                continue;
+            }
+            const bool mine = (need >> lane) & 1u;
+            const int first = nd.link0;
+            pair_tile(x, w, nd.link1 - nd.link0, [&](int j) { return __ldg(x.bodies + first + j); }, mine, p, a);
+            if (mine) npp += (unsigned long long) (nd.link1 - nd.link0);
+        } else {
+            if (!x.left_ok(k) || !x.right_ok(k, nd.link0)) {
+                if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
+                continue;
+            }
+            if (sp + 2 > kNearStack) {
+                if (lane == 0) atomicOr(err, (uint32_t) kErrStackOverflow);
+                return;
+            }
+            if (lane == 0) {
+                w.stack[sp] = make_int2(nd.link0, (int) need);  // right child, second
+                w.stack[sp + 1] = make_int2(k + 1, (int) need);  // left child, first
+            }
+            sp += 2;
+            __syncwarp();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kNearThreads, 2) near_kernel(DualNodes nodes, const int *__restrict__ num_nodes,
+                                                               const float4 *__restrict__ bodies, int n, float G,
+                                                               float eps, float theta, float4 *__restrict__ acc,
+                                                               unsigned long long *__restrict__ counts, NearPool pool,
+                                                               uint32_t *__restrict__ err) {
+    __shared__ NearWarp s_warps[kNearWarps];
+    const int lane = threadIdx.x & 31;
+    NearWarp &w = s_warps[threadIdx.x >> 5];
+    const Ctx x{nodes, bodies, G, eps, theta, *num_nodes, n};
+    const unsigned long long nunits = min(pool.counters[2], (unsigned long long) pool.unit_cap);
+    const unsigned long long nitems = min(pool.counters[0], (unsigned long long) pool.item_cap);
+    unsigned long long npp = 0, nnp = 0;
+    for (;;) {
+        unsigned long long u = 0;
+        if (lane == 0) u = atomicAdd(&pool.counters[3], 1ull);
+        u = __shfl_sync(0xffffffffu, u, 0);
+        if (u >= nunits) break;
+        const int2 unit = pool.units[u];
+        const int leaf = unit.x;
+        if (leaf < 0 || leaf >= x.nn) {
+            if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
+            continue;
+        }
+        const int2 lr = __ldg(nodes.link + leaf);
+        const int tend = min(lr.y, unit.y + 32);
+        if (lr.y < 0 || !x.range_ok(unit.y, tend)) {
+            if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
+            continue;
+        }
+        const int t = unit.y + lane;
+        const bool valid = t < tend;
+        const float4 q = valid ? __ldg(bodies + t) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float p[3] = {q.x, q.y, q.z};
+        const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+        float a[3] = {0.f, 0.f, 0.f};
+        int plen = 0;
+        int guard = 0;
+        for (int it = pool.head[leaf]; it >= 0; ++guard) {
+            if ((unsigned long long) it >= nitems || guard > (1 << 24)) {
+                if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
+                break;
+            }
+            const int4 item = pool.items[it];
+            const int *words = pool.words + item.z;
+            if (item.y == kItemBodies) {
+                // runs of consecutive close bodies: (first body, length) pairs
+                for (int r = 0; r + 1 < item.w; r += 2) {
+                    const int b0 = words[r], len = words[r + 1];
+                    if (len < 0 || len > x.n || !x.range_ok(b0, b0 + len)) {
+                        if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
+                        continue;
+                    }
+                    pair_tile(x, w, len, [&](int j) { return __ldg(bodies + b0 + j); }, valid, p, a);
+                    if (valid) npp += (unsigned long long) len;
+                }
+            } else {
+                for (int r = 0; r < item.w; ++r) {
+                    const int root = words[r];
+                    if (root < 0 || root >= x.nn) {
+                        if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
+                        continue;
+                    }
+                    warp_walk(x, w, root, vmask, p, a, plen, npp, nnp, err);
+                }
+            }
+            it = item.x;
+        }
+        if (__any_sync(0xffffffffu, plen > 0)) flush_priv(x, w, plen, p, a);
+        if (valid) {
+            float4 v = acc[t];
+            v.x += a[0];
+            v.y += a[1];
+            v.z += a[2];
+            acc[t] = v;
+        }
+    }
+    const unsigned long long c[2] = {npp, nnp};
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        unsigned long long v = c[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0 && v) atomicAdd(counts + k, v);
+    }
+}
+
 }  // namespace
 
 void launch_dual_traverse(const DualNodes &nodes, const int *num_nodes, const float4 *bodies, int64_t n, float G,
@@ -718,10 +938,26 @@ void launch_dual_traverse(const DualNodes &nodes, const int *num_nodes, const fl
                           uint32_t *err, cudaStream_t s) {
     if (n <= 0) return;
     cudaMemsetAsync(acc, 0, (size_t) n * sizeof(float4), s);
+    cudaMemsetAsync(ws.near.head, 0xFF, (size_t) ws.near.head_cap * sizeof(int), s);
+    cudaMemsetAsync(ws.near.counters, 0, 4 * sizeof(unsigned long long), s);
     load_balanced_break_kernel<<<1, 32, 0, s>>>(nodes, num_nodes, ws.roots, ws.num_roots, err);
     dual_kernel<<<kDualRoots, kThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta, acc, counts,
                                                 ws.roots, ws.num_roots, ws.arena, (int) ws.arena_words, ws.tasks,
-                                                err);
+                                                ws.near, err);
+    near_kernel<<<ws.near_blocks, kNearThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta, acc,
+                                                        counts, ws.near, err);
+}
+
+void dual_near_sizes(int64_t n, int64_t *item_cap, int64_t *word_cap) {
+    *item_cap = 4 * n + 65536;
+    *word_cap = std::min<int64_t>(64 * n + (int64_t(1) << 22), (int64_t(1) << 31) - 1);
+}
+
+int dual_near_blocks(int device) {
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, near_kernel, kNearThreads, 0);
+    return std::max(1, sms * std::max(per_sm, 1));
 }
 
 int64_t dual_arena_words(int64_t n) {

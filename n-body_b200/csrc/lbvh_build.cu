@@ -406,10 +406,29 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(int n, TreeWorkspace tw,
     if (i == 0) *tw.num_nodes = tw.cnt[i];
 }
 
+// Smallest float s >= 0 with RN(sqrt(s)) >= b (sqrt is monotone, so the set is an up-set).
+__device__ float sqrt_threshold(float b) {
+    if (isnan(b)) return b;
+    if (isinf(b)) return b;
+    auto pred = [&](float v) { return __fsqrt_rn(v) >= b; };
+    float v = fmul(b, b);
+    if (isinf(v)) v = FLT_MAX;
+    if (pred(v)) {
+        for (int k = 0; k < 64; ++k) {
+            const float pv = nextafterf(v, 0.f);
+            if (pv >= 0.f && pv < v && pred(pv)) v = pv;
+            else break;
+        }
+    } else {
+        for (int k = 0; k < 64 && !pred(v); ++k) v = nextafterf(v, __int_as_float(0x7f800000));
+    }
+    return v;
+}
+
 // Dual-tree node arrays (order 3 summaries): bounding box, centre of mass and mass, packed
-// quadrupole and octupole, links.
+// quadrupole and octupole, links, and the criterion thresholds for theta.
 __device__ void write_dual_record(const DualNodes &nodes, int pre, const Summ<3> &s, int first, int last,
-                                  int link0, int link1, uint32_t *err) {
+                                  int link0, int link1, float theta, uint32_t *err) {
     if (pre < 0 || pre >= nodes.capacity) {
         atomicOr(err, (uint32_t) kErrNodeOverflow);
         return;
@@ -419,6 +438,10 @@ __device__ void write_dual_record(const DualNodes &nodes, int pre, const Summ<3>
     const float diag = __fsqrt_rn(fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz)));
     nodes.bmin[pre] = make_float4(s.bmin[0], s.bmin[1], s.bmin[2], __int_as_float(last - first + 1));
     nodes.bmax[pre] = make_float4(s.bmax[0], s.bmax[1], s.bmax[2], diag);
+    // DiagonalOverSeparation (DiagonalOverSeparation.h:29-49): RN(diag / sep) < theta for the
+    // active node, RN(RN(3 diag) / sep) < theta for the passive node
+    const float b_near = mac_threshold(diag, theta), b_far = mac_threshold(fmul(3.0f, diag), theta);
+    nodes.thr[pre] = make_float4(b_near, sqrt_threshold(b_near), b_far, sqrt_threshold(b_far));
     nodes.com[pre] = make_float4(s.com[0], s.com[1], s.com[2], s.M);
     float4 *q = nodes.q + (int64_t) pre * 4;
     q[0] = make_float4(s.q[0], s.q[1], s.q[2], s.q[3]);
@@ -428,7 +451,8 @@ __device__ void write_dual_record(const DualNodes &nodes, int pre, const Summ<3>
     nodes.link[pre] = make_int2(link0, link1);
 }
 
-__global__ void __launch_bounds__(kThreads) emit_dual_kernel(int n, TreeWorkspace tw, DualNodes nodes, uint32_t *err) {
+__global__ void __launch_bounds__(kThreads) emit_dual_kernel(int n, TreeWorkspace tw, DualNodes nodes, float theta,
+                                                              uint32_t *err) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1 || !tw.splittable[i]) return;
     int pre = 0;
@@ -447,22 +471,22 @@ __global__ void __launch_bounds__(kThreads) emit_dual_kernel(int n, TreeWorkspac
     const int lslot = slot_of(lc, n);
     const int right_pre = pre + 1 + tw.cnt[lslot];
     const int2 ri = tw.range[i];
-    write_dual_record(nodes, pre, load_slot<3>(tw, i), ri.x, ri.y, right_pre, -1 - ri.x, err);
+    write_dual_record(nodes, pre, load_slot<3>(tw, i), ri.x, ri.y, right_pre, -1 - ri.x, theta, err);
     if (is_final_leaf(tw.splittable, lc)) {
         int2 r = lc < 0 ? make_int2(~lc, ~lc) : tw.range[lc];
-        write_dual_record(nodes, pre + 1, load_slot<3>(tw, lslot), r.x, r.y, r.x, r.y + 1, err);
+        write_dual_record(nodes, pre + 1, load_slot<3>(tw, lslot), r.x, r.y, r.x, r.y + 1, theta, err);
     }
     if (is_final_leaf(tw.splittable, rc)) {
         int2 r = rc < 0 ? make_int2(~rc, ~rc) : tw.range[rc];
-        write_dual_record(nodes, right_pre, load_slot<3>(tw, slot_of(rc, n)), r.x, r.y, r.x, r.y + 1, err);
+        write_dual_record(nodes, right_pre, load_slot<3>(tw, slot_of(rc, n)), r.x, r.y, r.x, r.y + 1, theta, err);
     }
     if (i == 0) *tw.num_nodes = tw.cnt[i];
 }
 
 __global__ void root_leaf_dual_kernel(const float4 *__restrict__ bodies, int n, TreeWorkspace tw, DualNodes nodes,
-                                      uint32_t *err) {
+                                      float theta, uint32_t *err) {
     if (n > 1 && tw.splittable[0]) return;
-    write_dual_record(nodes, 0, leaf_summary<3>(bodies, 0, n - 1), 0, n - 1, 0, n, err);
+    write_dual_record(nodes, 0, leaf_summary<3>(bodies, 0, n - 1), 0, n - 1, 0, n, theta, err);
     *tw.num_nodes = 1;
 }
 
@@ -479,8 +503,8 @@ __global__ void root_leaf_kernel(const float4 *__restrict__ bodies, int n, TreeW
 
 }  // namespace
 
-void launch_build_dual_tree(const uint64_t *sorted_codes, const float4 *bodies, int64_t n64, int leaf, TreeWorkspace &tw,
-                            const DualNodes &nodes, uint32_t *err, cudaStream_t s) {
+void launch_build_dual_tree(const uint64_t *sorted_codes, const float4 *bodies, int64_t n64, int leaf, float theta,
+                            TreeWorkspace &tw, const DualNodes &nodes, uint32_t *err, cudaStream_t s) {
     const int n = (int) n64;
     if (n <= 0) {
         cudaMemsetAsync(tw.num_nodes, 0, sizeof(int), s);
@@ -493,9 +517,9 @@ void launch_build_dual_tree(const uint64_t *sorted_codes, const float4 *bodies, 
                                                   tw.parent, tw.splittable);
         cudaMemsetAsync(tw.visit, 0, (size_t) internal * sizeof(int), s);
         summarize_kernel<3><<<blocks, kThreads, 0, s>>>(bodies, n, tw, err);
-        emit_dual_kernel<<<blocks, kThreads, 0, s>>>(n, tw, nodes, err);
+        emit_dual_kernel<<<blocks, kThreads, 0, s>>>(n, tw, nodes, theta, err);
     }
-    root_leaf_dual_kernel<<<1, 1, 0, s>>>(bodies, n, tw, nodes, err);
+    root_leaf_dual_kernel<<<1, 1, 0, s>>>(bodies, n, tw, nodes, theta, err);
 }
 
 void launch_build_tree(const uint64_t *sorted_codes, const float4 *bodies, int64_t n64, int leaf, int order,

@@ -109,6 +109,7 @@ enum DeviceError : uint32_t {
     kErrStackOverflow = 1u << 3,     // traversal stack full (a push was dropped)
     kErrTraverseLimit = 1u << 4,     // traversal met an invalid link or exceeded its round limit
     kErrDualArena = 1u << 5,         // dual-tree list or task storage exhausted
+    kErrNearPool = 1u << 6,          // dual-tree near-field pool too small (the host grows it and retries)
 };
 
 // ---- launchers (stream-ordered; defined in the .cu files) ----
@@ -173,26 +174,43 @@ void launch_build_tree(const uint64_t *sorted_codes, const float4 *bodies, int64
 // diagonal length as BoundingBox::diagonalLength computes it),
 // com = (centre of mass, mass), q = 4 float4 per node: Q2 (6) then Q3 (10);
 // link = (first body, end body) at a leaf, (right child, -1 - first body) at an internal node.
+// thr = exact criterion thresholds for the configured theta: (B, S) with
+// RN(diag / sep) < theta  <=>  sep >= B  <=>  (when one separation vector is zero) |v|^2 >= S,
+// and the same pair for the passive test RN(3 diag / sep) < theta.
 struct DualNodes {
-    float4 *bmin = nullptr, *bmax = nullptr, *com = nullptr, *q = nullptr;
+    float4 *bmin = nullptr, *bmax = nullptr, *com = nullptr, *q = nullptr, *thr = nullptr;
     int2 *link = nullptr;
     int64_t capacity = 0;
 };
-void launch_build_dual_tree(const uint64_t *sorted_codes, const float4 *bodies, int64_t n, int leaf, TreeWorkspace &tw,
-                            const DualNodes &nodes, uint32_t *err, cudaStream_t s);
+void launch_build_dual_tree(const uint64_t *sorted_codes, const float4 *bodies, int64_t n, int leaf, float theta,
+                            TreeWorkspace &tw, const DualNodes &nodes, uint32_t *err, cudaStream_t s);
 
 // dualtree.cu
 constexpr int kDualRoots = 256;   // starting passive nodes (Tree::loadBalancedBreak(256))
 constexpr int kDualTasks = 4096;  // task records per block
+// Near-field work handed from the traversal to the near-field kernel: per passive leaf, a list
+// of items (activeTree roots, or close bodies) whose payload lives in one word pool.
+struct NearPool {
+    int *head = nullptr;                  // per node: newest item of the passive leaf, -1 if none
+    int4 *items = nullptr;                // (next item, kind, payload offset, payload count)
+    int *words = nullptr;                 // payload: node or body indices
+    int2 *units = nullptr;                // (passive leaf, first target) per 32-target unit
+    unsigned long long *counters = nullptr;  // items, words, units, unit cursor
+    int64_t head_cap = 0, item_cap = 0, word_cap = 0, unit_cap = 0;
+};
 struct DualWorkspace {
     int *roots = nullptr;           // starting passive nodes (at most kDualRoots)
     int *num_roots = nullptr;
     int *arena = nullptr;           // per block: arena_words words of lists and local fields
     int *tasks = nullptr;           // per block: kDualTasks task records of 6 ints
     int64_t arena_words = 0;
+    NearPool near;
+    int near_blocks = 0;            // resident blocks of the near-field kernel
 };
-// Arena words per block for n bodies.
+// Arena words per block, near-pool sizes and the near kernel's resident grid for n bodies.
 int64_t dual_arena_words(int64_t n);
+void dual_near_sizes(int64_t n, int64_t *item_cap, int64_t *word_cap);
+int dual_near_blocks(int device);
 void launch_dual_traverse(const DualNodes &nodes, const int *num_nodes, const float4 *bodies, int64_t n, float G,
                           float eps, float theta, float4 *acc, unsigned long long *counts, DualWorkspace &ws,
                           uint32_t *err, cudaStream_t s);

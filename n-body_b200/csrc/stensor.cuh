@@ -54,12 +54,23 @@ __device__ __forceinline__ float comp(const float v[3], int i) { return i == 0 ?
 // (Gravity.h:43-58).
 struct Coef {
     float g1, g2, g3, g4;
+    Coef() = default;
     __device__ explicit Coef(float r) {
         const float r2 = r * r, r3 = r * r2, r4 = r * r3, r5 = r * r4;
         g1 = (-1.0f / r2) / r;
         g2 = (3.0f / r3) / r2;
         g3 = (-15.0f / r4) / r3;
         g4 = (105.0f / r5) / r4;
+    }
+    // the same coefficients from 1 / r: g_k = (-1)^k (2k-1)!! / r^(2k+1)
+    __device__ static Coef from_inverse(float inv) {
+        Coef c;
+        const float i2 = inv * inv, i3 = inv * i2, i5 = i3 * i2, i7 = i5 * i2, i9 = i7 * i2;
+        c.g1 = -i3;
+        c.g2 = 3.0f * i5;
+        c.g3 = -15.0f * i7;
+        c.g4 = 105.0f * i9;
+        return c;
     }
 };
 

@@ -189,3 +189,18 @@ def test_dual_rejects_batches_and_other_orders(nb):
     with dual_solver(nb, pm) as s:
         with pytest.raises(nb.NBodyError):
             s.set_instances([50, 50], pm)
+
+
+def test_dual_pool_growth_theta_zero(nb):
+    """theta = 0 at N = 60000 asks for far more near-field roots than the initial pool holds: the
+    context grows the pool and reruns the pass; the result is every pair, as the direct sum."""
+    pm, _ = nb.scenarios.uniform_ball(60000, seed=12)
+    with dual_solver(nb, pm, leaf=16, theta=0.0) as s:
+        acc = s.update_accelerations()
+        c = s.counts()
+    assert c["particle_particle"] == 60000 * 60000
+    assert c["node_particle"] == c["particle_node"] == c["node_node"] == 0
+    with nb.NaiveSolver(bodies=pm, rule=nb.Gravity(1.0, 1e-4)) as d:
+        ref = d.update_accelerations()
+    err = rel_err(acc, ref)
+    assert np.sqrt(np.mean(err ** 2)) < 1e-5
