@@ -156,33 +156,6 @@ __device__ __forceinline__ float soft_inv_r(const float R[3], float eps) {
     return rsqrtf(fmaf(R[0], R[0], fmaf(R[1], R[1], fmaf(R[2], R[2], eps))));
 }
 
-// Gravity::particleParticle (Gravity.h:199-209), added into a
-__device__ __forceinline__ void pair(const Ctx &x, float4 b, const float p[3], float a[3]) {
-    const float R[3] = {p[0] - b.x, p[1] - b.y, p[2] - b.z};
-    if (R[0] == 0.f && R[1] == 0.f && R[2] == 0.f) return;
-    const float inv = soft_inv_r(R, x.eps);
-    const float s = (b.w * x.G) * (inv * inv * inv);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) a[i] = fmaf(-R[i], s, a[i]);
-}
-
-// Gravity::nodeParticle for MultipoleMassSummary<3> (Gravity.h:239-259), added into a
-__device__ void node_particle3(const Ctx &x, int k, const DNode &n, const float p[3], float a[3]) {
-    const float R[3] = {p[0] - n.com[0], p[1] - n.com[1], p[2] - n.com[2]};
-    if (R[0] == 0.f && R[1] == 0.f && R[2] == 0.f) return;
-    const float inv = soft_inv_r(R, x.eps);
-    const st::Coef c = st::Coef::from_inverse(inv);
-    float q2[6], q3[10], d3[10], d4[15], v3[3], v4[3];
-    load_q(x.nodes, k, q2, q3);
-    st::D3(R, c, d3);
-    st::D4(R, c, d4);
-    st::t3_dot_t2(d3, q2, v3);
-    st::t4_dot_t3(d4, q3, v4);
-    const float mono = -n.M * (inv * inv * inv);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) a[i] += x.G * (R[i] * mono + v3[i] / 2.0f - v4[i] / 6.0f);
-}
-
 // Gravity::nodeNode for MultipoleMassSummary<3> -> MultipoleAccelerationSummary<4> (M2L,
 // Gravity.h:352-392), added into the local field f about pc. As in the reference, the moment
 // terms carry no factor G.
@@ -739,62 +712,107 @@ __global__ void load_balanced_break_kernel(DualNodes nodes, const int *__restric
 
 // ---------------------------------------------------------------------------------------------
 // Near field of the passive leaves (second kernel).
+//
+// A unit is up to 32 targets of one passive leaf. With T targets, the warp runs G = 32 / T
+// replicas of each: lane l serves target l % T as replica l / T. Decisions are per target (every
+// replica of a target computes the same criterion); pair tiles and queued M2P terms are split
+// between the replicas, whose partial sums are added in replica order at the end of the unit. So
+// short leaves still keep the whole warp busy. Terms are summed without G; G is applied once.
 
 constexpr int kNearThreads = 256;
 constexpr int kNearWarps = kNearThreads / 32;
-constexpr int kNearStack = kMaxTreeDepth + 4;  // (node, lane mask) entries of one warp's walk
-constexpr int kPriv = 16;                      // queued M2P nodes per lane
+constexpr int kNearStack = kMaxTreeDepth + 4;  // (node, target mask) entries of one warp's walk
+constexpr int kPriv = 16;                      // queued M2P nodes per target
 
 struct NearWarp {
     int2 stack[kNearStack];
-    int priv[kPriv][32];  // [slot][lane]
-    float4 tile[32];      // staged source bodies
+    int priv[kPriv][32];  // [slot][target]
+    float4 tile[32];      // staged source bodies, then the replicas' partial sums
 };
 
-// Pairs of the warp's targets (lanes in `mine`) with sources src(0..m): the warp stages 32 at a
-// time in shared memory and every lane reads them back as broadcasts.
-template<typename Src>
-__device__ __forceinline__ void pair_tile(const Ctx &x, NearWarp &w, int m, Src src, bool mine, const float p[3],
-                                          float a[3]) {
+struct Lane {
+    int t, r, T, G;     // target, replica, targets in the unit, replicas
+    bool active;        // r < G
+};
+
+// Gravity::particleParticle (Gravity.h:199-209) without G, added into a. With eps > 0 a source at
+// the target's own position contributes -0 * s = 0 and needs no test; with eps = 0 it is skipped.
+template<bool EPS0>
+__device__ __forceinline__ void pair_nog(float4 b, const float p[3], float eps, float a[3]) {
+    const float rx = p[0] - b.x, ry = p[1] - b.y, rz = p[2] - b.z;
+    const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps)));
+    if (EPS0 && r2 == 0.f) return;
+    const float inv = rsqrtf(r2);
+    const float s = b.w * (inv * inv * inv);
+    a[0] = fmaf(-rx, s, a[0]);
+    a[1] = fmaf(-ry, s, a[1]);
+    a[2] = fmaf(-rz, s, a[2]);
+}
+
+// Gravity::nodeParticle for MultipoleMassSummary<3> (Gravity.h:239-259) without G, added into a.
+__device__ __noinline__ void m2p_nog(const Ctx &x, int k, const float p[3], float a[3]) {
+    const float4 c4 = __ldg(x.nodes.com + k);
+    const float R[3] = {p[0] - c4.x, p[1] - c4.y, p[2] - c4.z};
+    if (R[0] == 0.f && R[1] == 0.f && R[2] == 0.f) return;
+    const float inv = soft_inv_r(R, x.eps);
+    const st::Coef c = st::Coef::from_inverse(inv);
+    float q2[6], q3[10], d3[10], d4[15], v3[3], v4[3];
+    load_q(x.nodes, k, q2, q3);
+    st::D3(R, c, d3);
+    st::D4(R, c, d4);
+    st::t3_dot_t2(d3, q2, v3);
+    st::t4_dot_t3(d4, q3, v4);
+    const float mono = -c4.w * (inv * inv * inv);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) a[i] += R[i] * mono + v3[i] / 2.0f - v4[i] / 6.0f;
+}
+
+// Pairs of the unit's targets with sources src(0..m) for lanes in `mine`: 32 sources at a time
+// are staged in shared memory; replica r takes sources r, r + G, ... of each tile.
+template<bool EPS0, typename Src>
+__device__ __forceinline__ void pair_tile(NearWarp &w, const Lane &L, int m, Src src, bool mine, const float p[3],
+                                          float eps, float a[3]) {
     const int lane = threadIdx.x & 31;
     for (int j0 = 0; j0 < m; j0 += 32) {
         const int c = min(32, m - j0);
         w.tile[lane] = lane < c ? src(j0 + lane) : make_float4(0.f, 0.f, 0.f, 0.f);
         __syncwarp();
         if (mine) {
-            int k = 0;
-            for (; k + 4 <= c; k += 4) {
-                pair(x, w.tile[k], p, a);
-                pair(x, w.tile[k + 1], p, a);
-                pair(x, w.tile[k + 2], p, a);
-                pair(x, w.tile[k + 3], p, a);
+            int k = L.r;
+            const int G = L.G;
+            for (; k + 3 * G < c; k += 4 * G) {
+                pair_nog<EPS0>(w.tile[k], p, eps, a);
+                pair_nog<EPS0>(w.tile[k + G], p, eps, a);
+                pair_nog<EPS0>(w.tile[k + 2 * G], p, eps, a);
+                pair_nog<EPS0>(w.tile[k + 3 * G], p, eps, a);
             }
-            for (; k < c; ++k) pair(x, w.tile[k], p, a);
+            for (; k < c; k += G) pair_nog<EPS0>(w.tile[k], p, eps, a);
         }
         __syncwarp();
     }
 }
 
-// M2P terms queued by each lane, evaluated target-major (each lane its own queue).
-__device__ __noinline__ void flush_priv(const Ctx &x, NearWarp &w, int len, const float p[3], float a[3]) {
-    const int lane = threadIdx.x & 31;
-    const int maxlen = __reduce_max_sync(0xffffffffu, (unsigned) len);
-    for (int i = 0; i < maxlen; ++i) {
-        if (i < len) {
-            const int k = w.priv[i][lane];
-            node_particle3(x, k, load_node(x.nodes, k), p, a);
-        }
+// The M2P terms queued per target (by its replica 0), split between the target's replicas.
+__device__ void flush_priv(const Ctx &x, NearWarp &w, const Lane &L, int plen, const float p[3], float a[3]) {
+    __syncwarp();  // queue entries written by the targets' first replicas
+    const int len = __shfl_sync(0xffffffffu, plen, L.t);  // the target's queue length
+    const int most = (int) __reduce_max_sync(0xffffffffu, (unsigned) len);
+    for (int i0 = 0; i0 < most; i0 += L.G) {
+        const int i = i0 + L.r;
+        if (L.active && i < len) m2p_nog(x, w.priv[i][L.t], p, a);
     }
     __syncwarp();
 }
 
-// activeTree (activeTree.h:24-79) from `root` for the warp's targets (lanes in `vmask`): one stack
-// entry per node with the mask of lanes that still descend. Approximated nodes are queued per lane.
-__device__ void warp_walk(const Ctx &x, NearWarp &w, int root, unsigned vmask, const float p[3], float a[3], int &plen,
-                          unsigned long long &npp, unsigned long long &nnp, uint32_t *err) {
+// activeTree (activeTree.h:24-79) from `root` for the unit's targets (bits of `tmask`): one stack
+// entry per node with the targets that still descend; approximated nodes are queued per target.
+template<bool EPS0>
+__device__ void warp_walk(const Ctx &x, NearWarp &w, const Lane &L, int root, unsigned tmask, const float p[3],
+                          float a[3], int &plen, unsigned long long &npp, unsigned long long &nnp, uint32_t *err) {
     const int lane = threadIdx.x & 31;
+    const unsigned lead = L.T >= 32 ? 0xffffffffu : ((1u << L.T) - 1u);  // replica-0 lanes = target bits
     int sp = 1;
-    if (lane == 0) w.stack[0] = make_int2(root, (int) vmask);
+    if (lane == 0) w.stack[0] = make_int2(root, (int) tmask);
     __syncwarp();
     while (sp > 0) {
         --sp;
@@ -803,29 +821,30 @@ __device__ void warp_walk(const Ctx &x, NearWarp &w, int root, unsigned vmask, c
         const int k = e.x;
         const unsigned m = (unsigned) e.y;
         const DNode nd = load_node(x.nodes, k);
-        const bool in = (m >> lane) & 1u;
+        const bool in = L.active && ((m >> L.t) & 1u);
         const bool ap = in && approx_for_point(nd, __ldg(x.nodes.thr + k), p);
-        if (ap) {
-            w.priv[plen][lane] = k;
+        if (ap && L.r == 0) {
+            w.priv[plen][L.t] = k;
             ++plen;
             ++nnp;
         }
         if (__any_sync(0xffffffffu, plen == kPriv)) {
             __syncwarp();
-            flush_priv(x, w, plen, p, a);
+            flush_priv(x, w, L, plen, p, a);
             plen = 0;
         }
-        const unsigned need = m & ~__ballot_sync(0xffffffffu, ap);
+        const unsigned need = m & ~(__ballot_sync(0xffffffffu, ap) & lead);
         if (need == 0) continue;
         if (nd.leaf()) {
             if (!x.range_ok(nd.link0, nd.link1)) {
                 if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
                 continue;
             }
-            const bool mine = (need >> lane) & 1u;
+            const bool mine = L.active && ((need >> L.t) & 1u);
             const int first = nd.link0;
-            pair_tile(x, w, nd.link1 - nd.link0, [&](int j) { return __ldg(x.bodies + first + j); }, mine, p, a);
-            if (mine) npp += (unsigned long long) (nd.link1 - nd.link0);
+            pair_tile<EPS0>(w, L, nd.link1 - nd.link0, [&](int j) { return __ldg(x.bodies + first + j); }, mine, p,
+                            x.eps, a);
+            if (mine && L.r == 0) npp += (unsigned long long) (nd.link1 - nd.link0);
         } else {
             if (!x.left_ok(k) || !x.right_ok(k, nd.link0)) {
                 if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
@@ -845,6 +864,7 @@ __device__ void warp_walk(const Ctx &x, NearWarp &w, int root, unsigned vmask, c
     }
 }
 
+template<bool EPS0>
 __global__ void __launch_bounds__(kNearThreads, 2) near_kernel(DualNodes nodes, const int *__restrict__ num_nodes,
                                                                const float4 *__restrict__ bodies, int n, float G,
                                                                float eps, float theta, float4 *__restrict__ acc,
@@ -870,15 +890,20 @@ __global__ void __launch_bounds__(kNearThreads, 2) near_kernel(DualNodes nodes, 
         }
         const int2 lr = __ldg(nodes.link + leaf);
         const int tend = min(lr.y, unit.y + 32);
-        if (lr.y < 0 || !x.range_ok(unit.y, tend)) {
+        if (lr.y < 0 || !x.range_ok(unit.y, tend) || tend == unit.y) {
             if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
             continue;
         }
-        const int t = unit.y + lane;
-        const bool valid = t < tend;
-        const float4 q = valid ? __ldg(bodies + t) : make_float4(0.f, 0.f, 0.f, 0.f);
+        Lane L;
+        L.T = tend - unit.y;
+        L.G = 32 / L.T;
+        L.t = lane % L.T;
+        L.r = lane / L.T;
+        L.active = L.r < L.G;
+        const int t = unit.y + L.t;
+        const float4 q = __ldg(bodies + t);
         const float p[3] = {q.x, q.y, q.z};
-        const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+        const unsigned tmask = L.T >= 32 ? 0xffffffffu : ((1u << L.T) - 1u);
         float a[3] = {0.f, 0.f, 0.f};
         int plen = 0;
         int guard = 0;
@@ -897,8 +922,8 @@ __global__ void __launch_bounds__(kNearThreads, 2) near_kernel(DualNodes nodes, 
                         if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
                         continue;
                     }
-                    pair_tile(x, w, len, [&](int j) { return __ldg(bodies + b0 + j); }, valid, p, a);
-                    if (valid) npp += (unsigned long long) len;
+                    pair_tile<EPS0>(w, L, len, [&](int j) { return __ldg(bodies + b0 + j); }, L.active, p, eps, a);
+                    if (L.active && L.r == 0) npp += (unsigned long long) len;
                 }
             } else {
                 for (int r = 0; r < item.w; ++r) {
@@ -907,19 +932,30 @@ __global__ void __launch_bounds__(kNearThreads, 2) near_kernel(DualNodes nodes, 
                         if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
                         continue;
                     }
-                    warp_walk(x, w, root, vmask, p, a, plen, npp, nnp, err);
+                    warp_walk<EPS0>(x, w, L, root, tmask, p, a, plen, npp, nnp, err);
                 }
             }
             it = item.x;
         }
-        if (__any_sync(0xffffffffu, plen > 0)) flush_priv(x, w, plen, p, a);
-        if (valid) {
-            float4 v = acc[t];
-            v.x += a[0];
-            v.y += a[1];
-            v.z += a[2];
-            acc[t] = v;
+        if (__any_sync(0xffffffffu, plen > 0)) flush_priv(x, w, L, plen, p, a);
+        // replicas' partial sums, added in replica order
+        w.tile[lane] = make_float4(a[0], a[1], a[2], 0.f);
+        __syncwarp();
+        if (L.r == 0) {
+            float s0 = a[0], s1 = a[1], s2 = a[2];
+            for (int r = 1; r < L.G; ++r) {
+                const float4 v = w.tile[r * L.T + L.t];
+                s0 += v.x;
+                s1 += v.y;
+                s2 += v.z;
+            }
+            float4 o = acc[t];
+            o.x += G * s0;
+            o.y += G * s1;
+            o.z += G * s2;
+            acc[t] = o;
         }
+        __syncwarp();
     }
     const unsigned long long c[2] = {npp, nnp};
 #pragma unroll
@@ -944,8 +980,12 @@ void launch_dual_traverse(const DualNodes &nodes, const int *num_nodes, const fl
     dual_kernel<<<kDualRoots, kThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta, acc, counts,
                                                 ws.roots, ws.num_roots, ws.arena, (int) ws.arena_words, ws.tasks,
                                                 ws.near, err);
-    near_kernel<<<ws.near_blocks, kNearThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta, acc,
-                                                        counts, ws.near, err);
+    if (eps == 0.f)
+        near_kernel<true><<<ws.near_blocks, kNearThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta,
+                                                                  acc, counts, ws.near, err);
+    else
+        near_kernel<false><<<ws.near_blocks, kNearThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta,
+                                                                   acc, counts, ws.near, err);
 }
 
 void dual_near_sizes(int64_t n, int64_t *item_cap, int64_t *word_cap) {
@@ -956,7 +996,7 @@ void dual_near_sizes(int64_t n, int64_t *item_cap, int64_t *word_cap) {
 int dual_near_blocks(int device) {
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, near_kernel, kNearThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, near_kernel<false>, kNearThreads, 0);
     return std::max(1, sms * std::max(per_sm, 1));
 }
 
