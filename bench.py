@@ -662,10 +662,11 @@ DUAL_THETA = 0.4
 DUAL_LEAF = 64           # LinearBVH's default maxLeafSize (LinearBVH.h:88)
 DUAL_SOFTENING = 0.005
 # Flop weights of the dual-tree interactions, counted from n-body_b200/csrc/dualtree.cu and
-# stensor.cuh after unrolling (FMA = 2): pair 20; M2P with octupole moments (D3, D4, two
-# contractions) 555; P2L into an order-4 field (D2..D4) 440; M2L (D2..D4, three contractions) 820.
+# stensor.cuh after unrolling (FMA = 2): pair 20; M2P with octupole moments (the two contractions
+# grouped for symmetric moments) 125; P2L into an order-4 field (D2..D4) 440; M2L (D2..D4, three
+# contractions) 820.
 DUAL_PAIR_FLOPS = 20
-DUAL_NP_FLOPS = 555
+DUAL_NP_FLOPS = 125
 DUAL_PN_FLOPS = 440
 DUAL_NN_FLOPS = 820
 

@@ -242,6 +242,65 @@ __device__ int stable_rank(int cls, Scan3 &s) {
     return pos;
 }
 
+// Stable block-wide partition of list[0..len) into classes 0, 1, 2 (c0, c1, c2; -1 drops the
+// entry), appending after the counts already in s.base. Each thread takes 4 consecutive entries
+// per round, so their loads overlap and one prefix sum serves 4 * kThreads entries. Every thread
+// of the block must call it.
+template<typename Classify>
+__device__ void stable_partition4(const int *list, int len, int *c0, int *c1, int *c2, Scan3 &s, Classify classify) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i0 = 0; i0 < len; i0 += 4 * kThreads) {
+        const int b = i0 + 4 * (int) threadIdx.x;
+        int e[4], cls[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) e[j] = b + j < len ? list[b + j] : -1;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) cls[j] = b + j < len ? classify(e[j]) : -1;
+        int v[3] = {0, 0, 0};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            v[0] += cls[j] == 0;
+            v[1] += cls[j] == 1;
+            v[2] += cls[j] == 2;
+        }
+        int x[3] = {v[0], v[1], v[2]};
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const int y = __shfl_up_sync(0xffffffffu, x[k], o);
+                if (lane >= o) x[k] += y;
+            }
+        }
+        if (lane == 31) {
+            s.wcnt[0][warp] = x[0];
+            s.wcnt[1][warp] = x[1];
+            s.wcnt[2][warp] = x[2];
+        }
+        __syncthreads();
+        int off[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            int pre = s.base[k];
+            for (int w = 0; w < warp; ++w) pre += s.wcnt[k][w];
+            off[k] = pre + x[k] - v[k];
+        }
+        __syncthreads();
+        if (threadIdx.x < 3) {
+            int t = 0;
+            for (int w = 0; w < kWarps; ++w) t += s.wcnt[threadIdx.x][w];
+            s.base[threadIdx.x] += t;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (cls[j] == 0) c0[off[0]++] = e[j];
+            else if (cls[j] == 1) c1[off[1]++] = e[j];
+            else if (cls[j] == 2) c2[off[2]++] = e[j];
+        }
+        __syncthreads();
+    }
+}
+
 // Block-wide exclusive prefix sum of v; every thread gets the block total.
 __device__ int block_exclusive_scan(int v, int *s_w, int &total) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -468,27 +527,22 @@ __global__ void __launch_bounds__(kThreads) dual_kernel(DualNodes nodes, const i
         int *c0 = arena + scratch;  // scratch for leaf-body offsets (far entries are not stored)
 
         // ---- classify the list (stable compaction): far c0, leaf / close c1, non-leaf c2 ----
-        for (int i0 = 0; i0 < len; i0 += kThreads) {
-            const int i = i0 + tid;
-            int cls = -1, e = -1;
-            if (i < len) {
-                e = list[i];
-                if (type == kLockstep) {
-                    const DNode A = load_node(nodes, e);
-                    if (node_node(A, P, theta) == 0) cls = 0;
-                    else if (A.leaf()) cls = x.range_ok(A.link0, A.link1) ? 1 : -1;
-                    else cls = (x.left_ok(e) && x.right_ok(e, A.link0)) ? 2 : -1;
-                    if (cls < 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
-                } else {
-                    const float4 q = __ldg(bodies + e);
-                    const float pe[3] = {q.x, q.y, q.z};
-                    cls = point_is_far(pe, P, pthr) ? 0 : 1;
-                }
-            }
-            const int pos = stable_rank(cls, s_scan);
-            if (cls == 0) c0[pos] = e;
-            else if (cls == 1) c1[pos] = e;
-            else if (cls == 2) c2[pos] = e;
+        if (type == kLockstep) {
+            stable_partition4(list, len, c0, c1, c2, s_scan, [&](int e) {
+                const DNode A = load_node(nodes, e);
+                int cls;
+                if (node_node(A, P, theta) == 0) cls = 0;
+                else if (A.leaf()) cls = x.range_ok(A.link0, A.link1) ? 1 : -1;
+                else cls = (x.left_ok(e) && x.right_ok(e, A.link0)) ? 2 : -1;
+                if (cls < 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
+                return cls;
+            });
+        } else {
+            stable_partition4(list, len, c0, c1, c2, s_scan, [&](int e) {
+                const float4 q = __ldg(bodies + e);
+                const float pe[3] = {q.x, q.y, q.z};
+                return point_is_far(pe, P, pthr) ? 0 : 1;
+            });
         }
         __syncthreads();  // the compacted lists are read by other threads below
         const int nfar = s_scan.base[0], nleaf = s_scan.base[1], nnon = s_scan.base[2];
@@ -749,22 +803,46 @@ __device__ __forceinline__ void pair_nog(float4 b, const float p[3], float eps, 
     a[2] = fmaf(-rz, s, a[2]);
 }
 
-// Gravity::nodeParticle for MultipoleMassSummary<3> (Gravity.h:239-259) without G, added into a.
+// Gravity::nodeParticle for MultipoleMassSummary<3> (Gravity.h:239-259) without G, added into a:
+//   a += -M R / r^3 + (D3 : Q2) / 2 - (D4 : Q3) / 6,
+// with the two full contractions (SymmetricTensor3.h:281-292) written out for symmetric moments:
+//   (D3 : Q2)_i = g3 R_i (R.Q2.R) + g2 (2 (Q2 R)_i + R_i tr Q2)
+//   (D4 : Q3)_i = g4 R_i (Q3 : RRR) + 3 g3 ((Q3 : RR)_i + R_i (t.R)) + 3 g2 t_i,  t_i = Q3_ikk,
+// which is the same sum over index tuples, grouped (about 100 flops instead of about 550).
 __device__ __noinline__ void m2p_nog(const Ctx &x, int k, const float p[3], float a[3]) {
     const float4 c4 = __ldg(x.nodes.com + k);
-    const float R[3] = {p[0] - c4.x, p[1] - c4.y, p[2] - c4.z};
-    if (R[0] == 0.f && R[1] == 0.f && R[2] == 0.f) return;
-    const float inv = soft_inv_r(R, x.eps);
-    const st::Coef c = st::Coef::from_inverse(inv);
-    float q2[6], q3[10], d3[10], d4[15], v3[3], v4[3];
-    load_q(x.nodes, k, q2, q3);
-    st::D3(R, c, d3);
-    st::D4(R, c, d4);
-    st::t3_dot_t2(d3, q2, v3);
-    st::t4_dot_t3(d4, q3, v4);
-    const float mono = -c4.w * (inv * inv * inv);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) a[i] += R[i] * mono + v3[i] / 2.0f - v4[i] / 6.0f;
+    const float rx = p[0] - c4.x, ry = p[1] - c4.y, rz = p[2] - c4.z;
+    if (rx == 0.f && ry == 0.f && rz == 0.f) return;
+    const float inv = rsqrtf(fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, x.eps))));
+    const float i2 = inv * inv, i3 = inv * i2, i5 = i3 * i2, i7 = i5 * i2, i9 = i7 * i2;
+    const float g2 = 3.0f * i5, g3 = -15.0f * i7, g4 = 105.0f * i9;
+    const float4 *q = x.nodes.q + (int64_t) k * 4;
+    const float4 qa = __ldg(q), qb = __ldg(q + 1), qc = __ldg(q + 2), qd = __ldg(q + 3);
+    // quadrupole xx xy xz yy yz zz; octupole xxx xxy xxz xyy xyz xzz yyy yyz yzz zzz
+    const float Qxx = qa.x, Qxy = qa.y, Qxz = qa.z, Qyy = qa.w, Qyz = qb.x, Qzz = qb.y;
+    const float Oxxx = qb.z, Oxxy = qb.w, Oxxz = qc.x, Oxyy = qc.y, Oxyz = qc.z, Oxzz = qc.w;
+    const float Oyyy = qd.x, Oyyz = qd.y, Oyzz = qd.z, Ozzz = qd.w;
+    // (D3 : Q2) / 2
+    const float qrx = fmaf(Qxx, rx, fmaf(Qxy, ry, Qxz * rz));
+    const float qry = fmaf(Qxy, rx, fmaf(Qyy, ry, Qyz * rz));
+    const float qrz = fmaf(Qxz, rx, fmaf(Qyz, ry, Qzz * rz));
+    const float rqr = fmaf(rx, qrx, fmaf(ry, qry, rz * qrz));
+    const float trq = Qxx + Qyy + Qzz;
+    const float s2r = 0.5f * fmaf(g3, rqr, g2 * trq), s2q = g2;  // R_i s2r + (Q2 R)_i s2q
+    // (D4 : Q3) / 6
+    const float xx = rx * rx, xy = rx * ry, xz = rx * rz, yy = ry * ry, yz = ry * rz, zz = rz * rz;
+    const float ox = fmaf(Oxxx, xx, fmaf(2.0f * Oxxy, xy, fmaf(2.0f * Oxxz, xz, fmaf(Oxyy, yy, fmaf(2.0f * Oxyz, yz, Oxzz * zz)))));
+    const float oy = fmaf(Oxxy, xx, fmaf(2.0f * Oxyy, xy, fmaf(2.0f * Oxyz, xz, fmaf(Oyyy, yy, fmaf(2.0f * Oyyz, yz, Oyzz * zz)))));
+    const float oz = fmaf(Oxxz, xx, fmaf(2.0f * Oxyz, xy, fmaf(2.0f * Oxzz, xz, fmaf(Oyyz, yy, fmaf(2.0f * Oyzz, yz, Ozzz * zz)))));
+    const float orrr = fmaf(rx, ox, fmaf(ry, oy, rz * oz));
+    const float tx = Oxxx + Oxyy + Oxzz, ty = Oxxy + Oyyy + Oyzz, tz = Oxxz + Oyyz + Ozzz;
+    const float tr = fmaf(tx, rx, fmaf(ty, ry, tz * rz));
+    const float s4r = fmaf(g4, orrr, 3.0f * g3 * tr) * (1.0f / 6.0f);  // R_i s4r + O_i s4o + t_i s4t
+    const float s4o = 0.5f * g3, s4t = 0.5f * g2;
+    const float sr = fmaf(-c4.w, i3, s2r - s4r);
+    a[0] += fmaf(rx, sr, fmaf(qrx, s2q, -fmaf(ox, s4o, tx * s4t)));
+    a[1] += fmaf(ry, sr, fmaf(qry, s2q, -fmaf(oy, s4o, ty * s4t)));
+    a[2] += fmaf(rz, sr, fmaf(qrz, s2q, -fmaf(oz, s4o, tz * s4t)));
 }
 
 // Pairs of the unit's targets with sources src(0..m) for lanes in `mine`: 32 sources at a time
