@@ -47,7 +47,7 @@ namespace nbg {
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 512;  // traversal block: one per start node, the whole block per task
 constexpr int kWarps = kThreads / 32;
 constexpr int kTaskInts = 6;  // type, passive node, list offset, list length, field offset, arena top
 constexpr int kLockstep = 0, kPassive = 1;
@@ -943,7 +943,7 @@ __device__ void warp_walk(const Ctx &x, NearWarp &w, const Lane &L, int root, un
 }
 
 template<bool EPS0>
-__global__ void __launch_bounds__(kNearThreads, 2) near_kernel(DualNodes nodes, const int *__restrict__ num_nodes,
+__global__ void __launch_bounds__(kNearThreads, 4) near_kernel(DualNodes nodes, const int *__restrict__ num_nodes,
                                                                const float4 *__restrict__ bodies, int n, float G,
                                                                float eps, float theta, float4 *__restrict__ acc,
                                                                unsigned long long *__restrict__ counts, NearPool pool,
