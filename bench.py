@@ -371,9 +371,33 @@ def _run_ours_on_stream(args, torch, nb, pm, vel, eps, stream, world, rank, devi
         "clocks": clk,
     }
     solver.close()
+    line["diagnostics"] = energy_diagnostics(nb, device)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(pm, eps)
     return line
+
+
+def energy_diagnostics(nb, device, n=65536, steps=100):
+    """Energy and momentum drift of the same solver configuration on a 65,536-body Plummer sphere
+    over 100 steps, both measured in FP64 on the device (nb_energy is an O(N^2) direct sum, so the
+    diagnostic run is smaller than the timed one)."""
+    from nbody_b200 import scenarios
+
+    pm, vel = scenarios.plummer(n, seed=SEED + 1000)
+    eps = scenarios.softening_to_epsilon(SOFTENING)
+    with nb.QuadrupoleLinearBVHSolver(bodies=pm, velocities=vel, rule=nb.Gravity(1.0, eps), theta=THETA,
+                                      max_leaf_size=LEAF, time_step=DT, device=device) as s:
+        k0, u0 = s.energy()
+        p0, v0 = s.bodies()
+        s.step(steps)
+        k1, u1 = s.energy()
+        p1, v1 = s.bodies()
+    mom0 = (p0[:, 3:4].astype(np.float64) * v0[:, :3]).sum(0)
+    mom1 = (p1[:, 3:4].astype(np.float64) * v1[:, :3]).sum(0)
+    e0, e1 = k0 + u0, k1 + u1
+    return {"n_bodies": n, "steps": steps, "energy_start": e0, "energy_end": e1,
+            "energy_rel_drift": abs(e1 - e0) / abs(e0), "momentum_drift": float(np.linalg.norm(mom1 - mom0)),
+            "method": "FP64 direct-sum potential and kinetic energy on the device (nb_energy)"}
 
 
 def _run_sharded_on_stream(args, torch, nb, pm, vel, eps, stream, world, rank, device):

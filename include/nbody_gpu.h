@@ -218,6 +218,11 @@ int nb_server_status(nb_server *sv, int64_t request_id, int32_t *state, int32_t 
 int nb_server_take_result(nb_server *sv, int64_t request_id, float *pos_mass, float *velocity);
 int nb_server_get_stats(nb_server *sv, nb_server_stats *out);
 
+/* Energy diagnostics of the current bodies in FP64 (synchronises): kinetic = sum 1/2 m |v|^2 and
+ * potential = -G/2 sum_i sum_j m_i m_j / sqrt(|r_ij|^2 + epsilon), pairs at equal positions
+ * excluded as the force excludes them (Gravity.h:203). O(n^2) on the device. */
+int nb_energy(nb_ctx *ctx, double *kinetic, double *potential);
+
 /* Direct sum on device pointers: accelerations of nt targets (4 floats each) from n bodies.
  * precision 32: FP32, acc 4 floats per target (NaiveSolver arithmetic).
  * precision 64: FP64 accumulation, acc 3 doubles per target (accuracy reference). */

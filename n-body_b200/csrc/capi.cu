@@ -948,6 +948,30 @@ int nb_get_tree(nb_ctx *ctx, int64_t *num_nodes, int32_t *record_floats, uint64_
     return device_status(ctx);
 }
 
+int nb_energy(nb_ctx *ctx, double *kinetic, double *potential) {
+    int rc = begin(ctx);
+    if (rc != NB_OK) return rc;
+    if (!kinetic || !potential) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "output is NULL");
+    const int64_t need = energy_parts(ctx->n) + 2;
+    if (ctx->acc64_cap < need) {
+        dev_free(ctx->acc64);
+        ctx->acc64_cap = 0;
+        NB_TRY(dev_alloc(&ctx->acc64, (size_t) need), "alloc energy buffer");
+        ctx->acc64_cap = need;
+    }
+    double *out = ctx->acc64 + need - 2;
+    launch_energy_f64(ctx->pos, ctx->vel, ctx->n, (double) ctx->cfg.G, (double) ctx->cfg.epsilon, ctx->acc64, out,
+                      ctx->stream);
+    NB_TRY(cudaGetLastError(), "energy");
+    double h[2] = {0.0, 0.0};
+    NB_TRY(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream), "read energy");
+    rc = device_status(ctx);
+    if (rc != NB_OK) return rc;
+    *kinetic = h[0];
+    *potential = h[1];
+    return NB_OK;
+}
+
 int nb_direct_device(nb_ctx *ctx, int64_t n, const void *d_bodies, int64_t nt, const void *d_targets, void *d_acc,
                      int32_t precision) {
     int rc = begin(ctx);

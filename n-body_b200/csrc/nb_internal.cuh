@@ -233,6 +233,11 @@ void launch_bh_traverse(int order, const NodeArrays &nodes, const int *num_nodes
                         const int4 *groups = nullptr, int64_t num_groups = 0, const int *inst_root = nullptr);
 
 // direct_sum.cu
+// FP64 energy diagnostics: (kinetic, potential) of n bodies into out[0..1]; parts needs
+// energy_parts(n) doubles.
+int64_t energy_parts(int64_t n);
+void launch_energy_f64(const float4 *bodies, const float4 *vel, int64_t n, double G, double eps, double *parts,
+                       double *out, cudaStream_t s);
 void launch_direct_f32(const float4 *bodies, int64_t n, const float4 *targets, int64_t nt, float G, float eps,
                        float4 *acc, cudaStream_t s);
 void launch_direct_f64(const float4 *bodies, int64_t n, const float4 *targets, int64_t nt, double G, double eps,

@@ -131,6 +131,7 @@ SIGNATURES = {
     "nb_get_phase_times": (C.c_int, [_vp, C.POINTER(PhaseTimes)]),
     "nb_get_tree": (C.c_int, [_vp, C.POINTER(_i64), C.POINTER(_i32), _vp, _vp, _vp, _vp]),
     "nb_direct_device": (C.c_int, [_vp, _i64, _vp, _i64, _vp, _vp, _i32]),
+    "nb_energy": (C.c_int, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "nb_sort_codes_noalloc": (C.c_int, [_vp, _vp, _vp, _i64, _vp]),
     "nb_set_instances": (C.c_int, [_vp, _i32, _vp, _vp, _vp, _vp]),
     "nb_instance_count": (_i32, [_vp]),
@@ -414,6 +415,12 @@ class Solver:
 
     def shard_gathered(self):
         self._check(lib().nb_shard_gathered(self._ctx))
+
+    def energy(self):
+        """(kinetic, potential) of the current bodies, FP64 on the device (nb_energy)."""
+        k, u = C.c_double(), C.c_double()
+        self._check(lib().nb_energy(self._ctx, C.byref(k), C.byref(u)))
+        return k.value, u.value
 
     def direct_device(self, n, d_bodies, nt, d_targets, d_acc, precision=32):
         self._check(lib().nb_direct_device(self._ctx, n, d_bodies, nt, d_targets, d_acc, precision))

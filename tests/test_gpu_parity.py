@@ -267,3 +267,34 @@ def test_repeatable(nb):
         s.set_bodies(pm)
         a2 = s.update_accelerations()
     assert np.array_equal(a1, a2)
+
+
+def test_energy_diagnostics_fp64(nb):
+    """nb_energy: FP64 kinetic and softened potential energy of the current bodies, against numpy."""
+    pm, vel = nb.scenarios.plummer(1500, seed=14)
+    pm[10] = pm[11]  # a coincident pair is excluded, as the force excludes it
+    eps, G = 1e-3, 1.7
+    with nb.QuadrupoleLinearBVHSolver(bodies=pm, velocities=vel, rule=nb.Gravity(G, eps)) as s:
+        k, u = s.energy()
+    p = pm[:, :3].astype(np.float64)
+    m = pm[:, 3].astype(np.float64)
+    d = p[None, :, :] - p[:, None, :]
+    r2 = (d * d).sum(-1)
+    same = r2 == 0.0
+    inv = np.where(same, 0.0, 1.0 / np.sqrt(r2 + np.float64(np.float32(eps))))
+    u_ref = -0.5 * np.float64(np.float32(G)) * (m[:, None] * m[None, :] * inv).sum()
+    k_ref = 0.5 * (m * (vel[:, :3].astype(np.float64) ** 2).sum(1)).sum()
+    assert abs(k - k_ref) <= 1e-12 * abs(k_ref)
+    assert abs(u - u_ref) <= 1e-12 * abs(u_ref)
+
+
+def test_energy_conserved_over_steps(nb):
+    """Leapfrog-style kick-drift with the quadrupole tree: total energy drifts little over 50 steps."""
+    pm, vel = nb.scenarios.plummer(20000, seed=15)
+    eps = nb.scenarios.softening_to_epsilon(0.01)
+    with nb.QuadrupoleLinearBVHSolver(bodies=pm, velocities=vel, rule=nb.Gravity(1.0, eps), theta=0.5,
+                                      max_leaf_size=16, time_step=1e-3) as s:
+        e0 = sum(s.energy())
+        s.step(50)
+        e1 = sum(s.energy())
+    assert abs(e1 - e0) <= 1e-3 * abs(e0)
