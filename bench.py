@@ -526,6 +526,10 @@ def run_batched(args):
                                          device=device)
         s.set_stream(stream.cuda_stream)
         s.set_instances(sizes, np.concatenate(bodies), np.concatenate(vels), thetas)
+        # leaf size measured on this batch (force passes only: the state does not change)
+        tuned = s.autotune(candidates=(4, 6, 8, 12, 16, 24), passes=2)
+        leaf = tuned.leaf
+        accuracy = batched_accuracy(nb, s, sizes, bodies, eps, torch, device)
         s.enable_graphs(True)
         s.step(max(args.warmup, 3))
         torch.cuda.synchronize(device)
@@ -545,7 +549,7 @@ def run_batched(args):
         ctxs = []
         for k in range(len(sizes)):
             c = nb.QuadrupoleLinearBVHSolver(bodies=bodies[k], velocities=vels[k], rule=nb.Gravity(1.0, eps),
-                                             theta=float(thetas[k]), max_leaf_size=LEAF, time_step=BATCH_DT,
+                                             theta=float(thetas[k]), max_leaf_size=leaf, time_step=BATCH_DT,
                                              device=device)
             c.set_stream(stream.cuda_stream)
             c.step(1)
@@ -571,16 +575,45 @@ def run_batched(args):
         "dtype": "f32", "data": "synthetic (seeded Plummer spheres)",
         "config": {"workload": f"batched-{len(sizes)}-plummer-quadrupole", "instances": int(len(sizes)),
                    "total_bodies": total, "n_min": int(sizes.min()), "n_max": int(sizes.max()),
-                   "softening": BATCH_SOFTENING, "leaf_size": LEAF, "order": ORDER, "dt": BATCH_DT,
+                   "softening": BATCH_SOFTENING, "leaf_size": leaf, "order": ORDER, "dt": BATCH_DT,
                    "graphs": "two steps per CUDA graph", "l2": "flushed (256 MB write) before the timed steps"},
         "sequential_plain_path": {"value": seq_value, "unit": "body-steps/s", "steps": seq_steps,
-                                  "ratio_batched_over_sequential": value / seq_value},
+                                  "leaf_size": leaf, "ratio_batched_over_sequential": value / seq_value},
+        "autotune": {"leaf_size": leaf, "ms_per_force_pass": {str(k): v for k, v in tuned.timings_ms.items()},
+                     "method": "force passes of this batch at each candidate leaf size, fastest kept"},
+        "accuracy": accuracy,
         "phases_ms_per_step": {k: phases[k] / max(phases["passes"], 1) for k in
                                ("bbox_ms", "morton_ms", "sort_ms", "gather_ms", "build_ms", "traverse_ms",
                                 "integrate_ms")},
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def batched_accuracy(nb, s, sizes, bodies, eps, torch, device, picks=(0, 85, 170, 255), targets=2048):
+    """Relative RMS force error of the batched pass against an FP64 direct sum, on up to 2048
+    seeded targets of four of the instances."""
+    acc = s.update_accelerations()
+    starts = np.concatenate([[0], np.cumsum(sizes)])
+    rng = np.random.default_rng(2024)
+    rels = []
+    for k in picks:
+        if k >= len(sizes):
+            continue
+        pm = bodies[k]
+        idx = np.sort(rng.choice(len(pm), min(targets, len(pm)), replace=False))
+        dpm = torch.from_numpy(pm).to(device)
+        dt = torch.from_numpy(pm[idx].copy()).to(device)
+        out = torch.zeros((len(idx), 3), dtype=torch.float64, device=device)
+        s.direct_device(len(pm), dpm.data_ptr(), len(idx), dt.data_ptr(), out.data_ptr(), 64)
+        s.synchronize()
+        ref = out.cpu().numpy()
+        got = acc[starts[k] + idx, :3].astype(np.float64)
+        rels.append(np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1))
+    r = np.concatenate(rels)
+    return {"force_rms_rel": float(np.sqrt(np.mean(r ** 2))), "force_max_rel": float(r.max()),
+            "instances_sampled": [int(k) for k in picks if k < len(sizes)], "targets_per_instance": targets,
+            "reference": "FP64 direct sum on GPU"}
 
 
 def serving_pools(seed=45, n_max=1 << 21):

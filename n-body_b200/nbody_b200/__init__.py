@@ -331,6 +331,15 @@ class Solver:
         self._check(lib().nb_get_instance_roots(self._ctx, _ptr(roots)))
         return roots
 
+    def instance_count(self) -> int:
+        return int(lib().nb_instance_count(self._ctx))
+
+    def autotune(self, cache=None, candidates=None, passes: int = 3, tolerance: float = 0.0):
+        """Pick the leaf size for the current bodies by measurement (see autotune.py)."""
+        from . import autotune as at
+
+        return at.autotune(self, cache, candidates or at.DEFAULT_CANDIDATES, passes, tolerance)
+
     def enable_graphs(self, on: bool = True):
         self._check(lib().nb_enable_graphs(self._ctx, int(on)))
 
