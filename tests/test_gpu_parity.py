@@ -298,3 +298,25 @@ def test_energy_conserved_over_steps(nb):
         s.step(50)
         e1 = sum(s.energy())
     assert abs(e1 - e0) <= 1e-3 * abs(e0)
+
+
+def test_config_c1_ten_steps(nb, oracle):
+    """The 10,000-body uniform-ball configuration (monopole, leaf 16, theta 0.5, softening 0.01,
+    dt 1e-3, 10 steps): trajectory against the oracle stepping with its own accelerations, and the
+    interaction counts of the first pass exact."""
+    pm, vel = nb.scenarios.uniform_ball(10000, seed=42)
+    eps = nb.scenarios.softening_to_epsilon(0.01)
+    with nb.LinearBVHSolver(bodies=pm, velocities=vel, rule=nb.Gravity(1.0, eps), theta=0.5, max_leaf_size=16,
+                            time_step=1e-3) as s:
+        s.update_accelerations()
+        c = s.counts()
+        s.step(10)
+        gpm, gvel = s.bodies()
+    a, rc = oracle.bh_accelerations(pm, eps=eps, theta=0.5, leaf=16, order=1)
+    assert c["particle_particle"] == rc[0] and c["node_particle"] == rc[1]
+    p, v = pm.copy(), vel.copy()
+    for _ in range(10):
+        a, _ = oracle.bh_accelerations(p, eps=eps, theta=0.5, leaf=16, order=1)
+        p, v = oracle.kick_drift(p, v, a, np.float32(1e-3))
+    assert np.abs(gpm[:, :3] - p[:, :3]).max() < 1e-5 * np.abs(p[:, :3]).max()
+    assert np.abs(gvel[:, :3] - v[:, :3]).max() < 1e-4 * np.abs(v[:, :3]).max()

@@ -154,3 +154,27 @@ def test_cli_rejects_bad_arguments(tmp_path, nb):
     assert run("--bogus", str(src)).returncode == 2
     r = run("-s", "barnes-hut-octree", "-i", "1", str(src))
     assert r.returncode == 1 and "unknown solver id" in r.stderr
+
+
+REFERENCE_SCENARIOS = "/root/reference/scenarios"
+
+
+@pytest.mark.parametrize("name", ["threebody.json", "test.json"])
+def test_reads_reference_scenario_files(tmp_path, nb, name):
+    """The reference's own scenario files (read in place when the reference tree is present)."""
+    src = os.path.join(REFERENCE_SCENARIOS, name)
+    if not os.path.exists(src):
+        pytest.skip("reference scenarios not present")
+    out = tmp_path / "out.json"
+    r = run("-i", "0", "-o", str(out), src)
+    assert r.returncode == 0, r.stderr
+    root = json.load(open(src))
+    pm, vel, _, G = nb.scenarios.read_json(str(out))
+    assert len(pm) == len(root["particles"])
+    for i, p in enumerate(root["particles"]):
+        if "position" in p:
+            assert pm[i, :3].tolist() == [np.float32(p["position"][c]) for c in "xyz"]
+        if "velocity" in p:
+            assert vel[i, :3].tolist() == [np.float32(p["velocity"][c]) for c in "xyz"]
+        assert pm[i, 3] == np.float32(p.get("mass", 0.0))
+    assert (G is None) == ("G" not in root)
