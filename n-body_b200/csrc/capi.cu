@@ -198,6 +198,10 @@ void free_dual(nb_ctx *ctx) {
     NearPool &np = ctx->dws.near;
     dev_free(np.head); dev_free(np.items); dev_free(np.words); dev_free(np.units); dev_free(np.counters);
     np.head_cap = np.item_cap = np.word_cap = np.unit_cap = 0;
+    SpillPool &sp = ctx->dws.spill;
+    dev_free(sp.head); dev_free(sp.recs); dev_free(sp.rec_field); dev_free(sp.words); dev_free(sp.work);
+    dev_free(sp.counters);
+    sp.head_cap = sp.rec_cap = sp.word_cap = sp.work_cap = 0;
     ctx->dual_cap = 0;
 }
 
@@ -232,6 +236,17 @@ int ensure_dual(nb_ctx *ctx) {
     NB_TRY(dev_alloc(&np.units, (size_t) np.unit_cap), "alloc near-field pool");
     NB_TRY(dev_alloc(&np.counters, 4), "alloc near-field pool");
     if (ctx->dws.near_blocks == 0) ctx->dws.near_blocks = dual_near_blocks(ctx->cfg.device);
+    SpillPool &sp = ctx->dws.spill;
+    sp.head_cap = (int64_t) slots;
+    sp.work_cap = (int64_t) slots;
+    dual_spill_sizes(c, &sp.rec_cap, &sp.word_cap);
+    NB_TRY(dev_alloc(&sp.head, (size_t) sp.head_cap), "alloc frontier pool");
+    NB_TRY(dev_alloc(&sp.work, (size_t) sp.work_cap), "alloc frontier pool");
+    NB_TRY(dev_alloc(&sp.recs, (size_t) sp.rec_cap), "alloc frontier pool");
+    NB_TRY(dev_alloc(&sp.rec_field, (size_t) sp.rec_cap), "alloc frontier pool");
+    NB_TRY(dev_alloc(&sp.words, (size_t) sp.word_cap), "alloc frontier pool");
+    NB_TRY(dev_alloc(&sp.counters, 4), "alloc frontier pool");
+    if (ctx->dws.frontier_blocks == 0) ctx->dws.frontier_blocks = dual_frontier_blocks(ctx->cfg.device);
     ctx->dual_cap = c;
     return NB_OK;
 }
@@ -358,15 +373,30 @@ int dual_traverse(nb_ctx *ctx, int64_t n, cudaStream_t s) {
         launch_dual_traverse(ctx->dnodes, ctx->tw.num_nodes, ctx->pos, n, ctx->cfg.G, ctx->cfg.epsilon,
                              ctx->cfg.theta, ctx->acc, ctx->counts, ctx->dws, ctx->err, s);
         unsigned long long *h = ctx->host_scratch;
+        SpillPool &sp = ctx->dws.spill;
         NB_TRY(cudaMemcpyAsync(h, np.counters, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
                "read near-field pool");
+        NB_TRY(cudaMemcpyAsync(h + 5, sp.counters, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
+               "read frontier pool");
         NB_TRY(cudaMemcpyAsync(h + 4, ctx->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s), "read status");
         NB_TRY(cudaStreamSynchronize(s), "dual-tree traversal");
         uint32_t e = 0;
         std::memcpy(&e, h + 4, sizeof(uint32_t));
         const bool pool = (e & kErrNearPool) != 0, arena = (e & kErrDualArena) != 0;
         if ((!pool && !arena) || attempt == 3) return NB_OK;
-        if (pool) {
+        if (pool && ((int64_t) h[5] > sp.rec_cap || (int64_t) h[6] > sp.word_cap)) {
+            const int64_t recs = (int64_t) h[5], words = (int64_t) h[6];
+            dev_free(sp.recs);
+            dev_free(sp.rec_field);
+            dev_free(sp.words);
+            sp.rec_cap = std::max<int64_t>(sp.rec_cap, recs + recs / 4 + 1024);
+            sp.word_cap = std::min<int64_t>(std::max<int64_t>(sp.word_cap, words + words / 4 + 4096),
+                                            (int64_t(1) << 31) - 1);
+            NB_TRY(dev_alloc(&sp.recs, (size_t) sp.rec_cap), "grow frontier pool");
+            NB_TRY(dev_alloc(&sp.rec_field, (size_t) sp.rec_cap), "grow frontier pool");
+            NB_TRY(dev_alloc(&sp.words, (size_t) sp.word_cap), "grow frontier pool");
+        }
+        if (pool && ((int64_t) h[0] > np.item_cap || (int64_t) h[1] > np.word_cap)) {
             const int64_t items = (int64_t) h[0], words = (int64_t) h[1];
             dev_free(np.items);
             dev_free(np.words);

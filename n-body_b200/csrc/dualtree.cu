@@ -39,6 +39,7 @@
 // serial recursion, the interactions evaluated are the same.
 #include <algorithm>
 #include <cfloat>
+#include <climits>
 
 #include "nb_internal.cuh"
 #include "stensor.cuh"
@@ -384,95 +385,96 @@ __device__ void append_item(const NearPool &pool, int leaf, int first, int size,
     }
 }
 
+// Hands the tasks of children `right` / `left` (where spill_r / spill_l) to the frontier kernel:
+// one copy of their shared list and one field each, linked to the child's record list. Only the
+// block that owns a frontier node's ancestors appends to its list, so the order is that block's
+// task order. The first record of a node registers it in the work list. Called by every thread.
+__device__ void spill_children(const SpillPool &sp, int type, const int *list, int len, const float *field_r,
+                               const float *field_l, int right, int left, bool spill_r, bool spill_l, uint32_t *err,
+                               int *s_slot) {
+    const int nrec = (spill_r ? 1 : 0) + (spill_l ? 1 : 0);
+    if (nrec == 0) return;  // uniform
+    if (threadIdx.x == 0) {
+        int slot = -1;
+        const unsigned long long words = (unsigned long long) len + (unsigned long long) F * nrec;
+        const unsigned long long rec = atomicAdd(&sp.counters[0], (unsigned long long) nrec);
+        const unsigned long long off = atomicAdd(&sp.counters[1], words);
+        if (rec + nrec <= (unsigned long long) sp.rec_cap && off + words <= (unsigned long long) sp.word_cap &&
+            right < sp.head_cap && left < sp.head_cap) {
+            int k = 0;
+            for (int side = 0; side < 2; ++side) {
+                const bool on = side == 0 ? spill_r : spill_l;
+                if (!on) continue;
+                const int c = side == 0 ? right : left;
+                const int r = (int) rec + k;
+                const int old = sp.head[c];
+                sp.recs[r] = make_int4(old, type, (int) off, len);
+                sp.rec_field[r] = (int) off + len + F * k;
+                sp.head[c] = r;
+                if (old < 0) {
+                    const unsigned long long w = atomicAdd(&sp.counters[2], 1ull);
+                    if (w < (unsigned long long) sp.work_cap) sp.work[w] = c;
+                    else atomicOr(err, (uint32_t) kErrNearPool);
+                }
+                ++k;
+            }
+            slot = (int) off;
+        } else {
+            atomicOr(err, (uint32_t) kErrNearPool);
+        }
+        s_slot[0] = slot;
+    }
+    __syncthreads();
+    const int off = s_slot[0];
+    if (off < 0) return;
+    for (int i = threadIdx.x; i < len; i += kThreads) sp.words[off + i] = list[i];
+    int k = 0;
+    for (int side = 0; side < 2; ++side) {
+        const bool on = side == 0 ? spill_r : spill_l;
+        if (!on) continue;
+        const float *f = side == 0 ? field_r : field_l;
+        for (int a = threadIdx.x; a < F; a += kThreads) sp.words[off + len + F * k + a] = __float_as_int(f[a]);
+        ++k;
+    }
+}
+
+__device__ __forceinline__ int node_size(const DualNodes &N, int k) { return __float_as_int(__ldg(N.bmin + k).w); }
+
 __device__ __forceinline__ void push_task(int *t, int type, int node, int list, int len, int field, int top) {
     t[0] = type; t[1] = node; t[2] = list; t[3] = len; t[4] = field; t[5] = top;
 }
 
+// FRONTIER = false: one block per start node; tasks of frontier nodes (at most `frontier` bodies,
+// parent above) are spilled. FRONTIER = true: blocks take frontier nodes from the work list and
+// run their spilled tasks, in record order, to completion.
+template<bool FRONTIER>
 __global__ void __launch_bounds__(kThreads) dual_kernel(DualNodes nodes, const int *__restrict__ num_nodes,
                                                         const float4 *__restrict__ bodies, int n, float G,
                                                         float eps, float theta, float4 *__restrict__ acc,
                                                         unsigned long long *__restrict__ counts,
                                                         const int *__restrict__ roots, const int *__restrict__ num_roots,
                                                         int *__restrict__ arena_all, int arena_words,
-                                                        int *__restrict__ tasks_all, NearPool pool,
-                                                        uint32_t *__restrict__ err) {
+                                                        int *__restrict__ tasks_all, NearPool pool, SpillPool spill,
+                                                        int frontier, uint32_t *__restrict__ err) {
     __shared__ float s_field[F];
     __shared__ float s_child[2][F];
     __shared__ float s_red[kWarps][F];
     __shared__ int s_task[kTaskInts];
     __shared__ Scan3 s_scan;
     __shared__ int s_w[kWarps];
-    __shared__ int s_ntask, s_fail, s_slot;
+    __shared__ int s_ntask, s_fail, s_slot, s_work;
 
-    if ((int) blockIdx.x >= *num_roots) return;  // uniform across the block
+    if (!FRONTIER && (int) blockIdx.x >= *num_roots) return;  // uniform across the block
     const int tid = threadIdx.x;
     const Ctx x{nodes, bodies, G, eps, theta, *num_nodes, n};
     int *arena = arena_all + (int64_t) blockIdx.x * arena_words;
     float *farena = reinterpret_cast<float *>(arena);
     int *tasks = tasks_all + (int64_t) blockIdx.x * kDualTasks * kTaskInts;
     unsigned long long npn = 0, nnn = 0;
-    const int root = roots[blockIdx.x];
-    if (root < 0 || root >= x.nn || x.nn <= 0) {
-        if (tid == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
-        return;
-    }
-    const DNode Rt = load_node(nodes, root);
+    // spill children at the frontier (first kernel only)
+    const int spill_size = FRONTIER ? -1 : frontier;
 
-    // ---- balancedLockstepDualTreeImplicitField: breadth-first over the active tree from its root;
-    // a node joins the starting list unless the criterion says "descend the active node" only and
-    // it is not a leaf, in which case its children join the next level ----
-    const int eq_cap = arena_words / 4;
-    int cur = eq_cap, curlen = 1;
-    if (tid == 0) {
-        arena[cur] = 0;
-        s_fail = 0;
-    }
-    if (tid < 3) s_scan.base[tid] = 0;
-    __syncthreads();
-    while (curlen > 0) {
-        const int nxt = cur + curlen;
-        for (int i0 = 0; i0 < curlen; i0 += kThreads) {
-            const int i = i0 + tid;
-            int a = -1, cls = -1, right = -1;
-            if (i < curlen) {
-                a = arena[cur + i];
-                const DNode A = load_node(nodes, a);
-                const int rec = node_node(A, Rt, theta);
-                cls = (rec != 1 || A.leaf()) ? 0 : 1;
-                right = A.link0;
-                if (cls == 1 && !(x.left_ok(a) && x.right_ok(a, right))) {
-                    atomicOr(err, (uint32_t) kErrTraverseLimit);
-                    cls = -1;
-                }
-            }
-            const int pos = stable_rank(cls, s_scan);
-            if (cls == 0) {
-                if (pos < eq_cap) arena[pos] = a;
-                else s_fail = 1;
-            } else if (cls == 1) {
-                if ((int64_t) nxt + 2 * (int64_t) pos + 1 < arena_words) {
-                    arena[nxt + 2 * pos] = a + 1;
-                    arena[nxt + 2 * pos + 1] = right;
-                } else {
-                    s_fail = 1;
-                }
-            }
-        }
-        __syncthreads();
-        const int nextlen = 2 * s_scan.base[1];
-        const bool failed = s_fail != 0;
-        __syncthreads();
-        if (tid == 1) s_scan.base[1] = 0;
-        cur = nxt;
-        curlen = failed ? 0 : nextlen;
-    }
-    __syncthreads();
-    if (tid == 0) {
-        const int eq = min(s_scan.base[0], eq_cap);
-        push_task(tasks, kLockstep, root, 0, eq, -1, eq);
-        s_ntask = 1;
-        if (s_fail) atomicOr(err, (uint32_t) kErrDualArena);
-    }
+    auto run_tasks = [&]() {
 
     // ---- depth-first task loop ----
     for (;;) {
@@ -619,12 +621,19 @@ __global__ void __launch_bounds__(kThreads) dual_kernel(DualNodes nodes, const i
                 farena[fr + a] = s_child[1][a];
                 farena[fl + a] = s_child[0][a];
             }
+            const bool sp_r = spill_size >= 0 && P.size > spill_size && node_size(nodes, right) <= spill_size;
+            const bool sp_l = spill_size >= 0 && P.size > spill_size && node_size(nodes, left) <= spill_size;
+            spill_children(spill, kPassive, c1, nleaf, s_child[1], s_child[0], right, left, sp_r, sp_l, err, &s_slot);
             if (tid == 0) {
-                if (nt - 1 + 2 <= kDualTasks) {
+                const int pushes = (sp_r ? 0 : 1) + (sp_l ? 0 : 1);
+                if (nt - 1 + pushes <= kDualTasks) {
                     int *t = tasks + (nt - 1) * kTaskInts;
-                    push_task(t, kPassive, right, scratch + len, nleaf, fr, fr + F);
-                    push_task(t + kTaskInts, kPassive, left, scratch + len, nleaf, fl, fl + F);
-                    s_ntask = nt + 1;
+                    if (!sp_r) {
+                        push_task(t, kPassive, right, scratch + len, nleaf, fr, fr + F);
+                        t += kTaskInts;
+                    }
+                    if (!sp_l) push_task(t, kPassive, left, scratch + len, nleaf, fl, fl + F);
+                    s_ntask = nt - 1 + pushes;
                 } else {
                     atomicOr(err, (uint32_t) kErrDualArena);
                 }
@@ -667,16 +676,132 @@ __global__ void __launch_bounds__(kThreads) dual_kernel(DualNodes nodes, const i
                 for (int b = l.x; b < l.y; ++b) dst[b - l.x] = b;
             }
         }
+        const bool sp_r = spill_size >= 0 && P.size > spill_size && node_size(nodes, right) <= spill_size;
+        const bool sp_l = spill_size >= 0 && P.size > spill_size && node_size(nodes, left) <= spill_size;
+        spill_children(spill, kLockstep, arena + dp, 2 * nnon, s_child[1], s_child[0], right, left, sp_r, sp_l, err,
+                       &s_slot);
         if (tid == 0) {
-            const int pushes = 2 + (total > 0 ? 1 : 0);
+            const int pushes = (sp_r ? 0 : 1) + (sp_l ? 0 : 1) + (total > 0 ? 1 : 0);
             if (!fits || nt - 1 + pushes > kDualTasks) {
                 atomicOr(err, (uint32_t) kErrDualArena);
             } else {
                 int *t = tasks + (nt - 1) * kTaskInts;
-                push_task(t, kLockstep, right, dp, 2 * nnon, fr, fr + F);
-                push_task(t + kTaskInts, kLockstep, left, dp, 2 * nnon, fl, fl + F);
-                if (total > 0) push_task(t + 2 * kTaskInts, kPassive, pk, lb, total, -1, lb + total);
+                if (!sp_r) {
+                    push_task(t, kLockstep, right, dp, 2 * nnon, fr, fr + F);
+                    t += kTaskInts;
+                }
+                if (!sp_l) {
+                    push_task(t, kLockstep, left, dp, 2 * nnon, fl, fl + F);
+                    t += kTaskInts;
+                }
+                if (total > 0) push_task(t, kPassive, pk, lb, total, -1, lb + total);
                 s_ntask = nt - 1 + pushes;
+            }
+        }
+    }
+
+    };  // run_tasks
+
+    if (!FRONTIER) {
+        const int root = roots[blockIdx.x];
+        if (root < 0 || root >= x.nn || x.nn <= 0) {
+            if (tid == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
+            return;
+        }
+        const DNode Rt = load_node(nodes, root);
+        // ---- balancedLockstepDualTreeImplicitField: breadth-first over the active tree from its root;
+        // a node joins the starting list unless the criterion says "descend the active node" only and
+        // it is not a leaf, in which case its children join the next level ----
+        const int eq_cap = arena_words / 4;
+        int cur = eq_cap, curlen = 1;
+        if (tid == 0) {
+            arena[cur] = 0;
+            s_fail = 0;
+        }
+        if (tid < 3) s_scan.base[tid] = 0;
+        __syncthreads();
+        while (curlen > 0) {
+            const int nxt = cur + curlen;
+            for (int i0 = 0; i0 < curlen; i0 += kThreads) {
+                const int i = i0 + tid;
+                int a = -1, cls = -1, right = -1;
+                if (i < curlen) {
+                    a = arena[cur + i];
+                    const DNode A = load_node(nodes, a);
+                    const int rec = node_node(A, Rt, theta);
+                    cls = (rec != 1 || A.leaf()) ? 0 : 1;
+                    right = A.link0;
+                    if (cls == 1 && !(x.left_ok(a) && x.right_ok(a, right))) {
+                        atomicOr(err, (uint32_t) kErrTraverseLimit);
+                        cls = -1;
+                    }
+                }
+                const int pos = stable_rank(cls, s_scan);
+                if (cls == 0) {
+                    if (pos < eq_cap) arena[pos] = a;
+                    else s_fail = 1;
+                } else if (cls == 1) {
+                    if ((int64_t) nxt + 2 * (int64_t) pos + 1 < arena_words) {
+                        arena[nxt + 2 * pos] = a + 1;
+                        arena[nxt + 2 * pos + 1] = right;
+                    } else {
+                        s_fail = 1;
+                    }
+                }
+            }
+            __syncthreads();
+            const int nextlen = 2 * s_scan.base[1];
+            const bool failed = s_fail != 0;
+            __syncthreads();
+            if (tid == 1) s_scan.base[1] = 0;
+            cur = nxt;
+            curlen = failed ? 0 : nextlen;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            const int eq = min(s_scan.base[0], eq_cap);
+            push_task(tasks, kLockstep, root, 0, eq, -1, eq);
+            s_ntask = 1;
+            if (s_fail) atomicOr(err, (uint32_t) kErrDualArena);
+        }
+        run_tasks();
+    } else {
+        const unsigned long long nwork = min(spill.counters[2], (unsigned long long) spill.work_cap);
+        const unsigned long long nrecs = min(spill.counters[0], (unsigned long long) spill.rec_cap);
+        for (;;) {
+            __syncthreads();
+            if (tid == 0) s_work = (int) min(atomicAdd(&spill.counters[3], 1ull), (unsigned long long) INT_MAX);
+            __syncthreads();
+            const int w = s_work;
+            if ((unsigned long long) w >= nwork) break;
+            const int c = spill.work[w];
+            if (c < 0 || c >= x.nn) {
+                if (tid == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
+                continue;
+            }
+            int guard = 0;
+            for (int r = spill.head[c]; r >= 0; ++guard) {
+                if ((unsigned long long) r >= nrecs || guard > (1 << 20)) {
+                    if (tid == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
+                    break;
+                }
+                const int4 rec = spill.recs[r];
+                const int fo = spill.rec_field[r];
+                const int len = rec.w;
+                if (len < 0 || (int64_t) len + F >= arena_words) {
+                    if (tid == 0) atomicOr(err, (uint32_t) kErrDualArena);
+                    r = rec.x;
+                    continue;
+                }
+                for (int i = tid; i < len; i += kThreads) arena[i] = spill.words[rec.z + i];
+                for (int a = tid; a < F; a += kThreads) arena[len + a] = spill.words[fo + a];
+                if (tid == 0) {
+                    push_task(tasks, rec.y, c, 0, len, len, len + F);
+                    s_ntask = 1;
+                }
+                __syncthreads();
+                run_tasks();
+                r = rec.x;
             }
         }
     }
@@ -1054,10 +1179,19 @@ void launch_dual_traverse(const DualNodes &nodes, const int *num_nodes, const fl
     cudaMemsetAsync(acc, 0, (size_t) n * sizeof(float4), s);
     cudaMemsetAsync(ws.near.head, 0xFF, (size_t) ws.near.head_cap * sizeof(int), s);
     cudaMemsetAsync(ws.near.counters, 0, 4 * sizeof(unsigned long long), s);
+    cudaMemsetAsync(ws.spill.head, 0xFF, (size_t) ws.spill.head_cap * sizeof(int), s);
+    cudaMemsetAsync(ws.spill.counters, 0, 4 * sizeof(unsigned long long), s);
     load_balanced_break_kernel<<<1, 32, 0, s>>>(nodes, num_nodes, ws.roots, ws.num_roots, err);
-    dual_kernel<<<kDualRoots, kThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta, acc, counts,
-                                                ws.roots, ws.num_roots, ws.arena, (int) ws.arena_words, ws.tasks,
-                                                ws.near, err);
+    // passive nodes of at most `frontier` bodies below a larger parent are handed to the second
+    // kernel, which balances them over the whole GPU
+    const int frontier = (int) std::max<int64_t>(256, n / 4096);
+    dual_kernel<false><<<kDualRoots, kThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta, acc,
+                                                       counts, ws.roots, ws.num_roots, ws.arena, (int) ws.arena_words,
+                                                       ws.tasks, ws.near, ws.spill, frontier, err);
+    dual_kernel<true><<<ws.frontier_blocks, kThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta, acc,
+                                                              counts, ws.roots, ws.num_roots, ws.arena,
+                                                              (int) ws.arena_words, ws.tasks, ws.near, ws.spill, -1,
+                                                              err);
     if (eps == 0.f)
         near_kernel<true><<<ws.near_blocks, kNearThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta,
                                                                   acc, counts, ws.near, err);
@@ -1069,6 +1203,18 @@ void launch_dual_traverse(const DualNodes &nodes, const int *num_nodes, const fl
 void dual_near_sizes(int64_t n, int64_t *item_cap, int64_t *word_cap) {
     *item_cap = 4 * n + 65536;
     *word_cap = std::min<int64_t>(64 * n + (int64_t(1) << 22), (int64_t(1) << 31) - 1);
+}
+
+void dual_spill_sizes(int64_t n, int64_t *rec_cap, int64_t *word_cap) {
+    *rec_cap = n / 8 + 65536;
+    *word_cap = std::min<int64_t>(16 * n + (int64_t(1) << 22), (int64_t(1) << 31) - 1);
+}
+
+int dual_frontier_blocks(int device) {
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dual_kernel<true>, kThreads, 0);
+    return std::max(1, std::min(kDualRoots, sms * std::max(per_sm, 1)));  // one arena per block
 }
 
 int dual_near_blocks(int device) {

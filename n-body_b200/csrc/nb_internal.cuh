@@ -198,6 +198,17 @@ struct NearPool {
     unsigned long long *counters = nullptr;  // items, words, units, unit cursor
     int64_t head_cap = 0, item_cap = 0, word_cap = 0, unit_cap = 0;
 };
+// Tasks handed from the first traversal kernel (above the frontier of passive nodes with at
+// most `frontier` bodies) to the second one, which takes frontier nodes from a work list.
+struct SpillPool {
+    int *head = nullptr;                  // per node: newest task record of a frontier node, -1 if none
+    int4 *recs = nullptr;                 // (next record, task type, list offset, list length)
+    int *rec_field = nullptr;             // field offset per record
+    int *words = nullptr;                 // list copies and fields (float bits)
+    int *work = nullptr;                  // frontier nodes with tasks, in registration order
+    unsigned long long *counters = nullptr;  // records, words, work items, work cursor
+    int64_t head_cap = 0, rec_cap = 0, word_cap = 0, work_cap = 0;
+};
 struct DualWorkspace {
     int *roots = nullptr;           // starting passive nodes (at most kDualRoots)
     int *num_roots = nullptr;
@@ -206,11 +217,15 @@ struct DualWorkspace {
     int64_t arena_words = 0;
     NearPool near;
     int near_blocks = 0;            // resident blocks of the near-field kernel
+    SpillPool spill;
+    int frontier_blocks = 0;        // resident blocks of the frontier-task kernel
 };
 // Arena words per block, near-pool sizes and the near kernel's resident grid for n bodies.
 int64_t dual_arena_words(int64_t n);
 void dual_near_sizes(int64_t n, int64_t *item_cap, int64_t *word_cap);
+void dual_spill_sizes(int64_t n, int64_t *rec_cap, int64_t *word_cap);
 int dual_near_blocks(int device);
+int dual_frontier_blocks(int device);
 void launch_dual_traverse(const DualNodes &nodes, const int *num_nodes, const float4 *bodies, int64_t n, float G,
                           float eps, float theta, float4 *acc, unsigned long long *counts, DualWorkspace &ws,
                           uint32_t *err, cudaStream_t s);
