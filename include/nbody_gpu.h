@@ -172,8 +172,8 @@ int nb_get_instance_roots(nb_ctx *ctx, int32_t *roots);
  * timing, when enabled, runs the steps uncaptured). */
 int nb_enable_graphs(nb_ctx *ctx, int enable);
 
-/* Target sharding of one instance over `world` processes, one GPU each (SURVEY multi-GPU row:
- * the path shards over targets, every rank needs all sources). Every rank holds the same state.
+/* Target sharding of one instance over `world` processes, one GPU each (the path shards over
+ * targets; every rank needs all sources). Every rank holds the same state.
  * A force pass still sorts and builds over all bodies, but evaluates accelerations, and nb_step
  * applies the kick-drift, only for this rank's slice of the Morton-ordered bodies:
  *   chunk = ceil(n / world) rounded up to a multiple of 32, slice = [rank * chunk, (rank+1) * chunk) ∩ [0, n).
