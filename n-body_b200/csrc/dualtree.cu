@@ -1184,7 +1184,7 @@ void launch_dual_traverse(const DualNodes &nodes, const int *num_nodes, const fl
     load_balanced_break_kernel<<<1, 32, 0, s>>>(nodes, num_nodes, ws.roots, ws.num_roots, err);
     // passive nodes of at most `frontier` bodies below a larger parent are handed to the second
     // kernel, which balances them over the whole GPU
-    const int frontier = (int) std::max<int64_t>(256, n / 4096);
+    const int frontier = (int) std::max<int64_t>(64, n / 4096);
     dual_kernel<false><<<kDualRoots, kThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta, acc,
                                                        counts, ws.roots, ws.num_roots, ws.arena, (int) ws.arena_words,
                                                        ws.tasks, ws.near, ws.spill, frontier, err);
