@@ -224,8 +224,11 @@ int ensure_dual(nb_ctx *ctx) {
     NB_TRY(dev_alloc(&ctx->dws.roots, kDualRoots), "alloc dual roots");
     NB_TRY(dev_alloc(&ctx->dws.num_roots, 1), "alloc dual roots");
     ctx->dws.arena_words = dual_arena_words(c);
-    NB_TRY(dev_alloc(&ctx->dws.arena, (size_t) kDualRoots * (size_t) ctx->dws.arena_words), "alloc dual arena");
-    NB_TRY(dev_alloc(&ctx->dws.tasks, (size_t) kDualRoots * kDualTasks * 6), "alloc dual tasks");
+    // one arena and task stack per traversal block: the start-node blocks and the frontier blocks
+    if (ctx->dws.frontier_blocks == 0) ctx->dws.frontier_blocks = dual_frontier_blocks(ctx->cfg.device);
+    ctx->dws.blocks = std::max(kDualRoots, ctx->dws.frontier_blocks);
+    NB_TRY(dev_alloc(&ctx->dws.arena, (size_t) ctx->dws.blocks * (size_t) ctx->dws.arena_words), "alloc dual arena");
+    NB_TRY(dev_alloc(&ctx->dws.tasks, (size_t) ctx->dws.blocks * kDualTasks * 6), "alloc dual tasks");
     NearPool &np = ctx->dws.near;
     np.head_cap = (int64_t) slots;
     dual_near_sizes(c, &np.item_cap, &np.word_cap);
@@ -246,7 +249,6 @@ int ensure_dual(nb_ctx *ctx) {
     NB_TRY(dev_alloc(&sp.rec_field, (size_t) sp.rec_cap), "alloc frontier pool");
     NB_TRY(dev_alloc(&sp.words, (size_t) sp.word_cap), "alloc frontier pool");
     NB_TRY(dev_alloc(&sp.counters, 4), "alloc frontier pool");
-    if (ctx->dws.frontier_blocks == 0) ctx->dws.frontier_blocks = dual_frontier_blocks(ctx->cfg.device);
     ctx->dual_cap = c;
     return NB_OK;
 }
@@ -409,7 +411,7 @@ int dual_traverse(nb_ctx *ctx, int64_t n, cudaStream_t s) {
         if (arena) {
             dev_free(ctx->dws.arena);
             ctx->dws.arena_words = std::min<int64_t>(2 * ctx->dws.arena_words, int64_t(1) << 28);
-            NB_TRY(dev_alloc(&ctx->dws.arena, (size_t) kDualRoots * (size_t) ctx->dws.arena_words),
+            NB_TRY(dev_alloc(&ctx->dws.arena, (size_t) ctx->dws.blocks * (size_t) ctx->dws.arena_words),
                    "grow dual arena");
         }
         e &= ~(uint32_t) (kErrNearPool | kErrDualArena);

@@ -48,7 +48,7 @@ namespace nbg {
 
 namespace {
 
-constexpr int kThreads = 512;  // traversal block: one per start node, the whole block per task
+constexpr int kThreads = 256;  // traversal block: the whole block works on one task at a time
 constexpr int kWarps = kThreads / 32;
 constexpr int kTaskInts = 6;  // type, passive node, list offset, list length, field offset, arena top
 constexpr int kLockstep = 0, kPassive = 1;
@@ -1214,7 +1214,7 @@ int dual_frontier_blocks(int device) {
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dual_kernel<true>, kThreads, 0);
-    return std::max(1, std::min(kDualRoots, sms * std::max(per_sm, 1)));  // one arena per block
+    return std::max(1, sms * std::max(per_sm, 1));
 }
 
 int dual_near_blocks(int device) {

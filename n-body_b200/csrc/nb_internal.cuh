@@ -219,6 +219,7 @@ struct DualWorkspace {
     int near_blocks = 0;            // resident blocks of the near-field kernel
     SpillPool spill;
     int frontier_blocks = 0;        // resident blocks of the frontier-task kernel
+    int blocks = 0;                 // arenas and task stacks allocated (one per traversal block)
 };
 // Arena words per block, near-pool sizes and the near kernel's resident grid for n bodies.
 int64_t dual_arena_words(int64_t n);
