@@ -201,6 +201,8 @@ typedef struct nb_server_stats {
     int64_t body_steps;      /* body-steps advanced so far */
     int64_t ticks, relayouts;
     uint64_t resident_bytes; /* budget charge of the running requests */
+    int64_t cancelled;       /* requests dropped by nb_server_cancel */
+    int64_t failed_ticks;    /* ticks that returned an error (the server stayed consistent) */
 } nb_server_stats;
 int nb_server_create(const nb_config *cfg, uint64_t hbm_budget_bytes, nb_server **out);
 int nb_server_destroy(nb_server *sv);
@@ -208,10 +210,19 @@ const char *nb_server_last_error(const nb_server *sv);
 /* The server's solver context (for nb_set_stream, nb_enable_timing, nb_get_counts). */
 void *nb_server_context(nb_server *sv);
 /* Queue a request (bodies copied; velocity may be NULL). Fails with NB_ERR_OUT_OF_MEMORY when
- * the request alone exceeds the budget. */
+ * the request alone exceeds the budget, and with NB_ERR_INVALID_ARGUMENT for non-finite input. */
 int nb_server_submit(nb_server *sv, int64_t n, const float *pos_mass, const float *velocity, float theta,
                      int32_t steps, int64_t *request_id);
+/* One tick. A failed tick leaves the server consistent: if the new layout could not be staged,
+ * the newly admitted requests return to the front of the queue; if it was staged but could not be
+ * loaded, the next tick loads it before stepping. */
 int nb_server_tick(nb_server *sv, int32_t *completed_now);
+/* Drop a request: queued or done ones at once, running ones from the layout at the next tick.
+ * A cancelled request is forgotten. */
+int nb_server_cancel(nb_server *sv, int64_t request_id);
+/* Fault injection for tests: the next `count` device allocations at `point` fail
+ * (0: the re-layout's staging buffers, 1: the context's buffers when they must grow). */
+int nb_server_inject_alloc_failures(nb_server *sv, int32_t point, int32_t count);
 /* state: 0 queued, 1 running, 2 done. */
 int nb_server_status(nb_server *sv, int64_t request_id, int32_t *state, int32_t *steps_done);
 /* Final bodies of a done request in its caller order (then the request is forgotten). */

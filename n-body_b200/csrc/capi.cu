@@ -10,6 +10,7 @@
 // and Solver::step adds the kick-drift kernel (which also reduces the next bounding box).
 // No phase has a host fallback: without a usable device nb_create fails.
 #include <algorithm>
+#include <cmath>
 #include <array>
 #include <cstdio>
 #include <cstring>
@@ -1236,7 +1237,8 @@ struct ServedRequest {
     float theta = 0.f;
     int32_t steps = 0, done = 0;
     int32_t state = 0;   // 0 queued, 1 running, 2 done
-    int64_t start = -1;  // first body position in the batch while resident
+    bool cancel = false; // running request to drop at the next tick
+    int64_t start = -1;  // first body position in the batch (or in the staged layout) while resident
     std::vector<float> pm, vel;  // input until admitted, result once done
 };
 
@@ -1253,59 +1255,91 @@ struct nb_server {
     float4 *tpos = nullptr, *tvel = nullptr;
     uint32_t *tid = nullptr;
     int64_t tcap = 0;
+    bool staged = false;          // the staging buffers hold the running set's layout; the context does not
+    bool dirty = false;           // the context's layout still holds requests that left the running set
+    int32_t fail_next[2] = {0, 0};  // injected allocation failures: staging buffers, context buffers
     nb_server_stats stats{};
 };
+
+// An injected allocation failure at `point` (fault-injection tests), consumed once.
+static bool injected(nb_server *sv, int point) {
+    if (sv->fail_next[point] <= 0) return false;
+    sv->fail_next[point] -= 1;
+    return true;
+}
 
 static int server_fail(nb_server *sv, int rc) {
     if (sv && sv->ctx) sv->error = sv->ctx->error;
     return rc;
 }
 
+// Lays the running set out anew. Two stages, so that a failure leaves a consistent server:
+//   1. staging: the staging buffers are grown if needed and every running request is copied into
+//      them (resident ones from the context, newcomers from their host copies). A failure here
+//      changes nothing; the caller puts the newcomers back in the queue.
+//   2. loading: the context's buffers are grown if needed and the staged layout is copied in,
+//      with the batch tables. A failure here leaves the layout staged (`staged`); the next tick
+//      finishes it before stepping.
 static int server_relayout(nb_server *sv) {
     nb_ctx *ctx = sv->ctx;
     cudaStream_t s = ctx->stream;
     int64_t total = 0;
     for (auto *r: sv->active) total += r->n;
-    if (total > sv->tcap) {
-        dev_free(sv->tpos); dev_free(sv->tvel); dev_free(sv->tid);
-        sv->tcap = 0;
-        if (dev_alloc(&sv->tpos, (size_t) total) != cudaSuccess || dev_alloc(&sv->tvel, (size_t) total) != cudaSuccess ||
-            dev_alloc(&sv->tid, (size_t) total) != cudaSuccess) {
-            sv->error = "out of device memory for the re-layout";
-            return NB_ERR_OUT_OF_MEMORY;
-        }
-        sv->tcap = total;
-    }
-    int64_t off = 0;
-    for (auto *r: sv->active) {
-        const size_t bytes = (size_t) r->n * sizeof(float4);
-        if (r->start >= 0) {  // resident: move device-to-device, rebase the caller indices
-            if (cudaMemcpyAsync(sv->tpos + off, ctx->pos + r->start, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
-                cudaMemcpyAsync(sv->tvel + off, ctx->vel + r->start, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
-                cudaMemcpyAsync(sv->tid + off, ctx->id + r->start, (size_t) r->n * 4, cudaMemcpyDeviceToDevice, s) !=
-                    cudaSuccess) {
-                sv->error = "re-layout copy failed";
-                return NB_ERR_CUDA;
+    if (!sv->staged) {
+        if (total > sv->tcap) {
+            if (injected(sv, 0)) {
+                sv->error = "out of device memory for the re-layout (injected)";
+                return NB_ERR_OUT_OF_MEMORY;
             }
-            launch_add_offset(sv->tid + off, r->n, off - r->start, s);
-        } else {  // newcomer: one copy in
-            if (cudaMemcpyAsync(sv->tpos + off, r->pm.data(), bytes, cudaMemcpyHostToDevice, s) != cudaSuccess ||
-                cudaMemcpyAsync(sv->tvel + off, r->vel.data(), bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) {
-                sv->error = "copy-in failed";
-                return NB_ERR_CUDA;
+            dev_free(sv->tpos); dev_free(sv->tvel); dev_free(sv->tid);
+            sv->tcap = 0;
+            if (dev_alloc(&sv->tpos, (size_t) total) != cudaSuccess ||
+                dev_alloc(&sv->tvel, (size_t) total) != cudaSuccess ||
+                dev_alloc(&sv->tid, (size_t) total) != cudaSuccess) {
+                cudaGetLastError();
+                dev_free(sv->tpos); dev_free(sv->tvel); dev_free(sv->tid);
+                sv->error = "out of device memory for the re-layout";
+                return NB_ERR_OUT_OF_MEMORY;
             }
-            launch_iota(sv->tid + off, r->n, s, (uint32_t) off);
+            sv->tcap = total;
         }
-        r->start = off;
-        off += r->n;
+        int64_t off = 0;
+        for (auto *r: sv->active) {
+            const size_t bytes = (size_t) r->n * sizeof(float4);
+            if (r->start >= 0) {  // resident: move device-to-device, rebase the caller indices
+                if (cudaMemcpyAsync(sv->tpos + off, ctx->pos + r->start, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+                    cudaMemcpyAsync(sv->tvel + off, ctx->vel + r->start, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+                    cudaMemcpyAsync(sv->tid + off, ctx->id + r->start, (size_t) r->n * 4, cudaMemcpyDeviceToDevice, s) !=
+                        cudaSuccess) {
+                    sv->error = "re-layout copy failed";
+                    return NB_ERR_CUDA;
+                }
+                launch_add_offset(sv->tid + off, r->n, off - r->start, s);
+            } else {  // newcomer: one copy in
+                if (cudaMemcpyAsync(sv->tpos + off, r->pm.data(), bytes, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+                    cudaMemcpyAsync(sv->tvel + off, r->vel.data(), bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+                    sv->error = "copy-in failed";
+                    return NB_ERR_CUDA;
+                }
+                launch_iota(sv->tid + off, r->n, s, (uint32_t) off);
+            }
+            off += r->n;
+        }
+        if (cudaStreamSynchronize(s) != cudaSuccess) {
+            sv->error = "re-layout failed";
+            return NB_ERR_CUDA;
+        }
+        off = 0;
+        for (auto *r: sv->active) {
+            r->start = off;
+            off += r->n;
+        }
+        sv->staged = true;
     }
-    if (cudaStreamSynchronize(s) != cudaSuccess) {
-        sv->error = "re-layout failed";
-        return NB_ERR_CUDA;
-    }
-    for (auto *r: sv->active) {  // host input copies are no longer needed
-        std::vector<float>().swap(r->pm);
-        std::vector<float>().swap(r->vel);
+    // 2. loading
+    if (total > ctx->cap && injected(sv, 1)) {
+        sv->error = "out of device memory for the context buffers (injected)";
+        return NB_ERR_OUT_OF_MEMORY;
     }
     int rc = ensure_capacity(ctx, total);
     if (rc != NB_OK) return server_fail(sv, rc);
@@ -1317,22 +1351,29 @@ static int server_relayout(nb_server *sv) {
     ctx->have_tree = false;
     ctx->have_acc = false;
     sv->stats.relayouts += 1;
-    if (total == 0) return NB_OK;
-    const size_t bytes = (size_t) total * sizeof(float4);
-    if (cudaMemcpyAsync(ctx->pos, sv->tpos, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
-        cudaMemcpyAsync(ctx->vel, sv->tvel, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
-        cudaMemcpyAsync(ctx->id, sv->tid, (size_t) total * 4, cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
-        sv->error = "re-layout copy failed";
-        return NB_ERR_CUDA;
+    if (total > 0) {
+        const size_t bytes = (size_t) total * sizeof(float4);
+        if (cudaMemcpyAsync(ctx->pos, sv->tpos, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+            cudaMemcpyAsync(ctx->vel, sv->tvel, bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+            cudaMemcpyAsync(ctx->id, sv->tid, (size_t) total * 4, cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+            sv->error = "re-layout copy failed";
+            return NB_ERR_CUDA;
+        }
+        std::vector<int64_t> sizes;
+        std::vector<float> thetas;
+        for (auto *r: sv->active) {
+            sizes.push_back(r->n);
+            thetas.push_back(r->theta);
+        }
+        rc = build_batch_tables(ctx, (int32_t) sizes.size(), sizes.data(), thetas.data());
+        if (rc != NB_OK) return server_fail(sv, rc);
     }
-    std::vector<int64_t> sizes;
-    std::vector<float> thetas;
-    for (auto *r: sv->active) {
-        sizes.push_back(r->n);
-        thetas.push_back(r->theta);
+    sv->staged = false;
+    for (auto *r: sv->active) {  // host input copies are no longer needed
+        std::vector<float>().swap(r->pm);
+        std::vector<float>().swap(r->vel);
     }
-    rc = build_batch_tables(ctx, (int32_t) sizes.size(), sizes.data(), thetas.data());
-    return rc == NB_OK ? NB_OK : server_fail(sv, rc);
+    return NB_OK;
 }
 
 // Copies a running request's bodies out, in its caller order.
@@ -1406,6 +1447,12 @@ int nb_server_submit(nb_server *sv, int64_t n, const float *pos_mass, const floa
         sv->error = "request larger than the whole memory budget";
         return NB_ERR_OUT_OF_MEMORY;
     }
+    for (int64_t k = 0; k < 4 * n; ++k) {
+        if (!std::isfinite(pos_mass[k]) || (velocity && !std::isfinite(velocity[k]))) {
+            sv->error = "non-finite position, mass or velocity";
+            return NB_ERR_INVALID_ARGUMENT;
+        }
+    }
     auto *r = new ServedRequest();
     r->id = sv->next_id++;
     r->n = n;
@@ -1425,12 +1472,26 @@ int nb_server_tick(nb_server *sv, int32_t *completed_now) {
     if (!sv) return NB_ERR_INVALID_ARGUMENT;
     nb_ctx *ctx = sv->ctx;
     if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return NB_ERR_CUDA;
+    if (completed_now) *completed_now = 0;
+    // 0. a layout left staged by a failed tick is loaded before anything else
+    if (sv->staged) {
+        int rc = server_relayout(sv);
+        if (rc != NB_OK) {
+            sv->stats.failed_ticks += 1;
+            return rc;
+        }
+    }
     int32_t completed = 0;
-    bool changed = false;
-    // 1. retire requests whose steps are done
+    bool changed = sv->dirty;
+    // 1. retire requests whose steps are done, drop cancelled ones
     std::vector<ServedRequest *> keep;
     for (auto *r: sv->active) {
-        if (r->done >= r->steps) {
+        if (r->cancel) {
+            sv->all.erase(r->id);
+            delete r;
+            sv->stats.cancelled += 1;
+            changed = true;
+        } else if (r->done >= r->steps) {
             int rc = server_collect(sv, r);
             if (rc != NB_OK) return rc;
             r->state = 2;
@@ -1445,6 +1506,7 @@ int nb_server_tick(nb_server *sv, int32_t *completed_now) {
     // 2. admit queued requests in arrival order while they fit the budget
     uint64_t resident = 0;
     for (auto *r: sv->active) resident += (uint64_t) r->n * kResidentBytesPerBody;
+    std::vector<ServedRequest *> admitted;
     while (!sv->queue.empty()) {
         ServedRequest *r = sv->queue.front();
         const uint64_t need = (uint64_t) r->n * kResidentBytesPerBody;
@@ -1458,13 +1520,36 @@ int nb_server_tick(nb_server *sv, int32_t *completed_now) {
         r->state = 1;
         r->start = -1;
         sv->active.push_back(r);
+        admitted.push_back(r);
         resident += need;
         changed = true;
     }
+    sv->stats.completed += completed;
+    if (completed_now) *completed_now = completed;
     if (changed) {
         int rc = server_relayout(sv);
-        if (rc != NB_OK) return rc;
+        if (rc != NB_OK) {
+            sv->stats.failed_ticks += 1;
+            if (!sv->staged) {
+                // nothing was laid out: the newcomers go back to the front of the queue, in order
+                for (auto it = admitted.rbegin(); it != admitted.rend(); ++it) {
+                    (*it)->state = 0;
+                    sv->queue.push_front(*it);
+                }
+                sv->active.resize(sv->active.size() - admitted.size());
+                resident = 0;
+                for (auto *r: sv->active) resident += (uint64_t) r->n * kResidentBytesPerBody;
+                // the context keeps its previous layout (retired or cancelled requests included,
+                // stepped but unused) until the next tick lays the running set out again
+                sv->dirty = true;
+            }
+            sv->stats.queued = (int64_t) sv->queue.size();
+            sv->stats.running = (int64_t) sv->active.size();
+            sv->stats.resident_bytes = resident;
+            return rc;
+        }
     }
+    sv->dirty = false;
     // 3. one batched step for every running request
     if (!sv->active.empty()) {
         int rc = nb_step(ctx, 1);
@@ -1475,11 +1560,41 @@ int nb_server_tick(nb_server *sv, int32_t *completed_now) {
         }
     }
     sv->stats.ticks += 1;
-    sv->stats.completed += completed;
     sv->stats.queued = (int64_t) sv->queue.size();
     sv->stats.running = (int64_t) sv->active.size();
     sv->stats.resident_bytes = resident;
-    if (completed_now) *completed_now = completed;
+    return NB_OK;
+}
+
+int nb_server_cancel(nb_server *sv, int64_t request_id) {
+    if (!sv) return NB_ERR_INVALID_ARGUMENT;
+    auto it = sv->all.find(request_id);
+    if (it == sv->all.end()) {
+        sv->error = "unknown request";
+        return NB_ERR_INVALID_ARGUMENT;
+    }
+    ServedRequest *r = it->second;
+    if (r->state == 1) {  // running: dropped from the layout at the next tick
+        r->cancel = true;
+        return NB_OK;
+    }
+    if (r->state == 0) {
+        for (auto q = sv->queue.begin(); q != sv->queue.end(); ++q) {
+            if (*q == r) {
+                sv->queue.erase(q);
+                break;
+            }
+        }
+    }
+    sv->all.erase(it);
+    delete r;
+    sv->stats.cancelled += 1;
+    return NB_OK;
+}
+
+int nb_server_inject_alloc_failures(nb_server *sv, int32_t point, int32_t count) {
+    if (!sv || point < 0 || point > 1 || count < 0) return NB_ERR_INVALID_ARGUMENT;
+    sv->fail_next[point] = count;
     return NB_OK;
 }
 

@@ -78,6 +78,8 @@ class ServerStats(C.Structure):
         ("ticks", C.c_int64),
         ("relayouts", C.c_int64),
         ("resident_bytes", C.c_uint64),
+        ("cancelled", C.c_int64),
+        ("failed_ticks", C.c_int64),
     ]
 
     def as_dict(self):
@@ -143,6 +145,8 @@ SIGNATURES = {
     "nb_server_context": (_vp, [_vp]),
     "nb_server_submit": (C.c_int, [_vp, _i64, _vp, _vp, C.c_float, _i32, C.POINTER(_i64)]),
     "nb_server_tick": (C.c_int, [_vp, C.POINTER(_i32)]),
+    "nb_server_cancel": (C.c_int, [_vp, _i64]),
+    "nb_server_inject_alloc_failures": (C.c_int, [_vp, _i32, _i32]),
     "nb_server_status": (C.c_int, [_vp, _i64, C.POINTER(_i32), C.POINTER(_i32)]),
     "nb_server_take_result": (C.c_int, [_vp, _i64, _vp, _vp]),
     "nb_server_get_stats": (C.c_int, [_vp, C.POINTER(ServerStats)]),
@@ -544,6 +548,14 @@ class Server:
         s = ServerStats()
         self._check(lib().nb_server_get_stats(self._h, C.byref(s)))
         return s.as_dict()
+
+    def cancel(self, rid: int):
+        self._check(lib().nb_server_cancel(self._h, rid))
+
+    def inject_alloc_failures(self, point: int, count: int = 1):
+        """Fault injection for tests: the next `count` allocations at `point` fail (0: staging
+        buffers of the re-layout, 1: the context's buffers)."""
+        self._check(lib().nb_server_inject_alloc_failures(self._h, point, count))
 
 
 def decode_records(records: np.ndarray, order: int) -> dict:

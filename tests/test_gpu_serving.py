@@ -73,3 +73,72 @@ def test_zero_step_request_returns_its_input(nb):
         sv.tick()
         out = sv.take_result(r, 100)
     assert np.array_equal(out[0], pm) and np.array_equal(out[1], vel)
+
+
+def test_rejects_non_finite_input(nb):
+    pm, vel = nb.scenarios.plummer(100, seed=4)
+    with nb.Server(rule=nb.Gravity(1.0, EPS), time_step=DT) as sv:
+        bad = pm.copy()
+        bad[7, 1] = np.nan
+        with pytest.raises(nb.NBodyError):
+            sv.submit(bad, vel, steps=1)
+        badv = vel.copy()
+        badv[3, 0] = np.inf
+        with pytest.raises(nb.NBodyError):
+            sv.submit(pm, badv, steps=1)
+        assert sv.stats()["submitted"] == 0
+
+
+def test_cancel_queued_and_running(nb):
+    sizes = [3000, 2000, 1500]
+    data = [nb.scenarios.plummer(n, seed=50 + k) for k, n in enumerate(sizes)]
+    with nb.Server(rule=nb.Gravity(1.0, EPS), time_step=DT, hbm_budget_bytes=(3000 + 2000) * 544) as sv:
+        a = sv.submit(*data[0], theta=0.5, steps=4)
+        b = sv.submit(*data[1], theta=0.5, steps=4)
+        c = sv.submit(*data[2], theta=0.5, steps=3)  # waits for memory
+        sv.tick()
+        assert sv.status(c)[0] == nb.Server.QUEUED
+        sv.cancel(c)  # queued: gone at once
+        with pytest.raises(nb.NBodyError):
+            sv.status(c)
+        sv.cancel(b)  # running: dropped from the layout at the next tick
+        while sv.status(a)[0] != nb.Server.DONE:
+            sv.tick()
+        with pytest.raises(nb.NBodyError):
+            sv.status(b)
+        st = sv.stats()
+        ra = sv.take_result(a, sizes[0])
+    assert st["cancelled"] == 2 and st["completed"] == 1
+    assert np.array_equal(ra[0], alone(nb, *data[0], 0.5, 4)[0])
+
+
+@pytest.mark.parametrize("point", [0, 1])
+def test_allocation_failure_keeps_server_consistent(nb, point):
+    """An allocation failure during a re-layout (injected on the host) fails that tick; the server
+    stays consistent, and once memory is available again every request still ends bit-identical
+    to a standalone run."""
+    small = [nb.scenarios.plummer(n, seed=70 + k) for k, n in enumerate([800, 600])]
+    big = nb.scenarios.plummer(9000, seed=79)  # needs larger staging and context buffers
+    with nb.Server(rule=nb.Gravity(1.0, EPS), time_step=DT) as sv:
+        ids = [sv.submit(*small[0], theta=0.5, steps=5), sv.submit(*small[1], theta=0.6, steps=5)]
+        sv.tick()
+        sv.tick()
+        sv.inject_alloc_failures(point, 1)
+        ids.append(sv.submit(*big, theta=0.5, steps=3))
+        with pytest.raises(nb.NBodyError):
+            sv.tick()
+        st = sv.stats()
+        assert st["failed_ticks"] == 1
+        if point == 0:
+            assert sv.status(ids[2])[0] == nb.Server.QUEUED  # put back, nothing laid out
+        else:
+            assert sv.status(ids[2])[0] == nb.Server.RUNNING  # staged; loaded at the next tick
+        guard = 0
+        while any(sv.status(r)[0] != nb.Server.DONE for r in ids):
+            sv.tick()
+            guard += 1
+            assert guard < 50
+        results = [sv.take_result(r, n) for r, n in zip(ids, [800, 600, 9000])]
+    refs = [alone(nb, *small[0], 0.5, 5), alone(nb, *small[1], 0.6, 5), alone(nb, *big, 0.5, 3)]
+    for (p, v), (pr, vr) in zip(results, refs):
+        assert np.array_equal(p, pr) and np.array_equal(v, vr)
