@@ -19,6 +19,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/nbody_gpu.h"
 #include "nb_internal.cuh"
 
@@ -318,16 +320,27 @@ cudaEvent_t take_event(nb_ctx *ctx) {
     return e;
 }
 
+// Phase boundaries of one pass: CUDA events on the context's stream when timing is enabled, and
+// an NVTX range per phase (host side, for timeline profilers; near free without one attached).
 struct Marks {
     nb_ctx *ctx;
     std::array<cudaEvent_t, kNumMarks> ev{};
     bool on;
+    bool range_open = false;
     explicit Marks(nb_ctx *c) : ctx(c), on(c->timing) {
         if (on)
             for (auto &e: ev) e = take_event(c);
     }
+    ~Marks() {
+        if (range_open) nvtxRangePop();
+    }
     void mark(int phase) {
+        static const char *const names[kNumMarks] = {"nb.bbox", "nb.morton", "nb.sort", "nb.gather", "nb.build",
+                                                     "nb.traverse", "nb.integrate", "nb.end"};
         if (on) cudaEventRecord(ev[phase], ctx->stream);
+        if (range_open) nvtxRangePop();
+        range_open = phase != kEnd;
+        if (range_open) nvtxRangePushA(names[phase]);
     }
     void commit() {
         if (on) ctx->pending.push_back(ev);
