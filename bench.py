@@ -631,7 +631,7 @@ def serving_pools(seed=45, n_max=1 << 21):
 
 
 def serve_run(nb, pools, rate, duration, rng, eps, steps_range=(10, 1000), n_range=(2048, 1 << 21),
-              budget=150 * 10 ** 9, drain=0.0):
+              budget=150 * 10 ** 9, drain=0.0, leaf=LEAF):
     """Open-loop Poisson arrivals for `duration` seconds (then `drain` more seconds of ticks).
     Latency = completion time - arrival time, wall clock."""
     arrivals = []
@@ -643,7 +643,7 @@ def serve_run(nb, pools, rate, duration, rng, eps, steps_range=(10, 1000), n_ran
         theta = float(rng.uniform(0.4, 0.7))
         arrivals.append((t, n, steps, theta, pm, vel))
         t += rng.exponential(1.0 / rate)
-    sv = nb.Server(rule=nb.Gravity(1.0, eps), order=ORDER, max_leaf_size=LEAF, time_step=DT, hbm_budget_bytes=budget)
+    sv = nb.Server(rule=nb.Gravity(1.0, eps), order=ORDER, max_leaf_size=leaf, time_step=DT, hbm_budget_bytes=budget)
     pending = {}  # id -> (arrival time, bodies)
     latencies = []
     t0 = time.perf_counter()
@@ -684,6 +684,22 @@ def serve_run(nb, pools, rate, duration, rng, eps, steps_range=(10, 1000), n_ran
     }
 
 
+def serving_leaf(nb, pools, eps, requests=64, seed=47):
+    """Leaf size for the server, measured on a sample batch of requests drawn like the stream."""
+    rng = np.random.default_rng(seed)
+    sizes, bodies, thetas = [], [], []
+    for _ in range(requests):
+        _, pm, _ = pools[rng.integers(0, 2)]
+        n = int(np.round(np.exp(rng.uniform(np.log(2048), np.log(1 << 21)))))
+        sizes.append(n)
+        bodies.append(pm[:n])
+        thetas.append(rng.uniform(0.4, 0.7))
+    with nb.QuadrupoleLinearBVHSolver(rule=nb.Gravity(1.0, eps), time_step=DT) as s:
+        s.set_instances(sizes, np.concatenate(bodies), thetas=np.asarray(thetas, np.float32))
+        tuned = s.autotune(candidates=(6, 8, 12, 16, 24), passes=1)
+    return tuned.leaf, tuned
+
+
 def run_serving(args):
     import torch
 
@@ -694,11 +710,12 @@ def run_serving(args):
     eps = float(np.float32(BATCH_SOFTENING) * np.float32(BATCH_SOFTENING))
     pools = serving_pools()
     rng = np.random.default_rng(46 + rank)
-    overload = serve_run(nb, pools, args.rate, args.duration, rng, eps)
+    leaf, tuned = serving_leaf(nb, pools, eps)
+    overload = serve_run(nb, pools, args.rate, args.duration, rng, eps, leaf=leaf)
     # calibrated run: arrival rate at 70 % of the measured capacity for the mean request size
     mean_work = np.mean([np.exp(rng.uniform(np.log(2048), np.log(1 << 21))) for _ in range(20000)]) * 505.0
     rate = max(0.7 * overload["throughput_body_steps_per_s"] / mean_work, 0.05)
-    calibrated = serve_run(nb, pools, rate, args.duration, rng, eps, drain=args.duration)
+    calibrated = serve_run(nb, pools, rate, args.duration, rng, eps, drain=args.duration, leaf=leaf)
     line = {
         "metric": "serving: aggregate body-steps/s and request latency p50/p99 (Poisson arrivals)",
         "value": overload["throughput_body_steps_per_s"], "unit": "body-steps/s", "n_gpus": world,
@@ -706,7 +723,9 @@ def run_serving(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (Plummer or uniform ball, 50/50)",
         "config": {"workload": "serving-poisson", "n_range": [2048, 1 << 21], "steps_range": [10, 1000],
                    "theta_range": [0.4, 0.7], "softening": BATCH_SOFTENING, "hbm_budget_bytes": 150 * 10 ** 9,
-                   "order": ORDER, "leaf_size": LEAF},
+                   "order": ORDER, "leaf_size": leaf},
+        "autotune": {"leaf_size": leaf, "ms_per_force_pass": {str(k): v for k, v in tuned.timings_ms.items()},
+                     "method": "force passes of a 64-request sample batch at each candidate leaf size"},
         "overload_run": overload,
         "calibrated_run": calibrated,
     }
