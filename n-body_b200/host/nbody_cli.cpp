@@ -3,13 +3,15 @@
 //
 //   nbody_cli [-s|--solver ID] [-i|--iterations N] [-t|--timestep DT] [-G|--gravity G]
 //             [-o|--output-file PATH] [--theta T] [--max-leaf-size L] [--epsilon E]
-//             [--device D] [--counts] SCENARIO
+//             [--device D] [--counts] [--checkpoint-every K --checkpoint-prefix P] SCENARIO
 //
 // SCENARIO is a JSON scenario (the reference's schema; a top-level "G" sets the constant, as
 // Application::on_open does) or a tipsy file. The solver ids are the reference's Solver::id()
 // strings. With --iterations 0 nothing runs on the device and the scenario is only converted
 // (JSON out), so I/O needs no GPU. The result is written as a JSON scenario; --counts prints the
-// last force pass's interaction counts as one JSON line on stdout.
+// last force pass's interaction counts as one JSON line on stdout. --checkpoint-every K writes the
+// state every K steps to P.<step>.json (the same schema, so a checkpoint resumes as a scenario).
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -26,15 +28,16 @@ namespace {
 void usage() {
     std::fprintf(stderr,
                  "usage: nbody_cli [-s ID] [-i N] [-t DT] [-G G] [-o OUT.json] [--theta T] [--max-leaf-size L]\n"
-                 "                 [--epsilon E] [--device D] [--counts] SCENARIO(.json|tipsy)\n"
+                 "                 [--epsilon E] [--device D] [--counts] [--checkpoint-every K --checkpoint-prefix P]\n"
+                 "                 SCENARIO(.json|tipsy)\n"
                  "solvers:");
     for (auto &id: solverIds()) std::fprintf(stderr, " %s", id.c_str());
     std::fprintf(stderr, "\n");
 }
 
 struct Options {
-    std::string solver = "linear-bvh-4p", input, output;
-    int iterations = 0, device = 0, leaf = -1;
+    std::string solver = "linear-bvh-4p", input, output, checkpoint_prefix;
+    int iterations = 0, device = 0, leaf = -1, checkpoint_every = 0;
     bool has_dt = false, has_G = false, has_theta = false, has_eps = false, counts = false;
     double dt = 0.0, G = 1.0, theta = 0.0, eps = 0.0;
 };
@@ -59,12 +62,15 @@ bool parse(int argc, char **argv, Options &o) {
         else if (a == "--epsilon") { o.eps = std::atof(next()); o.has_eps = true; }
         else if (a == "--device") o.device = std::atoi(next());
         else if (a == "--counts") o.counts = true;
+        else if (a == "--checkpoint-every") o.checkpoint_every = std::atoi(next());
+        else if (a == "--checkpoint-prefix") o.checkpoint_prefix = next();
         else if (a == "-h" || a == "--help") return false;
         else if (!a.empty() && a[0] == '-') {
             std::fprintf(stderr, "unknown option %s\n", a.c_str());
             return false;
         } else o.input = a;
     }
+    if (o.checkpoint_every < 0 || (o.checkpoint_every > 0 && o.checkpoint_prefix.empty())) return false;
     return !o.input.empty() && o.iterations >= 0;
 }
 
@@ -90,7 +96,21 @@ int main(int argc, char **argv) {
             if (o.has_theta) solver->setTheta((float) o.theta);
             if (o.leaf > 0) solver->setMaxLeafSize(o.leaf);
             if (o.has_dt) solver->setTimeStep((float) o.dt);
-            solver->step(o.iterations);
+            const float G = rule.g();
+            if (o.checkpoint_every > 0) {
+                // device-resident steps between checkpoints; each checkpoint copies the state out once
+                for (int done = 0; done < o.iterations;) {
+                    const int k = std::min(o.checkpoint_every, o.iterations - done);
+                    solver->step(k);
+                    done += k;
+                    const std::string path = o.checkpoint_prefix + "." + std::to_string(done) + ".json";
+                    std::ofstream out(path);
+                    out << scenario_to_json(sim, sc.hasG || o.has_G ? &G : nullptr);
+                    if (!out.good()) throw Error(NB_ERR_INVALID_ARGUMENT, "cannot write " + path);
+                }
+            } else {
+                solver->step(o.iterations);
+            }
             counts = solver->counts();
             solver_id = solver->id();
         }

@@ -154,6 +154,9 @@ def test_cli_rejects_bad_arguments(tmp_path, nb):
     assert run("--bogus", str(src)).returncode == 2
     r = run("-s", "barnes-hut-octree", "-i", "1", str(src))
     assert r.returncode == 1 and "unknown solver id" in r.stderr
+    # a checkpoint interval needs a prefix and must not be negative
+    assert run("-i", "2", "--checkpoint-every", "1", str(src)).returncode == 2
+    assert run("-i", "2", "--checkpoint-every", "-1", "--checkpoint-prefix", str(tmp_path / "c"), str(src)).returncode == 2
 
 
 REFERENCE_SCENARIOS = "/root/reference/scenarios"
