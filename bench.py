@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--workload", choices=["plummer-1m", "batched", "serving", "dual-4m"], default="plummer-1m",
                     help="plummer-1m: one N=2^20 instance (the headline); batched: 256 uneven instances; "
                          "serving: Poisson request stream into the continuous-batching server")
-    ap.add_argument("--duration", type=float, default=20.0, help="serving: seconds of arrivals per run")
+    ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals per run")
     ap.add_argument("--rate", type=float, default=40.0, help="serving: arrivals per second (open loop)")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--shard-targets", action="store_true",
@@ -684,20 +684,66 @@ def serve_run(nb, pools, rate, duration, rng, eps, steps_range=(10, 1000), n_ran
     }
 
 
-def serving_leaf(nb, pools, eps, requests=64, seed=47):
-    """Leaf size for the server, measured on a sample batch of requests drawn like the stream."""
+def serving_sample(pools, requests=64, seed=47):
+    """A sample batch of requests drawn like the stream: sizes, (bodies, velocities), thetas."""
     rng = np.random.default_rng(seed)
     sizes, bodies, thetas = [], [], []
     for _ in range(requests):
-        _, pm, _ = pools[rng.integers(0, 2)]
+        _, pm, vel = pools[rng.integers(0, 2)]
         n = int(np.round(np.exp(rng.uniform(np.log(2048), np.log(1 << 21)))))
         sizes.append(n)
-        bodies.append(pm[:n])
-        thetas.append(rng.uniform(0.4, 0.7))
+        bodies.append((pm[:n], vel[:n]))
+        thetas.append(float(rng.uniform(0.4, 0.7)))
+    return sizes, bodies, thetas
+
+
+def serving_leaf(nb, sample, eps):
+    """Leaf size for the server, measured on the sample batch of requests."""
+    sizes, bodies, thetas = sample
     with nb.QuadrupoleLinearBVHSolver(rule=nb.Gravity(1.0, eps), time_step=DT) as s:
-        s.set_instances(sizes, np.concatenate(bodies), thetas=np.asarray(thetas, np.float32))
+        s.set_instances(sizes, np.concatenate([b[0] for b in bodies]), thetas=np.asarray(thetas, np.float32))
         tuned = s.autotune(candidates=(6, 8, 12, 16, 24), passes=1)
     return tuned.leaf, tuned
+
+
+def serving_sample_vs_sequential(nb, sample, eps, leaf, torch, steps=2):
+    """The sample batch advanced together (one batched step per tick, as the server runs it) against
+    the same requests advanced one after another through the plain single-instance path, on the
+    device clock. Both run the same steps of the same bodies, with identical results."""
+    sizes, bodies, thetas = sample
+    total = int(sum(sizes))
+    stream = torch.cuda.Stream()  # the contexts launch on this stream, the events are recorded on it
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    with nb.QuadrupoleLinearBVHSolver(rule=nb.Gravity(1.0, eps), max_leaf_size=leaf, time_step=DT) as s:
+        s.set_stream(stream.cuda_stream)
+        s.set_instances(sizes, np.concatenate([b[0] for b in bodies]), np.concatenate([b[1] for b in bodies]),
+                        np.asarray(thetas, np.float32))
+        s.step(3)
+        torch.cuda.synchronize()
+        t0.record(stream)
+        s.step(steps)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        batched_ms = t0.elapsed_time(t1)
+    seq_ms = 0.0
+    for n, (pm, vel), theta in zip(sizes, bodies, thetas):
+        with nb.QuadrupoleLinearBVHSolver(bodies=pm, velocities=vel, rule=nb.Gravity(1.0, eps), theta=theta,
+                                          max_leaf_size=leaf, time_step=DT) as c:
+            c.set_stream(stream.cuda_stream)
+            c.step(1)
+            torch.cuda.synchronize()
+            t0.record(stream)
+            c.step(steps)
+            t1.record(stream)
+            torch.cuda.synchronize()
+            seq_ms += t0.elapsed_time(t1)
+    batched = total * steps / (batched_ms / 1000.0)
+    sequential = total * steps / (seq_ms / 1000.0)
+    return {"requests": len(sizes), "total_bodies": total, "steps": steps, "leaf_size": leaf,
+            "batched_body_steps_per_s": batched, "sequential_plain_body_steps_per_s": sequential,
+            "ratio_batched_over_sequential": batched / sequential,
+            "ratio_served_over_sequential": None}
 
 
 def run_serving(args):
@@ -710,8 +756,13 @@ def run_serving(args):
     eps = float(np.float32(BATCH_SOFTENING) * np.float32(BATCH_SOFTENING))
     pools = serving_pools()
     rng = np.random.default_rng(46 + rank)
-    leaf, tuned = serving_leaf(nb, pools, eps)
+    sample = serving_sample(pools)
+    leaf, tuned = serving_leaf(nb, sample, eps)
+    versus = serving_sample_vs_sequential(nb, sample, eps, leaf, torch)
     overload = serve_run(nb, pools, args.rate, args.duration, rng, eps, leaf=leaf)
+    # the server's own throughput (re-layouts, admission and retirement included) on the stream
+    versus["ratio_served_over_sequential"] = (overload["throughput_body_steps_per_s"] /
+                                              versus["sequential_plain_body_steps_per_s"])
     # calibrated run: arrival rate at 70 % of the measured capacity for the mean request size
     mean_work = np.mean([np.exp(rng.uniform(np.log(2048), np.log(1 << 21))) for _ in range(20000)]) * 505.0
     rate = max(0.7 * overload["throughput_body_steps_per_s"] / mean_work, 0.05)
@@ -726,6 +777,7 @@ def run_serving(args):
                    "order": ORDER, "leaf_size": leaf},
         "autotune": {"leaf_size": leaf, "ms_per_force_pass": {str(k): v for k, v in tuned.timings_ms.items()},
                      "method": "force passes of a 64-request sample batch at each candidate leaf size"},
+        "sample_batch_vs_sequential": versus,
         "overload_run": overload,
         "calibrated_run": calibrated,
     }
