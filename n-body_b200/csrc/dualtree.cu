@@ -906,27 +906,13 @@ constexpr int kPriv = 16;                      // queued M2P nodes per target
 struct NearWarp {
     int2 stack[kNearStack];
     int priv[kPriv][32];  // [slot][target]
-    float4 tile[32];      // staged source bodies, then the replicas' partial sums
+    float4 tile[32];      // staged source bodies (16 interleaved pairs), then the replicas' partial sums
 };
 
 struct Lane {
     int t, r, T, G;     // target, replica, targets in the unit, replicas
     bool active;        // r < G
 };
-
-// Gravity::particleParticle (Gravity.h:199-209) without G, added into a. With eps > 0 a source at
-// the target's own position contributes -0 * s = 0 and needs no test; with eps = 0 it is skipped.
-template<bool EPS0>
-__device__ __forceinline__ void pair_nog(float4 b, const float p[3], float eps, float a[3]) {
-    const float rx = p[0] - b.x, ry = p[1] - b.y, rz = p[2] - b.z;
-    const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps)));
-    if (EPS0 && r2 == 0.f) return;
-    const float inv = rsqrtf(r2);
-    const float s = b.w * (inv * inv * inv);
-    a[0] = fmaf(-rx, s, a[0]);
-    a[1] = fmaf(-ry, s, a[1]);
-    a[2] = fmaf(-rz, s, a[2]);
-}
 
 // Gravity::nodeParticle for MultipoleMassSummary<3> (Gravity.h:239-259) without G, added into a:
 //   a += -M R / r^3 + (D3 : Q2) / 2 - (D4 : Q3) / 6,
@@ -970,29 +956,69 @@ __device__ __noinline__ void m2p_nog(const Ctx &x, int k, const float p[3], floa
     a[2] += fmaf(rz, sr, fmaf(qrz, s2q, -fmaf(oz, s4o, tz * s4t)));
 }
 
-// Pairs of the unit's targets with sources src(0..m) for lanes in `mine`: 32 sources at a time
-// are staged in shared memory; replica r takes sources r, r + G, ... of each tile.
+// Gravity::particleParticle (Gravity.h:199-209) without G for two sources against one target, in
+// paired FP32 arithmetic (sm_100 FADD2/FFMA2/FMUL2: one instruction for both halves):
+// u = (x_a, x_b, y_a, y_b), v = (z_a, z_b, m_a, m_b), np = -p in both halves. Per half:
+// d = b - p, r2 = d.d + eps, a += d m / r2^(3/2). With eps > 0 a source at the target's own
+// position adds 0 * s = 0 and a padding source (zero mass at the origin) adds 0; with eps = 0 a
+// source at zero distance is skipped.
+template<bool EPS0>
+__device__ __forceinline__ void pair2_nog(float2 npx, float2 npy, float2 npz, float2 eps2, float4 u, float4 v,
+                                          float2 &ax, float2 &ay, float2 &az) {
+    const float2 dx = __fadd2_rn(make_float2(u.x, u.y), npx);
+    const float2 dy = __fadd2_rn(make_float2(u.z, u.w), npy);
+    const float2 dz = __fadd2_rn(make_float2(v.x, v.y), npz);
+    const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
+    float2 inv;
+    inv.x = rsqrtf(r2.x);
+    inv.y = rsqrtf(r2.y);
+    float2 s = __fmul2_rn(make_float2(v.z, v.w), __fmul2_rn(__fmul2_rn(inv, inv), inv));
+    if (EPS0) {
+        if (r2.x == 0.f) s.x = 0.f;
+        if (r2.y == 0.f) s.y = 0.f;
+    }
+    ax = __ffma2_rn(dx, s, ax);
+    ay = __ffma2_rn(dy, s, ay);
+    az = __ffma2_rn(dz, s, az);
+}
+
+// Pairs of the unit's targets with sources src(0..m) for lanes in `mine`. 32 sources at a time are
+// staged in shared memory as 16 interleaved pairs (sources 2j and 2j+1 in one 32-byte record, so
+// that each 16-byte load yields two register pairs); replica r takes pairs r, r + G, ...
 template<bool EPS0, typename Src>
 __device__ __forceinline__ void pair_tile(NearWarp &w, const Lane &L, int m, Src src, bool mine, const float p[3],
                                           float eps, float a[3]) {
     const int lane = threadIdx.x & 31;
+    float *tf = reinterpret_cast<float *>(w.tile);
+    const int slot = (lane >> 1) * 8 + (lane & 1);
+    const float2 npx = make_float2(-p[0], -p[0]), npy = make_float2(-p[1], -p[1]), npz = make_float2(-p[2], -p[2]);
+    const float2 eps2 = make_float2(eps, eps);
+    float2 ax = make_float2(0.f, 0.f), ay = ax, az = ax;
     for (int j0 = 0; j0 < m; j0 += 32) {
         const int c = min(32, m - j0);
-        w.tile[lane] = lane < c ? src(j0 + lane) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 b = lane < c ? src(j0 + lane) : make_float4(0.f, 0.f, 0.f, 0.f);
+        tf[slot] = b.x;
+        tf[slot + 2] = b.y;
+        tf[slot + 4] = b.z;
+        tf[slot + 6] = b.w;
         __syncwarp();
         if (mine) {
-            int k = L.r;
+            const int np = (c + 1) >> 1;
             const int G = L.G;
-            for (; k + 3 * G < c; k += 4 * G) {
-                pair_nog<EPS0>(w.tile[k], p, eps, a);
-                pair_nog<EPS0>(w.tile[k + G], p, eps, a);
-                pair_nog<EPS0>(w.tile[k + 2 * G], p, eps, a);
-                pair_nog<EPS0>(w.tile[k + 3 * G], p, eps, a);
+            int k = L.r;
+            for (; k + G < np; k += 2 * G) {
+                const float4 u0 = w.tile[2 * k], v0 = w.tile[2 * k + 1];
+                const float4 u1 = w.tile[2 * (k + G)], v1 = w.tile[2 * (k + G) + 1];
+                pair2_nog<EPS0>(npx, npy, npz, eps2, u0, v0, ax, ay, az);
+                pair2_nog<EPS0>(npx, npy, npz, eps2, u1, v1, ax, ay, az);
             }
-            for (; k < c; k += G) pair_nog<EPS0>(w.tile[k], p, eps, a);
+            if (k < np) pair2_nog<EPS0>(npx, npy, npz, eps2, w.tile[2 * k], w.tile[2 * k + 1], ax, ay, az);
         }
         __syncwarp();
     }
+    a[0] += ax.x + ax.y;
+    a[1] += ay.x + ay.y;
+    a[2] += az.x + az.y;
 }
 
 // The M2P terms queued per target (by its replica 0), split between the target's replicas.
