@@ -50,7 +50,11 @@ PAIR_FLOPS = 20
 QUAD_NODE_FLOPS = 56
 MONO_NODE_FLOPS = 20
 FP32_FLOP_PER_CLK_PER_SM = 256  # 128 FP32 lanes x FMA
+MUFU_PER_CLK_PER_SM = 16        # rsqrt results per clock per SM (4 per sub-partition)
 NUM_SMS = 148
+# Minimum HBM bytes per body and step of the memory-bound phases (float4 state, 64-bit keys):
+# bbox 16, Morton 28, sort 8 passes x 24 = 192, gather 32, Karras build 40, moments 24, kick-drift 80.
+BODY_STEP_BYTES = 16 + 28 + 192 + 32 + 40 + 24 + 80
 CPU_SAMPLE_TARGETS = 32768
 
 
@@ -362,6 +366,7 @@ def _run_ours_on_stream(args, torch, nb, pm, vel, eps, stream, world, rank, devi
                          "frac": (sort_bytes / (sort_ms / 1000.0) / 1e9) / hbm_peak if sort_ms > 0 and hbm_peak
                          else None, "bytes_per_sort": sort_bytes, "ms_per_sort": sort_ms,
                          "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)"},
+        "body_step_roofline": body_step_roofline(args.n, counts, t_max / args.steps, sm_mhz, hbm_peak),
         "phases_ms_per_step": {k: phases[k] / passes for k in
                                ("bbox_ms", "morton_ms", "sort_ms", "gather_ms", "build_ms", "traverse_ms",
                                 "integrate_ms")},
@@ -375,6 +380,21 @@ def _run_ours_on_stream(args, torch, nb, pm, vel, eps, stream, world, rank, devi
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(pm, eps)
     return line
+
+
+def body_step_roofline(n, counts, step_ms, sm_mhz, hbm_gbs):
+    """Lower bound on one step: the memory-bound phases at the measured copy bandwidth plus the
+    interactions at the slower of the FP32 pipe (flop weights) and the MUFU pipe (one rsqrt each)."""
+    flops = counts["particle_particle"] * PAIR_FLOPS + counts["node_particle"] * QUAD_NODE_FLOPS
+    rsqrt = counts["particle_particle"] + counts["node_particle"]
+    t_mem = BODY_STEP_BYTES * n / ((hbm_gbs or 6650.0) * 1e9)
+    t_fp32 = flops / (NUM_SMS * FP32_FLOP_PER_CLK_PER_SM * sm_mhz * 1e6)
+    t_mufu = rsqrt / (NUM_SMS * MUFU_PER_CLK_PER_SM * sm_mhz * 1e6)
+    t_roof = t_mem + max(t_fp32, t_mufu)
+    return {"t_roofline_ms": t_roof * 1e3, "t_measured_ms": step_ms, "frac": t_roof * 1e3 / step_ms,
+            "memory_ms": t_mem * 1e3, "fp32_ms": t_fp32 * 1e3, "mufu_ms": t_mufu * 1e3,
+            "bytes_per_body": BODY_STEP_BYTES,
+            "peaks": "HBM: MEASURED_PEAKS.json hbm_gbs; FP32 and MUFU: per-SM rates x 148 SMs x measured SM clock"}
 
 
 def energy_diagnostics(nb, device, n=65536, steps=100):
