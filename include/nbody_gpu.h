@@ -181,7 +181,9 @@ int nb_enable_graphs(nb_ctx *ctx, int enable);
  * (recv = the buffers of nb_shard_buffers, rank r's chunk at offset r * chunk; an NCCL in-place
  * all-gather) and calls nb_shard_gathered. Sharded contexts step once per nb_step call;
  * accelerations are valid for the own slice only. Call nb_set_shard before nb_set_bodies, so the
- * buffers get room for world * chunk bodies. Not for batches or the dual-tree solver. */
+ * buffers get room for world * chunk bodies. Not for batches. The dual-tree solver drops every
+ * task whose passive node holds none of the slice's targets, so its far-field and near-field work
+ * both split over the ranks. */
 int nb_shard_range(int64_t n, int32_t rank, int32_t world, int64_t *chunk, int64_t *first, int64_t *count);
 int nb_set_shard(nb_ctx *ctx, int32_t rank, int32_t world);
 /* Current state buffers (Morton slot order, float4 per body; they alternate between passes, so

@@ -383,11 +383,11 @@ int64_t launches_per_pass(const nb_ctx *ctx, bool with_bbox, bool with_drift) {
 // The dual-tree traversal and near field. The near-field pool and the per-block arenas are sized
 // from the body count; when a pass finds them too small (error bits kErrNearPool / kErrDualArena),
 // the host grows them to the sizes the pass asked for and runs the traversal again.
-int dual_traverse(nb_ctx *ctx, int64_t n, cudaStream_t s) {
+int dual_traverse(nb_ctx *ctx, int64_t n, int64_t first, int64_t count, cudaStream_t s) {
     NearPool &np = ctx->dws.near;
     for (int attempt = 0;; ++attempt) {
         launch_dual_traverse(ctx->dnodes, ctx->tw.num_nodes, ctx->pos, n, ctx->cfg.G, ctx->cfg.epsilon,
-                             ctx->cfg.theta, ctx->acc, ctx->counts, ctx->dws, ctx->err, s);
+                             ctx->cfg.theta, ctx->acc, ctx->counts, ctx->dws, ctx->err, s, first, first + count);
         unsigned long long *h = ctx->host_scratch;
         SpillPool &sp = ctx->dws.spill;
         NB_TRY(cudaMemcpyAsync(h, np.counters, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
@@ -523,7 +523,8 @@ int force_pass(nb_ctx *ctx, Marks &mk) {
         launch_build_dual_tree(ctx->keys, ctx->pos, n, ctx->cfg.max_leaf_size, ctx->cfg.theta, ctx->tw, ctx->dnodes,
                                ctx->err, s);
         mk.mark(kTraverse);
-        const int rc = dual_traverse(ctx, n, s);
+        // a sharded context evaluates only its slice of the Morton-ordered targets
+        const int rc = dual_traverse(ctx, n, first, count, s);
         if (rc != NB_OK) return rc;
         ctx->have_tree = true;
         ctx->acc_is_bh = true;
@@ -658,8 +659,8 @@ int nb_set_config(nb_ctx *ctx, const nb_config *cfg) {
     int rc = validate(ctx, cfg);
     if (rc != NB_OK) return rc;
     if (cfg->device != ctx->cfg.device) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "the device cannot change");
-    if (cfg->solver == NB_SOLVER_DUAL_LINEAR_BVH && (ctx->num_inst > 0 || ctx->shard_world > 1))
-        return fail(ctx, NB_ERR_UNSUPPORTED, "the dual-tree solver runs one unsharded instance");
+    if (cfg->solver == NB_SOLVER_DUAL_LINEAR_BVH && ctx->num_inst > 0)
+        return fail(ctx, NB_ERR_UNSUPPORTED, "the dual-tree solver runs one instance (no batches)");
     ctx->cfg = *cfg;
     ctx->have_tree = false;
     drop_graph(ctx);
@@ -1184,8 +1185,6 @@ int nb_set_shard(nb_ctx *ctx, int32_t rank, int32_t world) {
     if (!ctx) return NB_ERR_INVALID_ARGUMENT;
     if (world < 1 || world > 4096 || rank < 0 || rank >= world)
         return fail(ctx, NB_ERR_INVALID_ARGUMENT, "shard rank out of range");
-    if (world > 1 && ctx->cfg.solver == NB_SOLVER_DUAL_LINEAR_BVH)
-        return fail(ctx, NB_ERR_UNSUPPORTED, "the dual-tree solver is not sharded");
     if (world > 1 && ctx->num_inst > 0)
         return fail(ctx, NB_ERR_UNSUPPORTED, "batched instances are not sharded");
     int64_t chunk = 0, first = 0, count = 0;

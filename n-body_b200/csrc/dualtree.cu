@@ -446,7 +446,9 @@ __device__ __forceinline__ void push_task(int *t, int type, int node, int list, 
 
 // FRONTIER = false: one block per start node; tasks of frontier nodes (at most `frontier` bodies,
 // parent above) are spilled. FRONTIER = true: blocks take frontier nodes from the work list and
-// run their spilled tasks, in record order, to completion.
+// run their spilled tasks, in record order, to completion. Only targets in [t_lo, t_hi) are
+// evaluated: a task whose passive node holds none of them is dropped with everything below it,
+// and the tasks that remain run exactly as in an unrestricted pass.
 template<bool FRONTIER>
 __global__ void __launch_bounds__(kThreads) dual_kernel(DualNodes nodes, const int *__restrict__ num_nodes,
                                                         const float4 *__restrict__ bodies, int n, float G,
@@ -455,7 +457,8 @@ __global__ void __launch_bounds__(kThreads) dual_kernel(DualNodes nodes, const i
                                                         const int *__restrict__ roots, const int *__restrict__ num_roots,
                                                         int *__restrict__ arena_all, int arena_words,
                                                         int *__restrict__ tasks_all, NearPool pool, SpillPool spill,
-                                                        int frontier, uint32_t *__restrict__ err) {
+                                                        int frontier, int t_lo, int t_hi,
+                                                        uint32_t *__restrict__ err) {
     __shared__ float s_field[F];
     __shared__ float s_child[2][F];
     __shared__ float s_red[kWarps][F];
@@ -500,6 +503,7 @@ __global__ void __launch_bounds__(kThreads) dual_kernel(DualNodes nodes, const i
             if (tid == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
             continue;
         }
+        if (pend <= t_lo || pfirst >= t_hi) continue;  // no target of this pass below the passive node
         if (tid < F) s_field[tid] = foff >= 0 ? farena[foff + tid] : 0.f;
         __syncthreads();
 
@@ -912,6 +916,7 @@ struct NearWarp {
 struct Lane {
     int t, r, T, G;     // target, replica, targets in the unit, replicas
     bool active;        // r < G
+    bool counted;       // replica 0 of a target of this pass (its interactions are counted)
 };
 
 // Gravity::nodeParticle for MultipoleMassSummary<3> (Gravity.h:239-259) without G, added into a:
@@ -1055,7 +1060,7 @@ __device__ void warp_walk(const Ctx &x, NearWarp &w, const Lane &L, int root, un
         if (ap && L.r == 0) {
             w.priv[plen][L.t] = k;
             ++plen;
-            ++nnp;
+            if (L.counted) ++nnp;
         }
         if (__any_sync(0xffffffffu, plen == kPriv)) {
             __syncwarp();
@@ -1073,7 +1078,7 @@ __device__ void warp_walk(const Ctx &x, NearWarp &w, const Lane &L, int root, un
             const int first = nd.link0;
             pair_tile<EPS0>(w, L, nd.link1 - nd.link0, [&](int j) { return __ldg(x.bodies + first + j); }, mine, p,
                             x.eps, a);
-            if (mine && L.r == 0) npp += (unsigned long long) (nd.link1 - nd.link0);
+            if (mine && L.counted) npp += (unsigned long long) (nd.link1 - nd.link0);
         } else {
             if (!x.left_ok(k) || !x.right_ok(k, nd.link0)) {
                 if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
@@ -1098,7 +1103,7 @@ __global__ void __launch_bounds__(kNearThreads, 4) near_kernel(DualNodes nodes, 
                                                                const float4 *__restrict__ bodies, int n, float G,
                                                                float eps, float theta, float4 *__restrict__ acc,
                                                                unsigned long long *__restrict__ counts, NearPool pool,
-                                                               uint32_t *__restrict__ err) {
+                                                               int t_lo, int t_hi, uint32_t *__restrict__ err) {
     __shared__ NearWarp s_warps[kNearWarps];
     const int lane = threadIdx.x & 31;
     NearWarp &w = s_warps[threadIdx.x >> 5];
@@ -1123,6 +1128,9 @@ __global__ void __launch_bounds__(kNearThreads, 4) near_kernel(DualNodes nodes, 
             if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
             continue;
         }
+        // a unit is evaluated whole (the same replica split as in an unrestricted pass), and only
+        // its targets in [t_lo, t_hi) are written
+        if (tend <= t_lo || unit.y >= t_hi) continue;
         Lane L;
         L.T = tend - unit.y;
         L.G = 32 / L.T;
@@ -1130,6 +1138,7 @@ __global__ void __launch_bounds__(kNearThreads, 4) near_kernel(DualNodes nodes, 
         L.r = lane / L.T;
         L.active = L.r < L.G;
         const int t = unit.y + L.t;
+        L.counted = L.r == 0 && t >= t_lo && t < t_hi;
         const float4 q = __ldg(bodies + t);
         const float p[3] = {q.x, q.y, q.z};
         const unsigned tmask = L.T >= 32 ? 0xffffffffu : ((1u << L.T) - 1u);
@@ -1152,7 +1161,7 @@ __global__ void __launch_bounds__(kNearThreads, 4) near_kernel(DualNodes nodes, 
                         continue;
                     }
                     pair_tile<EPS0>(w, L, len, [&](int j) { return __ldg(bodies + b0 + j); }, L.active, p, eps, a);
-                    if (L.active && L.r == 0) npp += (unsigned long long) len;
+                    if (L.counted) npp += (unsigned long long) len;
                 }
             } else {
                 for (int r = 0; r < item.w; ++r) {
@@ -1170,7 +1179,7 @@ __global__ void __launch_bounds__(kNearThreads, 4) near_kernel(DualNodes nodes, 
         // replicas' partial sums, added in replica order
         w.tile[lane] = make_float4(a[0], a[1], a[2], 0.f);
         __syncwarp();
-        if (L.r == 0) {
+        if (L.r == 0 && t >= t_lo && t < t_hi) {
             float s0 = a[0], s1 = a[1], s2 = a[2];
             for (int r = 1; r < L.G; ++r) {
                 const float4 v = w.tile[r * L.T + L.t];
@@ -1200,8 +1209,9 @@ __global__ void __launch_bounds__(kNearThreads, 4) near_kernel(DualNodes nodes, 
 
 void launch_dual_traverse(const DualNodes &nodes, const int *num_nodes, const float4 *bodies, int64_t n, float G,
                           float eps, float theta, float4 *acc, unsigned long long *counts, DualWorkspace &ws,
-                          uint32_t *err, cudaStream_t s) {
+                          uint32_t *err, cudaStream_t s, int64_t t_lo, int64_t t_hi) {
     if (n <= 0) return;
+    const int lo = (int) std::max<int64_t>(0, std::min(t_lo, n)), hi = (int) std::max<int64_t>(lo, std::min(t_hi, n));
     cudaMemsetAsync(acc, 0, (size_t) n * sizeof(float4), s);
     cudaMemsetAsync(ws.near.head, 0xFF, (size_t) ws.near.head_cap * sizeof(int), s);
     cudaMemsetAsync(ws.near.counters, 0, 4 * sizeof(unsigned long long), s);
@@ -1213,17 +1223,17 @@ void launch_dual_traverse(const DualNodes &nodes, const int *num_nodes, const fl
     const int frontier = (int) std::max<int64_t>(64, n / 4096);
     dual_kernel<false><<<kDualRoots, kThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta, acc,
                                                        counts, ws.roots, ws.num_roots, ws.arena, (int) ws.arena_words,
-                                                       ws.tasks, ws.near, ws.spill, frontier, err);
+                                                       ws.tasks, ws.near, ws.spill, frontier, lo, hi, err);
     dual_kernel<true><<<ws.frontier_blocks, kThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta, acc,
                                                               counts, ws.roots, ws.num_roots, ws.arena,
                                                               (int) ws.arena_words, ws.tasks, ws.near, ws.spill, -1,
-                                                              err);
+                                                              lo, hi, err);
     if (eps == 0.f)
         near_kernel<true><<<ws.near_blocks, kNearThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta,
-                                                                  acc, counts, ws.near, err);
+                                                                  acc, counts, ws.near, lo, hi, err);
     else
         near_kernel<false><<<ws.near_blocks, kNearThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta,
-                                                                   acc, counts, ws.near, err);
+                                                                   acc, counts, ws.near, lo, hi, err);
 }
 
 void dual_near_sizes(int64_t n, int64_t *item_cap, int64_t *word_cap) {

@@ -227,9 +227,11 @@ void dual_near_sizes(int64_t n, int64_t *item_cap, int64_t *word_cap);
 void dual_spill_sizes(int64_t n, int64_t *rec_cap, int64_t *word_cap);
 int dual_near_blocks(int device);
 int dual_frontier_blocks(int device);
+// Accelerations of the targets in [t_lo, t_hi) of the Morton-ordered bodies (all sources act);
+// [0, n) for an unsharded pass.
 void launch_dual_traverse(const DualNodes &nodes, const int *num_nodes, const float4 *bodies, int64_t n, float G,
                           float eps, float theta, float4 *acc, unsigned long long *counts, DualWorkspace &ws,
-                          uint32_t *err, cudaStream_t s);
+                          uint32_t *err, cudaStream_t s, int64_t t_lo, int64_t t_hi);
 
 // traverse.cu
 struct TraverseWorkspace {

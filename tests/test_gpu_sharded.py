@@ -13,27 +13,31 @@ pytestmark = pytest.mark.gpu
 EPS = 1e-4
 
 
-def make(nb, cls, pm, vel, rank=None, world=None):
-    s = cls(rule=nb.Gravity(1.0, EPS), theta=0.5, max_leaf_size=16, time_step=1e-3)
+def make(nb, cls, pm, vel, rank=None, world=None, theta=0.5, leaf=16):
+    s = cls(rule=nb.Gravity(1.0, EPS), theta=theta, max_leaf_size=leaf, time_step=1e-3)
     if world is not None:
         s.set_shard(rank, world)
     s.set_bodies(pm, vel)
     return s
 
 
-@pytest.mark.parametrize("cls_name,n,world", [
-    ("QuadrupoleLinearBVHSolver", 50000, 2),
-    ("LinearBVHSolver", 12345, 3),
-    ("QuadrupoleLinearBVHSolver", 40, 2),
-    ("NaiveSolver", 3000, 2),
+@pytest.mark.parametrize("cls_name,n,world,theta,leaf", [
+    ("QuadrupoleLinearBVHSolver", 50000, 2, 0.5, 16),
+    ("LinearBVHSolver", 12345, 3, 0.5, 16),
+    ("QuadrupoleLinearBVHSolver", 40, 2, 0.5, 16),
+    ("NaiveSolver", 3000, 2, 0.5, 16),
+    # dual tree: tasks of passive nodes outside a rank's slice are dropped, the rest run unchanged
+    ("OctupoleImplicitLinearBVHFMMSolver", 60000, 3, 0.4, 64),
+    ("OctupoleImplicitLinearBVHFMMSolver", 20000, 4, 0.4, 16),
+    ("MultipoleImplicitLinearBVHFMMSolver", 9000, 2, 0.5, 32),
 ])
-def test_emulated_ranks_equal_unsharded(nb, cls_name, n, world):
+def test_emulated_ranks_equal_unsharded(nb, cls_name, n, world, theta, leaf):
     import torch
 
     cls = getattr(nb, cls_name)
     pm, vel = nb.scenarios.plummer(n, seed=5)
-    ref = make(nb, cls, pm, vel)
-    ranks = [make(nb, cls, pm, vel, r, world) for r in range(world)]
+    ref = make(nb, cls, pm, vel, theta=theta, leaf=leaf)
+    ranks = [make(nb, cls, pm, vel, r, world, theta, leaf) for r in range(world)]
     chunk, _, _ = nb.shard_range(n, 0, world)
     try:
         for _ in range(4):
@@ -77,5 +81,26 @@ def test_shard_guards(nb):
         with pytest.raises(nb.NBodyError):
             s.set_shard(2, 2)
     with nb.OctupoleImplicitLinearBVHFMMSolver() as s:
+        s.set_shard(0, 2)  # the dual-tree solver shards over targets as well
         with pytest.raises(nb.NBodyError):
-            s.set_shard(0, 2)
+            s.set_instances([500, 500], pm)
+
+
+def test_dual_shard_counts_add_up(nb):
+    """The ranks' interaction counts: every pair term of the unsharded pass belongs to exactly one
+    target, so the ranks' pair counts add up to it; far-field tasks above the slices run on every
+    rank whose slice they cover, so node-node counts add up to at least the unsharded count."""
+    pm, vel = nb.scenarios.plummer(40000, seed=9)
+    world = 3
+    with make(nb, nb.OctupoleImplicitLinearBVHFMMSolver, pm, vel, theta=0.4, leaf=64) as ref:
+        ref.update_accelerations()
+        c_ref = ref.counts()
+    pp = nn = 0
+    for r in range(world):
+        with make(nb, nb.OctupoleImplicitLinearBVHFMMSolver, pm, vel, r, world, theta=0.4, leaf=64) as s:
+            s.update_accelerations()
+            c = s.counts()
+            pp += c["particle_particle"]
+            nn += c["node_node"]
+    assert pp == c_ref["particle_particle"]
+    assert nn >= c_ref["node_node"]
