@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals per run")
     ap.add_argument("--rate", type=float, default=40.0, help="serving: arrivals per second (open loop)")
     ap.add_argument("--instances", type=int, default=256)
+    ap.add_argument("--emulate-ranks", type=int, default=0,
+                    help="dual-4m: also run each of W target shards' force pass alone on this GPU")
     ap.add_argument("--shard-targets", action="store_true",
                     help="N>1: one instance sharded over the ranks' targets with an NCCL all-gather of "
                          "positions and velocities per step (strong scaling) instead of one instance per rank")
@@ -925,7 +927,8 @@ def run_dual(args):
                      "force_rms_abs": abs_rms, "sample_targets": int(len(idx)),
                      "reference": "FP64 direct sum on GPU"},
         "interactions": counts,
-        "roofline": {"bound": "fp32", "kernel": "dual_kernel (lock-step / passive-tree tasks)",
+        "roofline": {"bound": "fp32",
+                     "kernel": "traversal phase: dual_kernel<0>, dual_kernel<1> (tasks) and near_kernel (near field)",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "flops_per_launch": flops, "ms_per_launch": trav_ms,
                      "peak_source": f"148 SMs x 256 FP32 flop/clk x {sm_mhz:.0f} MHz measured under load"},
@@ -935,10 +938,45 @@ def run_dual(args):
         "gpu_launches": int(phases["launches"]),
         "clocks": clk,
     }
+    if args.emulate_ranks > 1:
+        line["emulated_target_shards"] = dual_shard_emulation(nb, torch, pm, vel, eps, args.emulate_ranks, device,
+                                                              sum(phases[k] for k in phases
+                                                                  if k.endswith("_ms") and k != "integrate_ms")
+                                                              / passes)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = dual_cpu_baseline(1 << 16, eps)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def dual_shard_emulation(nb, torch, pm, vel, eps, world, device, unsharded_ms):
+    """Each of `world` target shards' force pass (nb_set_shard(r, world)) run alone on this GPU,
+    device time per pass. A rank of a real run takes its pass plus the all-gather of its chunk of
+    positions and velocities over NVLink, which this does not include."""
+    n = len(pm)
+    chunk, _, _ = nb.shard_range(n, 0, world)
+    per_rank = []
+    for r in range(world):
+        s = nb.OctupoleImplicitLinearBVHFMMSolver(rule=nb.Gravity(1.0, eps), theta=DUAL_THETA,
+                                                  max_leaf_size=DUAL_LEAF, time_step=DT, device=device)
+        try:
+            s.set_shard(r, world)
+            s.set_bodies(pm, vel)
+            s.update_accelerations_async()  # sizes the pools for this shard
+            s.synchronize()
+            s.enable_timing(True)
+            s.update_accelerations_async()
+            t = s.phase_times()
+            per_rank.append(sum(v for k, v in t.items() if k.endswith("_ms")) / max(t["passes"], 1))
+        finally:
+            s.close()
+        torch.cuda.synchronize(device)
+    worst = max(per_rank)
+    return {"ranks": world, "force_pass_ms_per_rank": per_rank, "max_ms": worst,
+            "unsharded_force_pass_ms": unsharded_ms, "speedup_of_slowest_rank": unsharded_ms / worst,
+            "allgather_bytes_per_rank": 32 * chunk * (world - 1),
+            "method": "each shard's force pass run alone on one GPU (device time, sort and build over all "
+                      "bodies included); the all-gather over NVLink is not included"}
 
 
 def main():
