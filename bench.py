@@ -74,7 +74,7 @@ def parse():
     ap.add_argument("--rate", type=float, default=40.0, help="serving: arrivals per second (open loop)")
     ap.add_argument("--instances", type=int, default=256)
     ap.add_argument("--emulate-ranks", type=int, default=0,
-                    help="dual-4m: also run each of W target shards' force pass alone on this GPU")
+                    help="plummer-1m, dual-4m: also run each of W target shards' force pass alone on this GPU")
     ap.add_argument("--shard-targets", action="store_true",
                     help="N>1: one instance sharded over the ranks' targets with an NCCL all-gather of "
                          "positions and velocities per step (strong scaling) instead of one instance per rank")
@@ -378,6 +378,12 @@ def _run_ours_on_stream(args, torch, nb, pm, vel, eps, stream, world, rank, devi
         "clocks": clk,
     }
     solver.close()
+    if args.emulate_ranks > 1:
+        make = lambda: nb.QuadrupoleLinearBVHSolver(rule=nb.Gravity(1.0, eps), theta=THETA, max_leaf_size=LEAF,
+                                                    time_step=DT, device=device)
+        line["emulated_target_shards"] = shard_emulation(
+            nb, torch, make, pm, vel, args.emulate_ranks, device,
+            sum(phases[k] for k in phases if k.endswith("_ms") and k != "integrate_ms") / passes)
     line["diagnostics"] = energy_diagnostics(nb, device)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(pm, eps)
@@ -939,17 +945,18 @@ def run_dual(args):
         "clocks": clk,
     }
     if args.emulate_ranks > 1:
-        line["emulated_target_shards"] = dual_shard_emulation(nb, torch, pm, vel, eps, args.emulate_ranks, device,
-                                                              sum(phases[k] for k in phases
-                                                                  if k.endswith("_ms") and k != "integrate_ms")
-                                                              / passes)
+        make = lambda: nb.OctupoleImplicitLinearBVHFMMSolver(rule=nb.Gravity(1.0, eps), theta=DUAL_THETA,
+                                                             max_leaf_size=DUAL_LEAF, time_step=DT, device=device)
+        line["emulated_target_shards"] = shard_emulation(
+            nb, torch, make, pm, vel, args.emulate_ranks, device,
+            sum(phases[k] for k in phases if k.endswith("_ms") and k != "integrate_ms") / passes)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = dual_cpu_baseline(1 << 16, eps)
     if rank == 0:
         print(json.dumps(line), flush=True)
 
 
-def dual_shard_emulation(nb, torch, pm, vel, eps, world, device, unsharded_ms):
+def shard_emulation(nb, torch, make, pm, vel, world, device, unsharded_ms):
     """Each of `world` target shards' force pass (nb_set_shard(r, world)) run alone on this GPU,
     device time per pass. A rank of a real run takes its pass plus the all-gather of its chunk of
     positions and velocities over NVLink, which this does not include."""
@@ -957,8 +964,7 @@ def dual_shard_emulation(nb, torch, pm, vel, eps, world, device, unsharded_ms):
     chunk, _, _ = nb.shard_range(n, 0, world)
     per_rank = []
     for r in range(world):
-        s = nb.OctupoleImplicitLinearBVHFMMSolver(rule=nb.Gravity(1.0, eps), theta=DUAL_THETA,
-                                                  max_leaf_size=DUAL_LEAF, time_step=DT, device=device)
+        s = make()
         try:
             s.set_shard(r, world)
             s.set_bodies(pm, vel)
