@@ -10,13 +10,21 @@
 //   - step() keeps the bodies on the device between calls and copies them back once per call;
 //     step(n) runs n steps on the device with a single copy back (the device-resident fast path).
 //   - There is no CPU fallback: constructing a solver without an sm_100 device throws.
+//   - The reference's sigc signals (signal_status, signal_computeTime, signal_finished) are plain
+//     std::function callbacks, and slot_step is stepAsync() on a std::thread.
 #pragma once
 
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
+#include <exception>
+#include <functional>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/nbody_gpu.h"
@@ -119,6 +127,7 @@ public:
     Solver(const Solver &) = delete;
     Solver &operator=(const Solver &) = delete;
     virtual ~Solver() {
+        if (_thread.joinable()) _thread.join();
         if (_ctx) nb_destroy(_ctx);
     }
 
@@ -149,11 +158,58 @@ public:
     }
 
     // Solver::step (Solver.h:103-113): accelerations, then v += a dt and x += v dt.
-    // step(n) runs n steps on the device and copies the bodies back once.
+    // step(n) runs n steps on the device and copies the bodies back once. Status callbacks see
+    // "Starting step" and "Finished step"; the compute-time callback gets the call's wall time
+    // (host copies included), as the reference's on_step reports it (Solver.h:155-185).
     void step(int n = 1) {
+        status("Starting step");
+        const auto t0 = std::chrono::steady_clock::now();
         upload();
         check(nb_step(_ctx, n));
         download();
+        const std::chrono::duration<double> took = std::chrono::steady_clock::now() - t0;
+        status("Finished step");
+        if (_on_compute_time) _on_compute_time(took);
+    }
+
+    // signal_status / signal_computeTime / signal_finished (Solver.h:143-149). Set them before
+    // stepping; with stepAsync they run on the stepping thread.
+    void onStatus(std::function<void(const std::string &)> f) { _on_status = std::move(f); }
+    void onComputeTime(std::function<void(std::chrono::duration<double>)> f) { _on_compute_time = std::move(f); }
+    void onFinished(std::function<void()> f) { _on_finished = std::move(f); }
+
+    // slot_step / on_step (Solver.h:151-185): one step on a background thread. A call while a step
+    // is still running is ignored (returns false), as the reference ignores a second spawn.
+    // wait() joins the thread and rethrows an error the step raised. Do not touch the simulation
+    // while a step runs.
+    bool stepAsync() {
+        std::lock_guard<std::mutex> lock(_thread_mutex);
+        if (_thread.joinable()) {
+            if (_running.load()) return false;
+            _thread.join();
+        }
+        _error = nullptr;
+        _running.store(true);
+        _thread = std::thread([this] {
+            try {
+                step(1);
+            } catch (...) {
+                _error = std::current_exception();
+            }
+            _running.store(false);
+            if (_on_finished) _on_finished();
+        });
+        return true;
+    }
+    bool stepping() const { return _running.load(); }
+    void wait() {
+        std::lock_guard<std::mutex> lock(_thread_mutex);
+        if (_thread.joinable()) _thread.join();
+        if (_error) {
+            std::exception_ptr e = _error;
+            _error = nullptr;
+            std::rethrow_exception(e);
+        }
     }
 
     InteractionCounts counts() const {
@@ -225,12 +281,22 @@ private:
     }
     // Host edits since the last transfer (positions, masses or velocities)
     bool changed() const { return _sim.packedPositionMass() != _shadow_pm || _sim.packedVelocity() != _shadow_v; }
+    void status(const char *what) {
+        if (_on_status) _on_status(what);
+    }
 
     Simulation &_sim;
     Gravity &_rule;
     nb_ctx *_ctx = nullptr;
     std::size_t _uploaded_count = SIZE_MAX;
     std::vector<float> _shadow_pm, _shadow_v;
+    std::function<void(const std::string &)> _on_status;
+    std::function<void(std::chrono::duration<double>)> _on_compute_time;
+    std::function<void()> _on_finished;
+    std::thread _thread;
+    std::mutex _thread_mutex;
+    std::atomic<bool> _running{false};
+    std::exception_ptr _error;
 };
 
 // LinearBVHSolver (LinearBVHSolver.h:18-31): centre-of-mass summaries, "linear-bvh"

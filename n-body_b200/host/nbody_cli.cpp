@@ -3,7 +3,8 @@
 //
 //   nbody_cli [-s|--solver ID] [-i|--iterations N] [-t|--timestep DT] [-G|--gravity G]
 //             [-o|--output-file PATH] [--theta T] [--max-leaf-size L] [--epsilon E]
-//             [--device D] [--counts] [--checkpoint-every K --checkpoint-prefix P] SCENARIO
+//             [--device D] [--counts] [--checkpoint-every K --checkpoint-prefix P] [--verbose]
+//             SCENARIO
 //
 // SCENARIO is a JSON scenario (the reference's schema; a top-level "G" sets the constant, as
 // Application::on_open does) or a tipsy file. The solver ids are the reference's Solver::id()
@@ -11,6 +12,8 @@
 // (JSON out), so I/O needs no GPU. The result is written as a JSON scenario; --counts prints the
 // last force pass's interaction counts as one JSON line on stdout. --checkpoint-every K writes the
 // state every K steps to P.<step>.json (the same schema, so a checkpoint resumes as a scenario).
+// --verbose runs one step at a time on the solver's background thread (stepAsync, the reference's
+// slot_step) and prints each step's compute time, as the reference's computeTime signal reports it.
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
@@ -29,6 +32,7 @@ void usage() {
     std::fprintf(stderr,
                  "usage: nbody_cli [-s ID] [-i N] [-t DT] [-G G] [-o OUT.json] [--theta T] [--max-leaf-size L]\n"
                  "                 [--epsilon E] [--device D] [--counts] [--checkpoint-every K --checkpoint-prefix P]\n"
+                 "                 [--verbose]\n"
                  "                 SCENARIO(.json|tipsy)\n"
                  "solvers:");
     for (auto &id: solverIds()) std::fprintf(stderr, " %s", id.c_str());
@@ -38,7 +42,7 @@ void usage() {
 struct Options {
     std::string solver = "linear-bvh-4p", input, output, checkpoint_prefix;
     int iterations = 0, device = 0, leaf = -1, checkpoint_every = 0;
-    bool has_dt = false, has_G = false, has_theta = false, has_eps = false, counts = false;
+    bool has_dt = false, has_G = false, has_theta = false, has_eps = false, counts = false, verbose = false;
     double dt = 0.0, G = 1.0, theta = 0.0, eps = 0.0;
 };
 
@@ -62,6 +66,7 @@ bool parse(int argc, char **argv, Options &o) {
         else if (a == "--epsilon") { o.eps = std::atof(next()); o.has_eps = true; }
         else if (a == "--device") o.device = std::atoi(next());
         else if (a == "--counts") o.counts = true;
+        else if (a == "--verbose") o.verbose = true;
         else if (a == "--checkpoint-every") o.checkpoint_every = std::atoi(next());
         else if (a == "--checkpoint-prefix") o.checkpoint_prefix = next();
         else if (a == "-h" || a == "--help") return false;
@@ -97,19 +102,28 @@ int main(int argc, char **argv) {
             if (o.leaf > 0) solver->setMaxLeafSize(o.leaf);
             if (o.has_dt) solver->setTimeStep((float) o.dt);
             const float G = rule.g();
-            if (o.checkpoint_every > 0) {
-                // device-resident steps between checkpoints; each checkpoint copies the state out once
-                for (int done = 0; done < o.iterations;) {
-                    const int k = std::min(o.checkpoint_every, o.iterations - done);
+            int done = 0;
+            if (o.verbose)
+                solver->onComputeTime([&](std::chrono::duration<double> d) {
+                    std::fprintf(stderr, "step %d: %.6f s\n", done + 1, d.count());
+                });
+            // device-resident steps between checkpoints; each checkpoint copies the state out once
+            const int chunk = o.verbose ? 1 : (o.checkpoint_every > 0 ? o.checkpoint_every : o.iterations);
+            while (done < o.iterations) {
+                const int k = std::min(chunk, o.iterations - done);
+                if (o.verbose) {
+                    solver->stepAsync();
+                    solver->wait();
+                } else {
                     solver->step(k);
-                    done += k;
+                }
+                done += k;
+                if (o.checkpoint_every > 0 && (done % o.checkpoint_every == 0 || done == o.iterations)) {
                     const std::string path = o.checkpoint_prefix + "." + std::to_string(done) + ".json";
                     std::ofstream out(path);
                     out << scenario_to_json(sim, sc.hasG || o.has_G ? &G : nullptr);
                     if (!out.good()) throw Error(NB_ERR_INVALID_ARGUMENT, "cannot write " + path);
                 }
-            } else {
-                solver->step(o.iterations);
             }
             counts = solver->counts();
             solver_id = solver->id();

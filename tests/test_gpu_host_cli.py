@@ -82,3 +82,22 @@ def test_cli_checkpoint_resume_is_exact(tmp_path, nb, solver_id, theta, leaf):
         assert G == G0 == np.float32(0.75)
         assert np.array_equal(p, p0), path
         assert np.array_equal(v[:, :3], v0[:, :3]), path
+
+
+def test_cli_verbose_steps_on_background_thread(tmp_path, nb):
+    """--verbose steps one at a time through Solver::stepAsync (the reference's slot_step) and
+    prints each step's compute time; the result equals stepping in one call, bit for bit."""
+    pm, vel = nb.scenarios.plummer(4000, seed=29)
+    src = tmp_path / "in.json"
+    nb.scenarios.write_json(str(src), pm, vel)
+    common = ["-s", "linear-bvh-4p", "-i", "4", "-t", "0.001", "--epsilon", "0.0001"]
+    plain, verbose = tmp_path / "plain.json", tmp_path / "verbose.json"
+    run(*common, "-o", str(plain), str(src))
+    r = run(*common, "--verbose", "-o", str(verbose), str(src))
+    lines = [l for l in r.stderr.splitlines() if l.startswith("step ")]
+    assert [l.split(":")[0] for l in lines] == ["step 1", "step 2", "step 3", "step 4"]
+    assert all(float(l.split(":")[1].split()[0]) > 0 for l in lines)
+    p0, v0, _, _ = nb.scenarios.read_json(str(plain))
+    p1, v1, _, _ = nb.scenarios.read_json(str(verbose))
+    assert np.array_equal(p0, p1)
+    assert np.array_equal(v0[:, :3], v1[:, :3])
