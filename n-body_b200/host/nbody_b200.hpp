@@ -14,7 +14,9 @@
 //     std::function callbacks, and slot_step is stepAsync() on a std::thread.
 #pragma once
 
+#include <algorithm>
 #include <atomic>
+#include <cfloat>
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -43,6 +45,26 @@ private:
 struct vec3 {
     float x = 0.f, y = 0.f, z = 0.f;
     friend bool operator==(const vec3 &a, const vec3 &b) { return a.x == b.x && a.y == b.y && a.z == b.z; }
+    friend vec3 operator+(const vec3 &a, const vec3 &b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+    friend vec3 operator-(const vec3 &a, const vec3 &b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+    friend vec3 operator*(const vec3 &a, float s) { return {a.x * s, a.y * s, a.z * s}; }
+    friend vec3 operator/(const vec3 &a, float s) { return {a.x / s, a.y / s, a.z / s}; }
+};
+
+// BoundingBox (src/NBody/Physics/BoundingBox.h:17-72): an empty box is (+max, -max), so the
+// first position extends it to a point.
+struct BoundingBox {
+    vec3 min{FLT_MAX, FLT_MAX, FLT_MAX}, max{-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    vec3 center() const { return (max + min) / 2.0f; }
+    vec3 diagonal() const { return max - min; }
+    float maxSideLength() const {
+        const vec3 d = diagonal();
+        return std::max({d.x, d.y, d.z});
+    }
+    // half-open in every axis, as the reference's contains()
+    bool contains(const vec3 &p) const {
+        return min.x <= p.x && min.y <= p.y && min.z <= p.z && p.x < max.x && p.y < max.y && p.z < max.z;
+    }
 };
 
 // Gravity rule: G and the softening epsilon added to r^2 (Gravity.h:195, 207, 407-409).
@@ -81,6 +103,49 @@ public:
         acceleration.clear();
         mass.clear();
     }
+
+    // Simulation::removeParticle (Simulation.cpp:73-79); the other particles keep their order.
+    void removeParticle(std::size_t i) {
+        if (i >= particleCount()) throw std::out_of_range("no such particle");
+        position.erase(position.begin() + (std::ptrdiff_t) i);
+        velocity.erase(velocity.begin() + (std::ptrdiff_t) i);
+        acceleration.erase(acceleration.begin() + (std::ptrdiff_t) i);
+        mass.erase(mass.begin() + (std::ptrdiff_t) i);
+    }
+
+    // Simulation::averagePosition / totalMass / centerOfMass / interactionCount / boundingBox
+    // (Simulation.cpp:85-132): float sums over the particles in order. Every particle is active
+    // and passive here, so the interaction count is N^2 and all three boxes are the same.
+    vec3 averagePosition() const {
+        vec3 sum;
+        for (const vec3 &p: position) sum = sum + p;
+        return sum / (float) particleCount();
+    }
+    float totalMass() const {
+        float m = 0.f;
+        for (float v: mass) m += v;
+        return m;
+    }
+    vec3 centerOfMass() const {
+        vec3 sum;
+        float m = 0.f;
+        for (std::size_t i = 0; i < particleCount(); ++i) {
+            sum = sum + position[i] * mass[i];
+            m += mass[i];
+        }
+        return sum / m;
+    }
+    std::size_t interactionCount() const { return particleCount() * particleCount(); }
+    BoundingBox boundingBox() const {
+        BoundingBox b;
+        for (const vec3 &p: position) {
+            b.min = {std::min(b.min.x, p.x), std::min(b.min.y, p.y), std::min(b.min.z, p.z)};
+            b.max = {std::max(b.max.x, p.x), std::max(b.max.y, p.y), std::max(b.max.z, p.z)};
+        }
+        return b;
+    }
+    BoundingBox activeBoundingBox() const { return boundingBox(); }
+    BoundingBox passiveBoundingBox() const { return boundingBox(); }
 
     // 4 floats per body, as the C ABI takes them
     std::vector<float> packedPositionMass() const {

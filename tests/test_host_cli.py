@@ -181,3 +181,47 @@ def test_reads_reference_scenario_files(tmp_path, nb, name):
             assert vel[i, :3].tolist() == [np.float32(p["velocity"][c]) for c in "xyz"]
         assert pm[i, 3] == np.float32(p.get("mass", 0.0))
     assert (G is None) == ("G" not in root)
+
+
+HOST_PROGRAM = r"""
+#include "nbody_b200.hpp"
+#include <cstdio>
+int main() {
+    nbody_b200::Simulation s;
+    s.newParticle({1, 2, 3}, {0, 0, 0}, 2.f);
+    s.newParticle({-1, 0, 5}, {0, 0, 0}, 1.f);
+    s.newParticle({4, -2, 1}, {1, 0, 0}, 1.f);
+    const auto c = s.centerOfMass(), a = s.averagePosition();
+    const auto b = s.boundingBox();
+    std::printf("%.9g %.9g %.9g\n%.9g %.9g %.9g\n", c.x, c.y, c.z, a.x, a.y, a.z);
+    std::printf("%.9g %.9g %.9g %.9g %.9g %.9g\n", b.min.x, b.min.y, b.min.z, b.max.x, b.max.y, b.max.z);
+    std::printf("%.9g %zu %d %d\n", s.totalMass(), s.interactionCount(), (int) b.contains({0, 0, 3}),
+                (int) b.contains(b.max));
+    s.removeParticle(0);
+    std::printf("%zu %.9g %.9g\n", s.particleCount(), s.position[0].x, s.mass[1]);
+    nbody_b200::BoundingBox empty;
+    std::printf("%d\n", (int) (empty.min.x > empty.max.x));
+}
+"""
+
+
+def test_simulation_helpers(tmp_path):
+    """Simulation's host-side summaries (averagePosition, totalMass, centerOfMass, boundingBox,
+    interactionCount, removeParticle) as the reference defines them (Simulation.cpp:73-132)."""
+    src = tmp_path / "sim.cpp"
+    src.write_text(HOST_PROGRAM)
+    exe = tmp_path / "sim"
+    subprocess.run(["g++", "-std=c++20", "-I", os.path.join(REPO, "n-body_b200", "host"), "-o", str(exe), str(src)],
+                   check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    f32 = np.float32
+    pos = np.array([[1, 2, 3], [-1, 0, 5], [4, -2, 1]], f32)
+    m = np.array([2, 1, 1], f32)
+    com = ((pos[0] * m[0] + pos[1] * m[1]) + pos[2] * m[2]) / ((m[0] + m[1]) + m[2])
+    avg = ((pos[0] + pos[1]) + pos[2]) / f32(3)
+    assert [f32(v) for v in out[0].split()] == list(com)
+    assert [f32(v) for v in out[1].split()] == list(avg)
+    assert [float(v) for v in out[2].split()] == [-1, -2, 1, 4, 2, 5]
+    assert out[3].split() == ["4", "9", "1", "0"]  # the box is half-open: its max corner is outside
+    assert out[4].split() == ["2", "-1", "1"]
+    assert out[5] == "1"
