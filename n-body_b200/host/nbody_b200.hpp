@@ -212,6 +212,10 @@ public:
 
     Simulation &simulation() { return _sim; }
     Gravity &rule() { return _rule; }
+    // Solver::maxThreadCount (Solver.h:38, 97-99) caps the reference's TBB workers. The device path
+    // has no host worker pool, so the value is kept for source compatibility and not used.
+    std::size_t &maxThreadCount() { return _max_threads; }
+    const std::size_t &maxThreadCount() const { return _max_threads; }
 
     // Solver::updateAccelerations (ActiveTreeSolver.h:33-72 / ImplicitDualTraversalSolver.h:42-69):
     // accelerations of the simulation's current bodies, written to simulation().acceleration.
@@ -362,6 +366,7 @@ private:
     std::mutex _thread_mutex;
     std::atomic<bool> _running{false};
     std::exception_ptr _error;
+    std::size_t _max_threads = std::thread::hardware_concurrency();
 };
 
 // LinearBVHSolver (LinearBVHSolver.h:18-31): centre-of-mass summaries, "linear-bvh"
