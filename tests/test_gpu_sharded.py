@@ -30,6 +30,7 @@ def make(nb, cls, pm, vel, rank=None, world=None, theta=0.5, leaf=16):
     ("OctupoleImplicitLinearBVHFMMSolver", 60000, 3, 0.4, 64),
     ("OctupoleImplicitLinearBVHFMMSolver", 20000, 4, 0.4, 16),
     ("MultipoleImplicitLinearBVHFMMSolver", 9000, 2, 0.5, 32),
+    ("OctupoleImplicitLinearBVHFMMSolver", 70, 4, 0.4, 16),  # chunks of 32: rank 3 holds no target
 ])
 def test_emulated_ranks_equal_unsharded(nb, cls_name, n, world, theta, leaf):
     import torch
