@@ -925,7 +925,7 @@ struct Lane {
 //   (D3 : Q2)_i = g3 R_i (R.Q2.R) + g2 (2 (Q2 R)_i + R_i tr Q2)
 //   (D4 : Q3)_i = g4 R_i (Q3 : RRR) + 3 g3 ((Q3 : RR)_i + R_i (t.R)) + 3 g2 t_i,  t_i = Q3_ikk,
 // which is the same sum over index tuples, grouped (about 100 flops instead of about 550).
-__device__ __noinline__ void m2p_nog(const Ctx &x, int k, const float p[3], float a[3]) {
+__device__ __forceinline__ void m2p_nog(const Ctx &x, int k, const float p[3], float a[3]) {
     const float4 c4 = __ldg(x.nodes.com + k);
     const float rx = p[0] - c4.x, ry = p[1] - c4.y, rz = p[2] - c4.z;
     if (rx == 0.f && ry == 0.f && rz == 0.f) return;
