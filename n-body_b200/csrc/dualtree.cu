@@ -805,6 +805,8 @@ __global__ void __launch_bounds__(kThreads) dual_kernel(DualNodes nodes, const i
                 }
                 __syncthreads();
                 run_tasks();
+                // every thread has read the empty task count before thread 0 sets up the next record
+                __syncthreads();
                 r = rec.x;
             }
         }
