@@ -449,8 +449,10 @@ __device__ __forceinline__ void push_task(int *t, int type, int node, int list, 
 // run their spilled tasks, in record order, to completion. Only targets in [t_lo, t_hi) are
 // evaluated: a task whose passive node holds none of them is dropped with everything below it,
 // and the tasks that remain run exactly as in an unrestricted pass.
+// Four blocks per SM (64 registers; the per-thread field accumulators spill a little): the task
+// loop is latency- and barrier-bound, so resident blocks matter more than the spills.
 template<bool FRONTIER>
-__global__ void __launch_bounds__(kThreads) dual_kernel(DualNodes nodes, const int *__restrict__ num_nodes,
+__global__ void __launch_bounds__(kThreads, 4) dual_kernel(DualNodes nodes, const int *__restrict__ num_nodes,
                                                         const float4 *__restrict__ bodies, int n, float G,
                                                         float eps, float theta, float4 *__restrict__ acc,
                                                         unsigned long long *__restrict__ counts,
@@ -1263,9 +1265,11 @@ int dual_near_blocks(int device) {
 }
 
 int64_t dual_arena_words(int64_t n) {
-    // lists along one root-to-leaf path of the passive tree; grows with the body count
+    // lists along one root-to-leaf path of the passive tree; grows with the body count. The largest
+    // use measured on two 2^21-body Hernquist spheres at theta 0.4 is 1.5 Mi words (a start-node
+    // block); a pass that runs out doubles the arenas and runs again.
     const int64_t w = 64 * n + (int64_t(1) << 16);
-    return std::min<int64_t>(std::max<int64_t>(w, int64_t(1) << 16), int64_t(1) << 23);
+    return std::min<int64_t>(std::max<int64_t>(w, int64_t(1) << 16), int64_t(1) << 22);
 }
 
 }  // namespace nbg
