@@ -73,6 +73,9 @@ def parse():
     ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals per run")
     ap.add_argument("--rate", type=float, default=40.0, help="serving: arrivals per second (open loop)")
     ap.add_argument("--instances", type=int, default=256)
+    ap.add_argument("--fp64-summaries", type=int, default=None,
+                    help="internal nodes with at least this many bodies combine their moments in FP64 "
+                         "(default: 65536 for dual-4m, as its configuration asks; off elsewhere)")
     ap.add_argument("--emulate-ranks", type=int, default=0,
                     help="plummer-1m, dual-4m: also run each of W target shards' force pass alone on this GPU")
     ap.add_argument("--shard-targets", action="store_true",
@@ -817,6 +820,9 @@ DUAL_HALF = 1 << 21
 DUAL_THETA = 0.4
 DUAL_LEAF = 64           # LinearBVH's default maxLeafSize (LinearBVH.h:88)
 DUAL_SOFTENING = 0.005
+# FP64 combination of the moments of nodes with at least this many bodies (the top levels: about
+# 6 of them at 2 x 2^21 bodies); the configuration asks for FP64 root-level moments
+DUAL_FP64_SUMMARIES = 65536
 # Flop weights of the dual-tree interactions, counted from n-body_b200/csrc/dualtree.cu and
 # stensor.cuh after unrolling (FMA = 2): pair 20; M2P with octupole moments (the two contractions
 # grouped for symmetric moments) 125; P2L into an order-4 field (D2..D4) 440; M2L (D2..D4, three
@@ -879,9 +885,9 @@ def run_dual(args):
                                                   theta=DUAL_THETA, max_leaf_size=DUAL_LEAF, time_step=DT,
                                                   device=device)
         s.set_stream(stream.cuda_stream)
-        # accuracy of the first force pass vs FP64 direct summation
-        acc = s.update_accelerations()
-        counts = s.counts()
+        fp64_min = DUAL_FP64_SUMMARIES if args.fp64_summaries is None else args.fp64_summaries
+        # accuracy of the first force pass vs FP64 direct summation, with the FP32 top-level
+        # summaries of the reference for comparison
         rng = np.random.default_rng(65536)
         idx = np.sort(rng.choice(n, min(65536, n), replace=False))
         dpm = torch.from_numpy(pm).to(device)
@@ -890,10 +896,17 @@ def run_dual(args):
         s.direct_device(n, dpm.data_ptr(), len(idx), dt_.data_ptr(), out.data_ptr(), 64)
         s.synchronize()
         ref = out.cpu().numpy()
+        del dpm, dt_, out
+        rel32 = None
+        if fp64_min > 0:
+            got32 = s.update_accelerations()[idx, :3].astype(np.float64)
+            rel32 = np.linalg.norm(got32 - ref, axis=1) / np.linalg.norm(ref, axis=1)
+        s.set_fp64_summaries(fp64_min)
+        acc = s.update_accelerations()
+        counts = s.counts()
         got = acc[idx, :3].astype(np.float64)
         rel = np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)
         abs_rms = float(np.sqrt(np.mean(np.sum((got - ref) ** 2, axis=1))))
-        del dpm, dt_, out
         for _ in range(max(args.warmup, 3)):
             flush.zero_()
             s.step(1)
@@ -928,10 +941,14 @@ def run_dual(args):
         "dtype": "f32", "data": "synthetic (seeded Hernquist spheres)",
         "config": {"workload": f"dual-hernquist-2x{half}-octupole", "n_bodies": n, "theta": DUAL_THETA,
                    "leaf_size": DUAL_LEAF, "softening": DUAL_SOFTENING, "dt": DT,
-                   "solver": "implicit-linear-bvh-fmm-8p", "l2": "flushed (256 MB write) before every timed step"},
+                   "solver": "implicit-linear-bvh-fmm-8p", "l2": "flushed (256 MB write) before every timed step",
+                   "summaries": f"FP32, FP64 combination for nodes of at least {fp64_min} bodies" if fp64_min
+                   else "FP32 (the reference's operations)"},
         "accuracy": {"force_rms_rel": float(np.sqrt(np.mean(rel ** 2))), "force_max_rel": float(rel.max()),
                      "force_rms_abs": abs_rms, "sample_targets": int(len(idx)),
-                     "reference": "FP64 direct sum on GPU"},
+                     "reference": "FP64 direct sum on GPU",
+                     "fp64_summaries_min_bodies": fp64_min,
+                     "force_rms_rel_fp32_summaries": None if rel32 is None else float(np.sqrt(np.mean(rel32 ** 2)))},
         "interactions": counts,
         "roofline": {"bound": "fp32",
                      "kernel": "traversal phase: dual_kernel<0>, dual_kernel<1> (tasks) and near_kernel (near field)",

@@ -172,6 +172,13 @@ int nb_get_instance_roots(nb_ctx *ctx, int32_t *roots);
  * timing, when enabled, runs the steps uncaptured). */
 int nb_enable_graphs(nb_ctx *ctx, int enable);
 
+/* Precision option, off by default (min_bodies = 0): internal tree nodes of at least min_bodies
+ * bodies combine their children's centre of mass and moments in FP64 and round once to FP32
+ * (MultipoleMassSummary.h:37-97 evaluated in double). Bounding boxes, and therefore every
+ * approximation decision and interaction count, are unchanged; with the option on, the summaries
+ * of those nodes are no longer bit-identical to the reference's FP32 ones. */
+int nb_set_fp64_summaries(nb_ctx *ctx, int64_t min_bodies);
+
 /* Target sharding of one instance over `world` processes, one GPU each (the path shards over
  * targets; every rank needs all sources). Every rank holds the same state.
  * A force pass still sorts and builds over all bodies, but evaluates accelerations, and nb_step

@@ -1174,6 +1174,15 @@ int nb_enable_graphs(nb_ctx *ctx, int enable) {
     return NB_OK;
 }
 
+int nb_set_fp64_summaries(nb_ctx *ctx, int64_t min_bodies) {
+    if (!ctx) return NB_ERR_INVALID_ARGUMENT;
+    if (min_bodies < 0) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "negative body count");
+    ctx->tw.fp64_min_bodies = (int) std::min<int64_t>(min_bodies, INT32_MAX);
+    ctx->have_tree = false;
+    drop_graph(ctx);  // captured builds hold the old setting
+    return NB_OK;
+}
+
 int nb_shard_range(int64_t n, int32_t rank, int32_t world, int64_t *chunk, int64_t *first, int64_t *count) {
     if (n < 0 || world < 1 || rank < 0 || rank >= world || !chunk || !first || !count)
         return NB_ERR_INVALID_ARGUMENT;

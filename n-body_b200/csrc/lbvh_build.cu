@@ -278,6 +278,58 @@ __device__ Summ<ORDER> internal_summary(const Summ<ORDER> &a, const Summ<ORDER> 
     return s;
 }
 
+// internal_summary's formulas (MultipoleMassSummary.h:37-97) evaluated in FP64 from the children's
+// FP32 summaries and rounded once: the precision option for the top levels of the tree. The
+// bounding box is exact in any precision (min / max do not round).
+template<int ORDER>
+__device__ Summ<ORDER> internal_summary_f64(const Summ<ORDER> &a, const Summ<ORDER> &b) {
+    Summ<ORDER> s;
+    const double M = (double) a.M + (double) b.M;
+    double c[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) c[k] = ((double) a.com[k] * (double) a.M + (double) b.com[k] * (double) b.M) / M;
+    s.M = (float) M;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) s.com[k] = (float) c[k];
+    if constexpr (ORDER >= 2) {
+        double q2[6] = {0, 0, 0, 0, 0, 0}, q3[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+        const Summ<ORDER> *cs[2] = {&a, &b};
+#pragma unroll
+        for (int ci = 0; ci < 2; ++ci) {
+            const Summ<ORDER> &ch = *cs[ci];
+            const double m = ch.M;
+            const double d[3] = {(double) ch.com[0] - c[0], (double) ch.com[1] - c[1], (double) ch.com[2] - c[2]};
+            const double t2[6] = {d[0] * d[0], d[0] * d[1], d[0] * d[2], d[1] * d[1], d[1] * d[2], d[2] * d[2]};
+#pragma unroll
+            for (int k = 0; k < 6; ++k) q2[k] += t2[k] * m + (double) ch.q[k];
+            if constexpr (ORDER >= 3) {
+#pragma unroll
+                for (int L = 0; L < 10; ++L) {
+                    int i[3];
+                    dims3(L, i);
+                    // (d (x) d (x) d) m + child octupole + sumOfOuterProducts(child quadrupole, d)
+                    const double sop = (double) ch.q[slot2u(i[0], i[1])] * d[i[2]] +
+                                       (double) ch.q[slot2u(i[1], i[2])] * d[i[0]] +
+                                       (double) ch.q[slot2u(i[2], i[0])] * d[i[1]];
+                    q3[L] += t2[slot2(i[0], i[1])] * d[i[2]] * m + (double) ch.q3[L] + sop;
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) s.q[k] = (float) q2[k];
+        if constexpr (ORDER >= 3) {
+#pragma unroll
+            for (int k = 0; k < 10; ++k) s.q3[k] = (float) q3[k];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        s.bmin[k] = gmin(b.bmin[k], gmin(a.bmin[k], FLT_MAX));
+        s.bmax[k] = gmax(b.bmax[k], gmax(a.bmax[k], -FLT_MAX));
+    }
+    return s;
+}
+
 __device__ __forceinline__ bool is_final_leaf(const uint8_t *splittable, int c) { return c < 0 || !splittable[c]; }
 __device__ __forceinline__ int slot_of(int c, int n) { return c >= 0 ? c : (n - 1) + ~c; }
 
@@ -304,7 +356,11 @@ __global__ void __launch_bounds__(kThreads) summarize_kernel(const float4 *__res
             if (atomicAdd(&tw.visit[p], 1) == 0) break;  // the sibling's thread finishes p
             __threadfence();
             const int sl = slot_of(tw.left[p], n), sr = slot_of(tw.right[p], n);
-            store_slot<ORDER>(tw, p, internal_summary<ORDER>(load_slot<ORDER>(tw, sl), load_slot<ORDER>(tw, sr)));
+            const int2 rg = tw.range[p];
+            if (tw.fp64_min_bodies > 0 && rg.y - rg.x + 1 >= tw.fp64_min_bodies)
+                store_slot<ORDER>(tw, p, internal_summary_f64<ORDER>(load_slot<ORDER>(tw, sl), load_slot<ORDER>(tw, sr)));
+            else
+                store_slot<ORDER>(tw, p, internal_summary<ORDER>(load_slot<ORDER>(tw, sl), load_slot<ORDER>(tw, sr)));
             tw.cnt[p] = 1 + __ldcg(tw.cnt + sl) + __ldcg(tw.cnt + sr);
             if (p == 0) break;
             p = tw.parent[p];

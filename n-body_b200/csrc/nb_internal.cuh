@@ -165,6 +165,9 @@ struct TreeWorkspace {
     int *cnt = nullptr;             // subtree node count per slot
     int *num_nodes = nullptr;       // device scalar: final node count
     int64_t capacity = 0;
+    // Precision option (0: off, the reference's FP32 operations everywhere): internal nodes of at
+    // least this many bodies combine their children's summaries in FP64, rounded once to FP32.
+    int fp64_min_bodies = 0;
 };
 void launch_build_tree(const uint64_t *sorted_codes, const float4 *bodies, int64_t n, int leaf, int order, float theta,
                        TreeWorkspace &tw, const NodeArrays &nodes, uint32_t *err, cudaStream_t s,

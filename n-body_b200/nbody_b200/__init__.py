@@ -139,6 +139,7 @@ SIGNATURES = {
     "nb_instance_count": (_i32, [_vp]),
     "nb_get_instance_roots": (C.c_int, [_vp, _vp]),
     "nb_enable_graphs": (C.c_int, [_vp, C.c_int]),
+    "nb_set_fp64_summaries": (C.c_int, [_vp, C.c_int64]),
     "nb_server_create": (C.c_int, [C.POINTER(Config), C.c_uint64, C.POINTER(_vp)]),
     "nb_server_destroy": (C.c_int, [_vp]),
     "nb_server_last_error": (C.c_char_p, [_vp]),
@@ -346,6 +347,11 @@ class Solver:
 
     def enable_graphs(self, on: bool = True):
         self._check(lib().nb_enable_graphs(self._ctx, int(on)))
+
+    def set_fp64_summaries(self, min_bodies: int):
+        """Combine the summaries of internal nodes with at least `min_bodies` bodies in FP64
+        (nb_set_fp64_summaries; 0 turns it off)."""
+        self._check(lib().nb_set_fp64_summaries(self._ctx, int(min_bodies)))
 
     def body_count(self) -> int:
         return int(lib().nb_body_count(self._ctx))

@@ -320,3 +320,29 @@ def test_config_c1_ten_steps(nb, oracle):
         p, v = oracle.kick_drift(p, v, a, np.float32(1e-3))
     assert np.abs(gpm[:, :3] - p[:, :3]).max() < 1e-5 * np.abs(p[:, :3]).max()
     assert np.abs(gvel[:, :3] - v[:, :3]).max() < 1e-4 * np.abs(v[:, :3]).max()
+
+
+@pytest.mark.parametrize("cls_name,n,theta,leaf", [
+    ("QuadrupoleLinearBVHSolver", 20000, 0.5, 16),
+    ("LinearBVHSolver", 9000, 0.5, 16),
+    ("OctupoleImplicitLinearBVHFMMSolver", 30000, 0.4, 64),
+])
+def test_fp64_top_level_summaries(nb, cls_name, n, theta, leaf):
+    """The precision option (nb_set_fp64_summaries): bounding boxes and so every decision and
+    interaction count stay the reference's; the FP64-combined moments move the accelerations by
+    rounding only, and turning the option off restores the FP32 results bit for bit."""
+    pm, _ = nb.scenarios.plummer(n, seed=31)
+    eps = 1e-4
+    with getattr(nb, cls_name)(bodies=pm, rule=nb.Gravity(1.0, eps), theta=theta, max_leaf_size=leaf) as s:
+        a32 = s.update_accelerations()[:, :3].astype(np.float64)
+        c32 = s.counts()
+        s.set_fp64_summaries(1)
+        a64 = s.update_accelerations()[:, :3].astype(np.float64)
+        c64 = s.counts()
+        s.set_fp64_summaries(0)
+        again = s.update_accelerations()[:, :3].astype(np.float64)
+    assert c64 == c32
+    assert np.array_equal(again, a32)
+    rel = np.linalg.norm(a64 - a32, axis=1) / np.linalg.norm(a32, axis=1)
+    assert np.sqrt(np.mean(rel ** 2)) < 1e-5
+    assert not np.array_equal(a64, a32)  # the option does change the top-level moments
