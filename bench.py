@@ -166,8 +166,14 @@ def accuracy(nb, solver, pm, eps, torch, device):
     rel = diff / mag
     m = pm[idx, 3].astype(np.float64)
     f_rms = np.sqrt(np.mean((mag * m) ** 2))
+    # the same pass with the top levels' moments combined in FP64 (the precision option), then back
+    solver.set_fp64_summaries(65536)
+    got64 = solver.update_accelerations()[idx, :3].astype(np.float64)
+    solver.set_fp64_summaries(0)
+    rel64 = np.linalg.norm(got64 - ref, axis=1) / mag
     return {
         "force_rms_rel": float(np.sqrt(np.mean(rel ** 2))),
+        "force_rms_rel_fp64_top_summaries": float(np.sqrt(np.mean(rel64 ** 2))),
         "force_max_rel": float(rel.max()),
         "rms_grader_pct": float(np.sqrt((rel ** 2).max()) * 100.0),
         "constitutional_pct": float(np.max(100.0 * diff * m / np.minimum(mag * m, f_rms))),
