@@ -2,8 +2,9 @@
 // theta) laid out back to back in one body array and advanced by one launch per phase.
 //
 // Per force pass:
-//   seg_bbox_kernel      one block per instance: exact FP32 min/max of its positions
-//                        (outerBoundingBox, SummaryType.h:73-81, per instance)
+//   seg_bbox_kernel      slices of up to 8192 bodies of each instance: exact FP32 min/max of its
+//                        positions (outerBoundingBox, SummaryType.h:73-81, per instance),
+//                        combined with order-preserving integer atomics as bbox_reduce does
 //   seg_morton_kernel    Morton code of every body in its instance's box (MortonSort.h:46-73) and
 //                        the eight digit histograms of all codes
 //   8 one-sweep passes   over all codes (radix_sort.cu), then 1-2 stable passes on the instance id
@@ -24,14 +25,20 @@ namespace {
 
 constexpr int kThreads = 256;
 
+// Block (k, j) reduces slice j of `slices` of instance k. inst_box holds 6 ordered uints per
+// instance (min.xyz, then ~max.xyz; see float_to_ordered), all reduced with atomicMin from all
+// ones, so the result does not depend on the order of the slices.
 __global__ void __launch_bounds__(kThreads) seg_bbox_kernel(const float4 *__restrict__ pos,
-                                                            const int2 *__restrict__ inst_range,
-                                                            float *__restrict__ inst_box) {
-    const int k = blockIdx.x;
+                                                            const int2 *__restrict__ inst_range, int slices,
+                                                            uint32_t *__restrict__ inst_box) {
+    const int k = blockIdx.x / slices, j = blockIdx.x - k * slices;
     const int2 r = inst_range[k];
+    const int64_t len = (int64_t) r.y - r.x + 1;
+    const int lo = r.x + (int) (len * j / slices), hi = r.x + (int) (len * (j + 1) / slices);
+    if (lo >= hi) return;  // uniform across the block
     float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
     float mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
-    for (int i = r.x + threadIdx.x; i <= r.y; i += blockDim.x) {
+    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
         const float4 p = __ldg(pos + i);
         mn[0] = gmin(mn[0], p.x); mn[1] = gmin(mn[1], p.y); mn[2] = gmin(mn[2], p.z);
         mx[0] = gmax(mx[0], p.x); mx[1] = gmax(mx[1], p.y); mx[2] = gmax(mx[2], p.z);
@@ -55,14 +62,14 @@ __global__ void __launch_bounds__(kThreads) seg_bbox_kernel(const float4 *__rest
         const int c = threadIdx.x;
         float a = smn[c][0], b = smx[c][0];
         for (int w = 1; w < kThreads / 32; ++w) { a = gmin(a, smn[c][w]); b = gmax(b, smx[c][w]); }
-        inst_box[6 * k + c] = a;
-        inst_box[6 * k + 3 + c] = b;
+        atomicMin(&inst_box[6 * k + c], float_to_ordered(a));
+        atomicMin(&inst_box[6 * k + 3 + c], ~float_to_ordered(b));
     }
 }
 
 __global__ void __launch_bounds__(kThreads) seg_morton_kernel(const float4 *__restrict__ pos, int64_t n,
                                                               const int *__restrict__ inst_of,
-                                                              const float *__restrict__ inst_box,
+                                                              const uint32_t *__restrict__ inst_box,
                                                               uint64_t *__restrict__ codes,
                                                               uint32_t *__restrict__ hist) {
     __shared__ uint32_t sh[8 * 256];
@@ -70,7 +77,9 @@ __global__ void __launch_bounds__(kThreads) seg_morton_kernel(const float4 *__re
     __syncthreads();
     const int64_t stride = (int64_t) gridDim.x * blockDim.x;
     for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const float *b = inst_box + 6 * inst_of[i];
+        const uint32_t *ob = inst_box + 6 * inst_of[i];
+        const float b[6] = {ordered_to_float(ob[0]), ordered_to_float(ob[1]), ordered_to_float(ob[2]),
+                            ordered_to_float(~ob[3]), ordered_to_float(~ob[4]), ordered_to_float(~ob[5])};
         const float mn[3] = {b[0], b[1], b[2]};
         const float dx = fsub(b[3], b[0]), dy = fsub(b[4], b[1]), dz = fsub(b[5], b[2]);
         const float scale = gmax(gmax(dx, dy), dz);
@@ -135,12 +144,15 @@ void launch_fill_tables(const int2 *inst_range, const int *group_first, int num_
     fill_tables_kernel<<<num_inst, kThreads, 0, s>>>(inst_range, group_first, inst_of, groups);
 }
 
-void launch_seg_bbox(const float4 *pos, const int2 *inst_range, int num_inst, float *inst_box, cudaStream_t s) {
+void launch_seg_bbox(const float4 *pos, const int2 *inst_range, int num_inst, int slices, uint32_t *inst_box,
+                     cudaStream_t s) {
     if (num_inst <= 0) return;
-    seg_bbox_kernel<<<num_inst, kThreads, 0, s>>>(pos, inst_range, inst_box);
+    slices = slices < 1 ? 1 : slices;
+    cudaMemsetAsync(inst_box, 0xFF, (size_t) num_inst * 6 * sizeof(uint32_t), s);
+    seg_bbox_kernel<<<(unsigned) ((int64_t) num_inst * slices), kThreads, 0, s>>>(pos, inst_range, slices, inst_box);
 }
 
-void launch_seg_morton(const float4 *pos, int64_t n, const int *inst_of, const float *inst_box, uint64_t *codes,
+void launch_seg_morton(const float4 *pos, int64_t n, const int *inst_of, const uint32_t *inst_box, uint64_t *codes,
                        uint32_t *hist, cudaStream_t s) {
     if (n <= 0) return;
     cudaMemsetAsync(hist, 0, 8 * 256 * sizeof(uint32_t), s);

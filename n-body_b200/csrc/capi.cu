@@ -74,7 +74,9 @@ struct nb_ctx {
     int32_t num_inst = 0;
     std::vector<int64_t> inst_start, inst_size;
     int *inst_of = nullptr, *inst_root = nullptr;
-    float *inst_theta2 = nullptr, *inst_box = nullptr;
+    float *inst_theta2 = nullptr;
+    uint32_t *inst_box = nullptr;  // 6 order-preserving uints per instance (min.xyz, ~max.xyz)
+    int inst_bbox_slices = 1;      // blocks per instance of the box reduction
     int2 *inst_range = nullptr;
     int4 *groups = nullptr;
     int64_t ngroups = 0;
@@ -441,7 +443,7 @@ int dual_traverse(nb_ctx *ctx, int64_t n, int64_t first, int64_t count, cudaStre
 int force_pass_batch(nb_ctx *ctx, Marks &mk) {
     const int64_t n = ctx->n;
     cudaStream_t s = ctx->stream;
-    launch_seg_bbox(ctx->pos, ctx->inst_range, ctx->num_inst, ctx->inst_box, s);
+    launch_seg_bbox(ctx->pos, ctx->inst_range, ctx->num_inst, ctx->inst_bbox_slices, ctx->inst_box, s);
     mk.mark(kMorton);
     launch_seg_morton(ctx->pos, n, ctx->inst_of, ctx->inst_box, ctx->keys, ctx->sw.hist, s);
     mk.mark(kSort);
@@ -1059,6 +1061,8 @@ static int build_batch_tables(nb_ctx *ctx, int32_t count, const int64_t *sizes, 
         hist[256 + (k >> 8)] += (uint32_t) sizes[k];
         start += sizes[k];
     }
+    const int64_t largest = count > 0 ? *std::max_element(sizes, sizes + count) : 1;
+    ctx->inst_bbox_slices = (int) std::min<int64_t>(std::max<int64_t>((largest + 8191) / 8192, 1), 64);
     const int passes = count > 256 ? 2 : 1;
     for (int p = 0; p < passes; ++p) {
         uint32_t acc = 0;

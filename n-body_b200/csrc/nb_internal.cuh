@@ -274,8 +274,10 @@ void launch_iota(uint32_t *id, int64_t n, cudaStream_t s, uint32_t first = 0);
 void launch_add_offset(uint32_t *id, int64_t n, int64_t delta, cudaStream_t s);
 
 // batch.cu
-void launch_seg_bbox(const float4 *pos, const int2 *inst_range, int num_inst, float *inst_box, cudaStream_t s);
-void launch_seg_morton(const float4 *pos, int64_t n, const int *inst_of, const float *inst_box, uint64_t *codes,
+// inst_box: 6 order-preserving uints per instance (min.xyz, ~max.xyz); slices: blocks per instance
+void launch_seg_bbox(const float4 *pos, const int2 *inst_range, int num_inst, int slices, uint32_t *inst_box,
+                     cudaStream_t s);
+void launch_seg_morton(const float4 *pos, int64_t n, const int *inst_of, const uint32_t *inst_box, uint64_t *codes,
                        uint32_t *hist, cudaStream_t s);
 void launch_inst_keys(const uint32_t *slot, int64_t n, const int *inst_of, uint64_t *ikeys, cudaStream_t s);
 void launch_compose(const uint32_t *order, int64_t n, const uint32_t *slot, const uint64_t *codes, uint32_t *perm,
