@@ -416,4 +416,50 @@ inline std::vector<std::string> solverIds() {
     return {"linear-bvh", "linear-bvh-4p", "naive", "implicit-linear-bvh-fmm-8p"};
 }
 
+// MultiSolver (MultiSolver.h:20-114): the solvers of solverIds() behind one object, one selected
+// at a time, so a caller can switch algorithms by id as the reference's application does. The
+// reference constructs every solver up front; here a solver (and its device context) is created
+// on its first selection and kept, so unused algorithms hold no device memory. The first solver
+// (by default "linear-bvh-4p") is selected on construction. An unknown id throws (the reference
+// logs an error and keeps its selection, MultiSolver.h:79-87).
+class MultiSolver {
+public:
+    MultiSolver(Simulation &sim, Gravity &rule, const std::string &initial = "linear-bvh-4p")
+        : _sim(sim), _rule(rule) {
+        select(initial);
+    }
+
+    void select(const std::string &id) {
+        const auto ids = solverIds();
+        for (std::size_t i = 0; i < ids.size(); ++i)
+            if (ids[i] == id) return select(i);
+        throw Error(NB_ERR_INVALID_ARGUMENT, "unknown solver id: " + id);
+    }
+    void select(std::size_t index) {
+        const auto ids = solverIds();
+        if (index >= ids.size()) throw Error(NB_ERR_INVALID_ARGUMENT, "solver index out of range");
+        if (_solvers.size() < ids.size()) _solvers.resize(ids.size());
+        if (!_solvers[index]) _solvers[index] = makeSolver(ids[index], _sim, _rule);
+        // a newly selected solver starts from the simulation's current bodies
+        _solvers[index]->invalidate();
+        _selected = index;
+    }
+    std::size_t selected() const { return _selected; }
+
+    Solver &get() { return *_solvers[_selected]; }
+    const Solver &get() const { return *_solvers[_selected]; }
+
+    std::string id() const { return get().id(); }
+    std::string name() const { return get().name(); }
+    void updateAccelerations() { get().updateAccelerations(); }
+    void step(int n = 1) { get().step(n); }
+    InteractionCounts counts() const { return get().counts(); }
+
+private:
+    Simulation &_sim;
+    Gravity &_rule;
+    std::vector<std::unique_ptr<Solver>> _solvers;
+    std::size_t _selected = 0;
+};
+
 }  // namespace nbody_b200

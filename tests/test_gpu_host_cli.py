@@ -101,3 +101,65 @@ def test_cli_verbose_steps_on_background_thread(tmp_path, nb):
     p1, v1, _, _ = nb.scenarios.read_json(str(verbose))
     assert np.array_equal(p0, p1)
     assert np.array_equal(v0[:, :3], v1[:, :3])
+
+
+MULTI_PROGRAM = r"""
+#include "nbody_b200.hpp"
+#include "scenario.hpp"
+#include <cstdio>
+#include <fstream>
+using namespace nbody_b200;
+static void configure(MultiSolver &ms) {
+    ms.get().setTheta(0.5f);
+    ms.get().setMaxLeafSize(16);
+    ms.get().setTimeStep(0.001f);
+}
+int main(int argc, char **argv) {
+    Scenario sc = load_scenario(argv[1]);
+    Gravity rule(1.0f, 1e-4f);
+    MultiSolver ms(sc.simulation, rule, "linear-bvh-4p");
+    configure(ms);
+    ms.step(3);
+    ms.select("naive");
+    configure(ms);
+    ms.step(1);
+    ms.select(1);  // linear-bvh-4p again: it resumes from the simulation's current bodies
+    configure(ms);
+    ms.step(1);
+    std::ofstream(argv[2]) << scenario_to_json(sc.simulation, nullptr);
+    std::printf("%s\n", ms.id().c_str());
+}
+"""
+
+
+def test_multisolver_switches_between_solvers(tmp_path, nb):
+    """MultiSolver::select switches algorithms on one simulation; each step equals the same step
+    through that solver class alone, bit for bit."""
+    src = tmp_path / "multi.cpp"
+    src.write_text(MULTI_PROGRAM)
+    exe = tmp_path / "multi"
+    lib = os.path.join(REPO, "n-body_b200", "lib")
+    host = os.path.join(REPO, "n-body_b200", "host")
+    subprocess.run(["g++", "-std=c++17", "-I", host, "-o", str(exe), str(src), "-L", lib, "-lnbody_b200",
+                    "-Wl,-rpath," + lib], check=True)
+    pm, vel = nb.scenarios.plummer(3000, seed=41)
+    scen = tmp_path / "in.json"
+    nb.scenarios.write_json(str(scen), pm, vel)
+    out = tmp_path / "out.json"
+    r = subprocess.run([str(exe), str(scen), str(out)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip() == "linear-bvh-4p"
+    p_cpp, v_cpp, _, _ = nb.scenarios.read_json(str(out))
+    rule = nb.Gravity(1.0, 1e-4)
+    kw = dict(rule=rule, theta=0.5, max_leaf_size=16, time_step=1e-3)
+    with nb.QuadrupoleLinearBVHSolver(bodies=pm, velocities=vel, **kw) as s:
+        s.step(3)
+        p, v = s.bodies()
+    with nb.NaiveSolver(bodies=p, velocities=v, **kw) as s:
+        s.step(1)
+        p, v = s.bodies()
+    with nb.QuadrupoleLinearBVHSolver(bodies=p, velocities=v, **kw) as s:
+        s.step(1)
+        p, v = s.bodies()
+    assert np.array_equal(p_cpp, p)
+    assert np.array_equal(v_cpp[:, :3], v[:, :3])

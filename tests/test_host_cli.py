@@ -225,3 +225,50 @@ def test_simulation_helpers(tmp_path):
     assert out[3].split() == ["4", "9", "1", "0"]  # the box is half-open: its max corner is outside
     assert out[4].split() == ["2", "-1", "1"]
     assert out[5] == "1"
+
+
+MULTI_PROGRAM = r"""
+#include "nbody_b200.hpp"
+#include <cstdio>
+#include <cstring>
+int main(int argc, char **argv) {
+    nbody_b200::Simulation sim;
+    sim.newParticle({0, 0, 0}, {0, 0, 0}, 1.f);
+    sim.newParticle({1, 0, 0}, {0, 0, 0}, 1.f);
+    nbody_b200::Gravity rule;
+    try {
+        nbody_b200::MultiSolver ms(sim, rule, argv[1]);
+        std::printf("selected %s\n", ms.id().c_str());
+    } catch (const nbody_b200::Error &e) {
+        std::printf("error %s\n", e.what());
+    }
+}
+"""
+
+
+def build_multi(tmp_path):
+    src = tmp_path / "multi.cpp"
+    src.write_text(MULTI_PROGRAM)
+    exe = tmp_path / "multi"
+    lib = os.path.join(REPO, "n-body_b200", "lib")
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(REPO, "n-body_b200", "host"), "-o", str(exe), str(src),
+                    "-L", lib, "-lnbody_b200", "-Wl,-rpath," + lib], check=True)
+    return exe
+
+
+def test_multisolver_rejects_unknown_ids(tmp_path):
+    """MultiSolver::select with an id the device path does not implement fails before any device
+    work (the reference logs "Unrecognized solver id", MultiSolver.h:79-87)."""
+    exe = build_multi(tmp_path)
+    out = subprocess.run([str(exe), "barnes-hut-octree"], capture_output=True, text=True, check=True).stdout
+    assert out.strip() == "error unknown solver id: barnes-hut-octree"
+
+
+def test_multisolver_without_gpu_fails_loudly(tmp_path):
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    exe = build_multi(tmp_path)
+    out = subprocess.run([str(exe), "linear-bvh-4p"], capture_output=True, text=True, check=True).stdout
+    assert out.startswith("error nb_create failed")
