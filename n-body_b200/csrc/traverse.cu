@@ -320,17 +320,13 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
                 if (is_int_open) {
                     const int sp = top + 2 * __popc(bi & lt);
                     if (sp + 1 < kTraverseStack) {
-                        stack[sp] = make_int2(l0, (int) m);          // right child
-                        stack[sp + 1] = make_int2(c + 1, (int) m);   // left child, popped first
+                        stack[sp] = make_int2(l0, (int) m);     // right child
+                        stack[sp + 1] = make_int2(c + 1, (int) m);  // left child, popped first
                     } else {
                         atomicOr(err, (uint32_t) kErrStackOverflow);
                     }
                 }
-                top += 2 * __popc(bi);
-                if (top > kTraverseStack) {  // a push was dropped: abandon the group rather than read unwritten entries
-                    top = 0;
-                    nmixed = 0;
-                }
+                top = min(top + 2 * __popc(bi), kTraverseStack);
                 __syncwarp();
                 // each round appends at most 32 entries per list: evaluate before the next one
                 if (napprox > kList - 32) flush_approx<ORDER, EPS0>(L, napprox, pay, p, eps, ax, ay, az, gnp);
@@ -384,11 +380,7 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
                         atomicOr(err, (uint32_t) kErrStackOverflow);
                     }
                 }
-                top += 2 * __popc(bi);
-                if (top > kTraverseStack) {  // a push was dropped: abandon the group rather than read unwritten entries
-                    top = 0;
-                    nmixed = 0;
-                }
+                top = min(top + 2 * __popc(bi), kTraverseStack);
                 __syncwarp();
                 if (napprox > kList - 32) flush_approx<ORDER, EPS0>(L, napprox, pay, p, eps, ax, ay, az, gnp);
                 if (npp > kList - 32) flush_pp<EPS0>(L, npp, bodies, p, eps, lane, ax, ay, az, gpp);
