@@ -45,6 +45,10 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kList = 64;          // capacity of each per-warp list; rounds append at most 32
+// Stack bound: a round pops up to 32 entries and pushes at most 2 per popped node, so at most 32
+// entries per tree level stay behind: at most 32 * depth + 64 entries. The Karras tree over 64-bit
+// codes with 32-bit index tie-breaks is at most 96 levels deep (3136 entries), within
+// kTraverseStack (4608); the overflow branch below only guards a corrupted tree.
 constexpr int kPriv = 32;          // per-target private list of partially accepted nodes
 constexpr unsigned kFull = 0xffffffffu;
 
