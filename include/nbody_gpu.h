@@ -14,7 +14,8 @@
  *     as (vx, vy, vz, unused), accelerations as (ax, ay, az, 0), always in the caller's order.
  *     The reference keeps Position/Velocity/Acceleration as glm::vec3 and Mass as float
  *     components in an EnTT registry (src/NBody/Simulation/Simulation.h:45); a caller gathers
- *     those views into these arrays.
+ *     those views into these arrays (one pass over view<Position, Mass>, one over
+ *     view<Velocity>) and scatters the accelerations back the same way.
  *   - "_device" variants take device pointers (16-byte aligned) on the context's device.
  *   - Work is ordered on the context's CUDA stream (nb_set_stream to share the caller's stream).
  *     Calls that return host data synchronise that stream.
