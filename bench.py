@@ -61,7 +61,9 @@ CPU_SAMPLE_TARGETS = 32768
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: the configuration's own count: 100 for plummer-1m, 50 for "
+                         "batched, 2 for dual-4m; 3 CPU samples for --impl reference)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=N_BODIES)
@@ -81,7 +83,13 @@ def parse():
     ap.add_argument("--shard-targets", action="store_true",
                     help="N>1: one instance sharded over the ranks' targets with an NCCL all-gather of "
                          "positions and velocities per step (strong scaling) instead of one instance per rank")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.steps is None:
+        if args.impl == "reference":
+            args.steps = 3
+        else:
+            args.steps = {"plummer-1m": 100, "batched": 50, "dual-4m": 2}.get(args.workload, 20)
+    return args
 
 
 def dist_env():
