@@ -13,12 +13,13 @@ warp traversal, then kick-drift) on the whole body set. Prints ONE JSON line on 
   roofline dominant kernel = the traversal (FP32 pipe + MUFU bound, no tensor-core work):
           achieved = counted interactions x flop weights / traversal event time; a second entry
           gives the sort's algorithmic HBM bytes against the measured copy bandwidth
-  cpu_baseline  the oracle (CPU restatement of the reference's TBB path) on a bounded sample:
-          full tree build over all N bodies plus the traversal of a seeded target subsample,
-          extrapolated to all N targets, OpenMP over all host cores
+  cpu_baseline  the oracle (CPU restatement of the reference's TBB path, timing build -O3
+          -march=native) for one whole measured step of the same workload: sort, build,
+          summaries, traversal of all N bodies, kick-drift; OpenMP over all host cores
 
 With --impl reference the same metric is measured for the reference's algorithm on the host
-cores (the oracle port: the reference itself cannot be built on this image).
+cores (the oracle port: the reference itself cannot be built on this image): whole steps,
+as many of the requested ones as fit in 150 s (at least one), the count stated in the line.
 Under torchrun (N > 1) every rank runs its own instance (weak scaling, no data-path collective);
 timing is the max over ranks.
 """
@@ -55,7 +56,6 @@ NUM_SMS = 148
 # Minimum HBM bytes per body and step of the memory-bound phases (float4 state, 64-bit keys):
 # bbox 16, Morton 28, sort 8 passes x 24 = 192, gather 32, Karras build 40, moments 24, kick-drift 80.
 BODY_STEP_BYTES = 16 + 28 + 192 + 32 + 40 + 24 + 80
-CPU_SAMPLE_TARGETS = 32768
 
 
 def parse():
@@ -190,37 +190,58 @@ def accuracy(nb, solver, pm, eps, torch, device):
     }
 
 
-def cpu_baseline(pm, eps, steps=1):
-    """The oracle (CPU restatement) on a bounded sample of the workload."""
+REF_BUDGET_S = 150.0   # the reference arm stops timing whole steps once this much has elapsed (>= 1 step)
+CPU_WARMUP_N = 1 << 16
+
+
+def _oracle_timing():
+    """The oracle's timing build (-O3 -march=native, compiled for this host on first use)."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle as O
 
-    O.lib()
-    n = len(pm)
-    threads = O.max_threads()
-    rng = np.random.default_rng(777)
-    s = min(CPU_SAMPLE_TARGETS, n)
-    idx = np.sort(rng.choice(n, s, replace=False))
-    tiny = pm[idx[:1]].copy()
-    t0 = time.perf_counter()
-    O.bh_targets(pm, tiny, eps=eps, theta=THETA, leaf=LEAF, order=ORDER)
-    t_build = time.perf_counter() - t0
-    t_total = 0.0
-    for _ in range(steps):
+    return O, O.timing_lib()
+
+
+def cpu_whole_steps(pm, vel, eps, max_steps, budget_s):
+    """Whole Solver::step()s of the oracle (the reference's algorithm, OpenMP over the host cores
+    where the reference runs tbb::parallel_for_each): Morton codes, sort, tree build, summaries,
+    the traversal of every body, then the kick-drift. Stops after max_steps, or once budget_s has
+    elapsed (at least one step). Returns (seconds per step list, threads)."""
+    O, L = _oracle_timing()
+    p, v = pm, vel
+    times = []
+    t_all = time.perf_counter()
+    for _ in range(max_steps):
         t0 = time.perf_counter()
-        O.bh_targets(pm, pm[idx], eps=eps, theta=THETA, leaf=LEAF, order=ORDER)
-        t_total += time.perf_counter() - t0
-    t_sample = t_total / steps
-    per_target = max(t_sample - t_build, 1e-12) / s
-    step_time = t_build + per_target * n
+        a, _ = O.bh_accelerations(p, eps=eps, theta=THETA, leaf=LEAF, order=ORDER, L=L)
+        p, v = O.kick_drift(p, v, a, DT, L=L)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_all > budget_s:
+            break
+    return times, O.max_threads(L)
+
+
+def cpu_warmup(eps):
+    """One untimed whole step at 2^16 bodies (builds the timing library, pages in, starts threads)."""
+    from nbody_b200 import scenarios
+
+    wp, wv = scenarios.plummer(CPU_WARMUP_N, seed=SEED)
+    cpu_whole_steps(wp, wv, eps, 1, 0.0)
+
+
+def cpu_baseline(pm, vel, eps):
+    """The oracle timed for one whole step of the workload (measured, not extrapolated)."""
+    cpu_warmup(eps)
+    times, threads = cpu_whole_steps(pm, vel, eps, 1, 0.0)
+    n = len(pm)
     return {
-        "value": n / step_time,
+        "value": n / times[0],
         "unit": "body-steps/s",
         "cores": threads,
         "kind": "port",
-        "sample": f"tree build over all {n} bodies + traversal of {s} seeded targets "
-                  f"({t_sample:.2f} s per sample), extrapolated to {n} targets "
-                  f"(est. {step_time:.1f} s per step)",
+        "sample": f"1 whole step measured at N = {n} (Morton sort, tree build, summaries, traversal of all "
+                  f"{n} bodies, kick-drift): {times[0]:.1f} s; oracle timing build -O3 -march=native, "
+                  f"OpenMP over {threads} host threads",
     }
 
 
@@ -231,19 +252,24 @@ def run_reference(args):
     sys.path.insert(0, os.path.join(REPO, "n-body_b200"))
     from nbody_b200 import scenarios
 
-    pm, _ = scenarios.plummer(args.n, seed=SEED)
+    pm, vel = scenarios.plummer(args.n, seed=SEED)
     eps = scenarios.softening_to_epsilon(SOFTENING)
-    if args.warmup > 0:
-        cpu_baseline(pm[: min(len(pm), 65536)], eps, steps=1)
-    vals = []
-    for _ in range(args.steps):
-        vals.append(cpu_baseline(pm, eps, steps=1))
-    value = float(np.median([v["value"] for v in vals]))
-    base = dict(vals[-1])
-    base["value"] = value
+    for _ in range(min(args.warmup, 1)):
+        cpu_warmup(eps)
+    times, threads = cpu_whole_steps(pm, vel, eps, args.steps, REF_BUDGET_S)
+    step_s = float(np.mean(times))
+    value = args.n / step_s
+    base = {
+        "value": value, "unit": "body-steps/s", "cores": threads, "kind": "port",
+        "sample": f"{len(times)} whole steps measured at N = {args.n} (of {args.steps} requested; timing stops "
+                  f"after {REF_BUDGET_S:.0f} s): Morton sort, tree build, summaries, traversal of all bodies, "
+                  f"kick-drift; oracle timing build -O3 -march=native, OpenMP over {threads} host threads",
+    }
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "body-steps/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * args.n / value,
+        "steps": len(times), "steps_requested": args.steps, "warmup": min(args.warmup, 1),
+        "warmup_note": f"one untimed whole step at N = {CPU_WARMUP_N}",
+        "ms_per_step": 1000.0 * step_s, "step_ms": [1000.0 * t for t in times],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(args), "cpu_baseline": base,
         "e2e": {"value": value, "unit": "body-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -403,7 +429,7 @@ def _run_ours_on_stream(args, torch, nb, pm, vel, eps, stream, world, rank, devi
             sum(phases[k] for k in phases if k.endswith("_ms") and k != "integrate_ms") / passes)
     line["diagnostics"] = energy_diagnostics(nb, device)
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(pm, eps)
+        line["cpu_baseline"] = cpu_baseline(pm, vel, eps)
     return line
 
 
@@ -540,15 +566,7 @@ def batched_instances(count, seed=44):
     """256 Plummer spheres with N log-uniform in [1024, 200000] and theta uniform in [0.4, 0.7]."""
     from nbody_b200 import scenarios
 
-    rng = np.random.default_rng(seed)
-    sizes = np.round(np.exp(rng.uniform(np.log(1024), np.log(200000), count))).astype(np.int64)
-    thetas = rng.uniform(0.4, 0.7, count).astype(np.float32)
-    bodies, vels = [], []
-    for k, n in enumerate(sizes):
-        pm, vel = scenarios.plummer(int(n), seed=seed * 1000 + k)
-        bodies.append(pm)
-        vels.append(vel)
-    return sizes, thetas, bodies, vels
+    return scenarios.batched_plummer(count, seed=seed)
 
 
 def run_batched(args):
@@ -852,13 +870,7 @@ def colliding_hernquist(half, seed=46):
     x = +10, approaching at 0.5 along x (+-0.25 each)."""
     from nbody_b200 import scenarios
 
-    a, va = scenarios.hernquist(half, seed=seed)
-    b, vb = scenarios.hernquist(half, seed=seed + 1)
-    a[:, 0] -= np.float32(10.0)
-    b[:, 0] += np.float32(10.0)
-    va[:, 0] += np.float32(0.25)
-    vb[:, 0] -= np.float32(0.25)
-    return np.concatenate([a, b]), np.concatenate([va, vb])
+    return scenarios.colliding_hernquist(half, seed=seed)
 
 
 def dual_cpu_baseline(half_sample, eps):

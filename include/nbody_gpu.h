@@ -168,6 +168,10 @@ int nb_set_instances(nb_ctx *ctx, int32_t count, const int64_t *sizes, const flo
 int32_t nb_instance_count(const nb_ctx *ctx);
 /* Preorder index of each instance's root in the last tree built (count entries; synchronises). */
 int nb_get_instance_roots(nb_ctx *ctx, int32_t *roots);
+/* SimpleTrackingRule counts (SimpleTrackingRule.h:29-51) of the last force pass, per instance of
+ * the batch: particle_particle[k] and node_particle[k] for instance k, exactly what a standalone
+ * solver over instance k counts (count must equal nb_instance_count; synchronises). */
+int nb_get_instance_counts(nb_ctx *ctx, int32_t count, uint64_t *particle_particle, uint64_t *node_particle);
 
 /* Capture pairs of steps in a CUDA graph and replay it in nb_step (off by default; per-phase
  * timing, when enabled, runs the steps uncaptured). */

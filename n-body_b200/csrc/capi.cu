@@ -80,6 +80,7 @@ struct nb_ctx {
     int2 *inst_range = nullptr;
     int4 *groups = nullptr;
     int64_t ngroups = 0;
+    unsigned long long *inst_counts = nullptr;  // (particle-particle, node-particle) per instance
     uint64_t *ikeys = nullptr, *ikeys2 = nullptr;
     uint32_t *ivals = nullptr, *ivals2 = nullptr;
     uint32_t *inst_offsets = nullptr, *inst_lookback = nullptr, *inst_tiles = nullptr;
@@ -180,7 +181,7 @@ void free_batch(nb_ctx *ctx) {
     dev_free(ctx->inst_of); dev_free(ctx->inst_root); dev_free(ctx->inst_theta2); dev_free(ctx->inst_box);
     dev_free(ctx->inst_range); dev_free(ctx->groups); dev_free(ctx->ikeys); dev_free(ctx->ikeys2);
     dev_free(ctx->ivals); dev_free(ctx->ivals2); dev_free(ctx->inst_offsets); dev_free(ctx->inst_lookback);
-    dev_free(ctx->inst_tiles); dev_free(ctx->group_first);
+    dev_free(ctx->inst_tiles); dev_free(ctx->group_first); dev_free(ctx->inst_counts);
     ctx->batch_body_cap = ctx->batch_inst_cap = ctx->batch_group_cap = 0;
     ctx->num_inst = 0;
     ctx->ngroups = 0;
@@ -447,7 +448,7 @@ int force_pass_batch(nb_ctx *ctx, Marks &mk) {
     mk.mark(kMorton);
     launch_seg_morton(ctx->pos, n, ctx->inst_of, ctx->inst_box, ctx->keys, ctx->sw.hist, s);
     mk.mark(kSort);
-    launch_radix_sort(ctx->keys, ctx->vals, n, ctx->sw, ctx->err, s);
+    NB_TRY(launch_radix_sort(ctx->keys, ctx->vals, n, ctx->sw, ctx->err, s), "radix sort");
     launch_inst_keys(ctx->vals, n, ctx->inst_of, ctx->ikeys, s);
     const int64_t tiles = sort_tiles(n);
     cudaMemsetAsync(ctx->inst_lookback, 0, (size_t) ctx->inst_passes * tiles * 256 * sizeof(uint32_t), s);
@@ -477,9 +478,10 @@ int force_pass_batch(nb_ctx *ctx, Marks &mk) {
                       ctx->nodes, ctx->err, s, seg);
     ctx->sorted_codes = ctx->sw.keys_alt;
     mk.mark(kTraverse);
+    cudaMemsetAsync(ctx->inst_counts, 0, (size_t) 2 * ctx->num_inst * sizeof(unsigned long long), s);
     launch_bh_traverse(ctx->cfg.order, ctx->nodes, ctx->tw.num_nodes, ctx->pos, n, ctx->pos, n, ctx->cfg.G,
                        ctx->cfg.epsilon, ctx->acc, ctx->counts, ctx->trav, ctx->err, s, ctx->groups, ctx->ngroups,
-                       ctx->inst_root);
+                       ctx->inst_root, ctx->inst_counts);
     ctx->have_tree = true;
     ctx->acc_is_bh = true;
     if (ctx->timing) ctx->times.launches += launches_per_pass(ctx, false, false) + 4 + ctx->inst_passes;
@@ -512,7 +514,7 @@ int force_pass(nb_ctx *ctx, Marks &mk) {
     mk.mark(kMorton);
     launch_morton_hist(ctx->pos, n, ctx->bbox, ctx->keys, ctx->sw.hist, s);
     mk.mark(kSort);
-    launch_radix_sort(ctx->keys, ctx->vals, n, ctx->sw, ctx->err, s);
+    NB_TRY(launch_radix_sort(ctx->keys, ctx->vals, n, ctx->sw, ctx->err, s), "radix sort");
     mk.mark(kGather);
     launch_gather_state(ctx->vals, n, ctx->pos, ctx->vel, ctx->id, ctx->pos2, ctx->vel2, ctx->id2, s);
     std::swap(ctx->pos, ctx->pos2);
@@ -885,6 +887,25 @@ int nb_synchronize(nb_ctx *ctx) {
     return device_status(ctx);
 }
 
+int nb_get_instance_counts(nb_ctx *ctx, int32_t count, uint64_t *particle_particle, uint64_t *node_particle) {
+    int rc = begin(ctx);
+    if (rc != NB_OK) return rc;
+    if (ctx->num_inst == 0) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "the context holds no batch of instances");
+    if (count != ctx->num_inst) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "count must equal the number of instances");
+    if (!particle_particle || !node_particle) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "output is NULL");
+    if (!ctx->acc_is_bh) return fail(ctx, NB_ERR_INVALID_ARGUMENT, "no force pass has run on this batch");
+    std::vector<unsigned long long> c((size_t) 2 * count);
+    NB_TRY(cudaMemcpyAsync(c.data(), ctx->inst_counts, c.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                           ctx->stream), "read instance counts");
+    rc = device_status(ctx);
+    if (rc != NB_OK) return rc;
+    for (int32_t k = 0; k < count; ++k) {
+        particle_particle[k] = c[2 * (size_t) k];
+        node_particle[k] = c[2 * (size_t) k + 1];
+    }
+    return NB_OK;
+}
+
 int nb_get_counts(nb_ctx *ctx, nb_counts *out) {
     int rc = begin(ctx);
     if (rc != NB_OK) return rc;
@@ -1090,13 +1111,14 @@ static int build_batch_tables(nb_ctx *ctx, int32_t count, const int64_t *sizes, 
     }
     if (count > ctx->batch_inst_cap) {
         dev_free(ctx->inst_root); dev_free(ctx->inst_theta2); dev_free(ctx->inst_box); dev_free(ctx->inst_range);
-        dev_free(ctx->group_first);
+        dev_free(ctx->group_first); dev_free(ctx->inst_counts);
         ctx->batch_inst_cap = 0;
         NB_TRY(dev_alloc(&ctx->inst_root, (size_t) count), "alloc batch");
         NB_TRY(dev_alloc(&ctx->inst_theta2, (size_t) count), "alloc batch");
         NB_TRY(dev_alloc(&ctx->inst_box, (size_t) count * 6), "alloc batch");
         NB_TRY(dev_alloc(&ctx->inst_range, (size_t) count), "alloc batch");
         NB_TRY(dev_alloc(&ctx->group_first, (size_t) count), "alloc batch");
+        NB_TRY(dev_alloc(&ctx->inst_counts, (size_t) 2 * count), "alloc batch");
         ctx->batch_inst_cap = count;
     }
     if (ngroups > ctx->batch_group_cap) {

@@ -121,6 +121,8 @@ void launch_morton_hist(const float4 *pos, int64_t n, const BBoxAccum *acc, uint
                         cudaStream_t s);
 
 // radix_sort.cu
+constexpr int kSortTileKeys = 2048;  // keys ranked per block (tile) of one one-sweep pass
+constexpr int kSortPasses = 8;       // 8-bit digits of the 64-bit keys
 struct SortWorkspace {
     uint64_t *keys_alt = nullptr;
     uint32_t *vals_alt = nullptr;
@@ -133,8 +135,10 @@ struct SortWorkspace {
 int64_t sort_tiles(int64_t n);
 size_t sort_lookback_words(int64_t n);
 // Sorts (keys, iota) by key; the sorted keys and slot indices end in keys/vals (ping-pong inside).
-void launch_radix_sort(uint64_t *keys, uint32_t *vals, int64_t n, SortWorkspace &ws, uint32_t *err,
-                       cudaStream_t s);
+// Returns the first error reported while queuing its memsets and launches (checked with
+// cudaPeekAtLastError, which clears nothing).
+cudaError_t launch_radix_sort(uint64_t *keys, uint32_t *vals, int64_t n, SortWorkspace &ws, uint32_t *err,
+                              cudaStream_t s);
 // One stable one-sweep pass on digit `pass` (bits 8*pass .. 8*pass+7) of the keys. offsets holds
 // the exclusive digit prefixes at [pass*256 + d] and a trivial-pass flag at [8*256 + pass];
 // lookback (pass x tiles x 256 words) and tile_counter[pass] must be zero. Pass 0 ignores vals_in
@@ -247,11 +251,13 @@ constexpr int kTraverseStack = 4608;
 int64_t traverse_resident_warps(int device);
 // groups (optional): one int4 (first target, target count <= 32, instance, 0) per warp task; the
 // traversal of a group starts at inst_root[instance]. Without groups, targets are cut into
-// consecutive groups of 32 that start at node 0.
+// consecutive groups of 32 that start at node 0. inst_counts (optional, with groups): per instance,
+// (particle-particle, node-particle) interaction counts are added at [2 * instance + {0, 1}].
 void launch_bh_traverse(int order, const NodeArrays &nodes, const int *num_nodes, const float4 *bodies, int64_t n_bodies,
                         const float4 *targets, int64_t n_targets, float G, float eps, float4 *acc,
                         unsigned long long *counts, TraverseWorkspace &ws, uint32_t *err, cudaStream_t s,
-                        const int4 *groups = nullptr, int64_t num_groups = 0, const int *inst_root = nullptr);
+                        const int4 *groups = nullptr, int64_t num_groups = 0, const int *inst_root = nullptr,
+                        unsigned long long *inst_counts = nullptr);
 
 // direct_sum.cu
 // FP64 energy diagnostics: (kinetic, potential) of n bodies into out[0..1]; parts needs
@@ -284,6 +290,11 @@ void launch_compose(const uint32_t *order, int64_t n, const uint32_t *slot, cons
                     uint64_t *codes_out, cudaStream_t s);
 void launch_fill_tables(const int2 *inst_range, const int *group_first, int num_inst, int *inst_of, int4 *groups,
                         cudaStream_t s);
+
+// SM count of a device, queried once per device (cached).
+int sm_count(int device);
+// SM count of the current device.
+int current_sm_count();
 
 // Largest number of bodies one context accepts (30-bit counts in the sort's look-back words,
 // 31-bit body indices in the tree).

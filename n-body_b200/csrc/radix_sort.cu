@@ -23,9 +23,10 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kItems = 8;
-constexpr int kTile = kThreads * kItems;
+constexpr int kTile = kSortTileKeys;
+static_assert(kThreads * kItems == kTile, "one tile is kItems keys per thread");
 constexpr int kWarps = kThreads / 32;
-constexpr int kPasses = 8;
+constexpr int kPasses = kSortPasses;
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagInc = 2u << 30;
 constexpr uint32_t kFlagMask = 3u << 30;
@@ -231,22 +232,28 @@ void launch_radix_pass(const uint64_t *keys_in, const uint32_t *vals_in, uint64_
                                                                    offsets, lookback, tile_counter, err);
 }
 
-void launch_radix_sort(uint64_t *keys, uint32_t *vals, int64_t n, SortWorkspace &ws, uint32_t *err,
-                       cudaStream_t s) {
-    if (n <= 0) return;
+cudaError_t launch_radix_sort(uint64_t *keys, uint32_t *vals, int64_t n, SortWorkspace &ws, uint32_t *err,
+                              cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
     const int64_t tiles = sort_tiles(n);
-    cudaMemsetAsync(ws.lookback, 0, (size_t) kPasses * tiles * 256 * sizeof(uint32_t), s);
-    cudaMemsetAsync(ws.tile_counter, 0, kPasses * sizeof(uint32_t), s);
+    cudaError_t e = cudaMemsetAsync(ws.lookback, 0, sort_lookback_words(n) * sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(ws.tile_counter, 0, kPasses * sizeof(uint32_t), s);
+    if (e != cudaSuccess) return e;
     scan_hist_kernel<<<kPasses, 256, 0, s>>>(ws.hist, ws.offsets, n);
+    if ((e = cudaPeekAtLastError()) != cudaSuccess) return e;
     uint64_t *kin = keys, *kout = ws.keys_alt;
     uint32_t *vin = vals, *vout = ws.vals_alt;
     for (int p = 0; p < kPasses; ++p) {
         onesweep_kernel<<<(unsigned) tiles, kThreads, 0, s>>>(kin, vin, kout, vout, n, p, ws.offsets, ws.lookback,
                                                                ws.tile_counter, err);
+        if ((e = cudaPeekAtLastError()) != cudaSuccess) return e;
         uint64_t *tk = kin; kin = kout; kout = tk;
         uint32_t *tv = vin; vin = vout; vout = tv;
     }
     // An even number of passes leaves the result in (keys, vals).
+    static_assert(kPasses % 2 == 0, "the sorted data must end in the caller's buffers");
+    return cudaSuccess;
 }
 
 }  // namespace nbg

@@ -13,6 +13,8 @@
 //     from the first use of the library on that GPU until the process exits;
 //   - the first call on a device looks up the array's device address (cudaGetSymbolAddress) with
 //     that device current; make that first call before any stream capture;
+//   - each call returns only once the sort has finished: it copies a status word to the host and
+//     synchronises the stream (pageable copy + cudaStreamSynchronize);
 //   - every call shares the one array and it keeps the previous call's contents: each call clears
 //     what must start at zero, but two calls that overlap on the GPU (different streams, or
 //     different host threads) race on the scratch and corrupt each other's results.
@@ -27,18 +29,21 @@ namespace nbg {
 namespace {
 
 constexpr int64_t kNoAllocMaxKeys = int64_t(1) << 20;
-constexpr int64_t kTileKeys = 2048;  // keys per tile of the one-sweep kernel (radix_sort.cu)
-constexpr int64_t kMaxTiles = (kNoAllocMaxKeys + kTileKeys - 1) / kTileKeys;
+constexpr int64_t kMaxTiles = (kNoAllocMaxKeys + kSortTileKeys - 1) / kSortTileKeys;
 
 constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr size_t kOffKeys = 0;
 constexpr size_t kOffVals = align256(kOffKeys + sizeof(uint64_t) * kNoAllocMaxKeys);
 constexpr size_t kOffHist = align256(kOffVals + sizeof(uint32_t) * kNoAllocMaxKeys);
-constexpr size_t kOffOffsets = align256(kOffHist + sizeof(uint32_t) * 8 * 256);
-constexpr size_t kOffLookback = align256(kOffOffsets + sizeof(uint32_t) * (8 * 256 + 8));
-constexpr size_t kOffTiles = align256(kOffLookback + sizeof(uint32_t) * 8 * kMaxTiles * 256);
-constexpr size_t kOffErr = align256(kOffTiles + sizeof(uint32_t) * 8);
+constexpr size_t kOffOffsets = align256(kOffHist + sizeof(uint32_t) * kSortPasses * 256);
+constexpr size_t kOffLookback = align256(kOffOffsets + sizeof(uint32_t) * (kSortPasses * 256 + kSortPasses));
+constexpr size_t kLookbackWords = (size_t) kSortPasses * kMaxTiles * 256;
+constexpr size_t kOffTiles = align256(kOffLookback + sizeof(uint32_t) * kLookbackWords);
+constexpr size_t kOffErr = align256(kOffTiles + sizeof(uint32_t) * kSortPasses);
 constexpr size_t kNoAllocScratchBytes = align256(kOffErr + sizeof(uint32_t));
+// The sort's launcher clears sort_lookback_words(n) look-back words: at the largest n accepted they
+// must fit before the tile tickets.
+static_assert(kOffLookback + sizeof(uint32_t) * kLookbackWords <= kOffTiles, "look-back region overlaps");
 
 static __device__ __align__(256) unsigned char g_sort_scratch[kNoAllocScratchBytes];
 
@@ -89,6 +94,7 @@ extern "C" int nb_sort_codes_noalloc(const uint64_t *d_codes, uint64_t *d_sorted
     if (n < 0 || n > kNoAllocMaxKeys) return NB_ERR_INVALID_ARGUMENT;
     if (n > 0 && (!d_codes || !d_sorted_codes || !d_sorted_ids)) return NB_ERR_INVALID_ARGUMENT;
     if (n == 0) return NB_OK;
+    if (sort_lookback_words(n) > kLookbackWords) return NB_ERR_INVALID_ARGUMENT;
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices) return NB_ERR_CUDA;
     unsigned char *base = nullptr;
@@ -106,17 +112,17 @@ extern "C" int nb_sort_codes_noalloc(const uint64_t *d_codes, uint64_t *d_sorted
     uint32_t *err = (uint32_t *) (base + kOffErr);
 
     // The scratch keeps the previous call's contents: clear what must start at zero.
-    if (cudaMemsetAsync(ws.hist, 0, sizeof(uint32_t) * 8 * 256, s) != cudaSuccess) return NB_ERR_CUDA;
+    if (cudaMemsetAsync(ws.hist, 0, sizeof(uint32_t) * kSortPasses * 256, s) != cudaSuccess) return NB_ERR_CUDA;
     if (cudaMemsetAsync(err, 0, sizeof(uint32_t), s) != cudaSuccess) return NB_ERR_CUDA;
     if (cudaMemcpyAsync(d_sorted_codes, d_codes, (size_t) n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s) !=
         cudaSuccess)
         return NB_ERR_CUDA;
-    const int64_t blocks = std::min<int64_t>((n + 256 * 8 - 1) / (256 * 8), 148 * 4);
+    const int64_t blocks = std::min<int64_t>((n + 256 * 8 - 1) / (256 * 8), (int64_t) current_sm_count() * 4);
     digit_hist_kernel<<<(unsigned) std::max<int64_t>(blocks, 1), 256, 0, s>>>(d_codes, n, ws.hist);
+    if (cudaPeekAtLastError() != cudaSuccess) return NB_ERR_CUDA;
     // Sorts in place in (d_sorted_codes, d_sorted_ids) with the scratch as the other buffer; the
     // launcher clears the look-back flags and tile tickets itself.
-    launch_radix_sort(d_sorted_codes, d_sorted_ids, n, ws, err, s);
-    if (cudaGetLastError() != cudaSuccess) return NB_ERR_CUDA;
+    if (launch_radix_sort(d_sorted_codes, d_sorted_ids, n, ws, err, s) != cudaSuccess) return NB_ERR_CUDA;
     uint32_t e = 0;
     if (cudaMemcpyAsync(&e, err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess) return NB_ERR_CUDA;
     if (cudaStreamSynchronize(s) != cudaSuccess) return NB_ERR_CUDA;

@@ -45,10 +45,9 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kList = 64;          // capacity of each per-warp list; rounds append at most 32
-// Stack bound: a round pops up to 32 entries and pushes at most 2 per popped node, so at most 32
-// entries per tree level stay behind: at most 32 * depth + 64 entries. The Karras tree over 64-bit
-// codes with 32-bit index tie-breaks is at most 96 levels deep (3136 entries), within
-// kTraverseStack (4608); the overflow branch below only guards a corrupted tree.
+// Stack: kTraverseStack entries per warp. No bound below that size is proven for every tree, so a
+// round whose pushes would not fit abandons its group and sets kErrStackOverflow (the host turns it
+// into an error); every entry on the stack has been written, so no stale entry is ever popped.
 constexpr int kPriv = 32;          // per-target private list of partially accepted nodes
 constexpr unsigned kFull = 0xffffffffu;
 
@@ -213,7 +212,8 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
                                                       unsigned long long *__restrict__ counts,
                                                       int2 *__restrict__ stack_base, unsigned *__restrict__ group_counter,
                                                       uint32_t *__restrict__ err, const int4 *__restrict__ groups,
-                                                      int num_group_tasks, const int *__restrict__ inst_root) {
+                                                      int num_group_tasks, const int *__restrict__ inst_root,
+                                                      unsigned long long *__restrict__ inst_counts) {
     __shared__ WarpLists lists[kWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     WarpLists &L = lists[warp];
@@ -234,12 +234,13 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
         if (lane == 0) g = (int) atomicAdd(group_counter, 1u);
         g = __shfl_sync(kFull, g, 0);
         if (g >= num_groups) break;
-        int first = g * 32, count = min(32, n_targets - g * 32), root = 0;
+        int first = g * 32, count = min(32, n_targets - g * 32), root = 0, inst = -1;
         if (groups) {
             const int4 ge = groups[g];
             first = ge.x;
             count = ge.y;
-            root = inst_root[ge.z];
+            inst = ge.z;
+            root = inst_root[inst];
         }
         const int i = first + lane;
         const bool valid = lane < count && i < n_targets;
@@ -321,16 +322,20 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
                 pos = warp_append(is_mix, nmixed, lt);
                 if (is_mix) { L.mixed_node[pos] = c; L.mixed_mask[pos] = m; }
                 const uint32_t bi = __ballot_sync(kFull, is_int_open);
-                if (is_int_open) {
-                    const int sp = top + 2 * __popc(bi & lt);
-                    if (sp + 1 < kTraverseStack) {
-                        stack[sp] = make_int2(l0, (int) m);     // right child
+                if (top + 2 * __popc(bi) > kTraverseStack) {
+                    // warp-uniform: a push would not fit, so the group is abandoned with an error
+                    // (every entry on the stack was written; nothing unwritten is ever popped)
+                    if (lane == 0) atomicOr(err, (uint32_t) kErrStackOverflow);
+                    top = 0;
+                    nmixed = 0;
+                } else {
+                    if (is_int_open) {
+                        const int sp = top + 2 * __popc(bi & lt);
+                        stack[sp] = make_int2(l0, (int) m);         // right child
                         stack[sp + 1] = make_int2(c + 1, (int) m);  // left child, popped first
-                    } else {
-                        atomicOr(err, (uint32_t) kErrStackOverflow);
                     }
+                    top += 2 * __popc(bi);
                 }
-                top = min(top + 2 * __popc(bi), kTraverseStack);
                 __syncwarp();
                 // each round appends at most 32 entries per list: evaluate before the next one
                 if (napprox > kList - 32) flush_approx<ORDER, EPS0>(L, napprox, pay, p, eps, ax, ay, az, gnp);
@@ -375,16 +380,18 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
                     L.pp_mask[pos] = O;
                 }
                 const uint32_t bi = __ballot_sync(kFull, is_int_open);
-                if (is_int_open) {
-                    const int sp = top + 2 * __popc(bi & lt);
-                    if (sp + 1 < kTraverseStack) {
+                if (top + 2 * __popc(bi) > kTraverseStack) {
+                    if (lane == 0) atomicOr(err, (uint32_t) kErrStackOverflow);
+                    top = 0;
+                    nmixed = 0;
+                } else {
+                    if (is_int_open) {
+                        const int sp = top + 2 * __popc(bi & lt);
                         stack[sp] = make_int2(l0, (int) O);
                         stack[sp + 1] = make_int2(c + 1, (int) O);
-                    } else {
-                        atomicOr(err, (uint32_t) kErrStackOverflow);
                     }
+                    top += 2 * __popc(bi);
                 }
-                top = min(top + 2 * __popc(bi), kTraverseStack);
                 __syncwarp();
                 if (napprox > kList - 32) flush_approx<ORDER, EPS0>(L, napprox, pay, p, eps, ax, ay, az, gnp);
                 if (npp > kList - 32) flush_pp<EPS0>(L, npp, bodies, p, eps, lane, ax, ay, az, gpp);
@@ -397,6 +404,14 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
         if (valid) {
             cnp += gnp;
             cpp += gpp;
+        }
+        if (inst_counts && inst >= 0) {
+            const unsigned ipp = __reduce_add_sync(kFull, valid ? gpp : 0u);
+            const unsigned inp = __reduce_add_sync(kFull, valid ? gnp : 0u);
+            if (lane == 0) {
+                atomicAdd(inst_counts + 2 * (int64_t) inst, (unsigned long long) ipp);
+                atomicAdd(inst_counts + 2 * (int64_t) inst + 1, (unsigned long long) inp);
+            }
         }
         __syncwarp();
     }
@@ -422,6 +437,26 @@ int blocks_per_sm() {
     return cached;
 }
 
+template<int ORDER, bool EPS0>
+void launch_variant(const NodeArrays &nodes, const int *num_nodes, const float4 *bodies, int n_bodies,
+                    const float4 *targets, int nt, float G, float eps, float4 *acc, unsigned long long *counts,
+                    TraverseWorkspace &ws, uint32_t *err, cudaStream_t s, const int4 *gtab, int64_t ngroups,
+                    const int *inst_root, unsigned long long *inst_counts) {
+    int device = 0;
+    cudaGetDevice(&device);
+    int64_t blocks = (int64_t) sm_count(device) * blocks_per_sm<ORDER, EPS0>();
+    blocks = std::min<int64_t>(blocks, ws.warps / kWarps);
+    const int64_t groups = gtab ? ngroups : (nt + 31) / 32;
+    blocks = std::min<int64_t>(blocks, (groups + kWarps - 1) / kWarps);
+    if (blocks < 1) blocks = 1;
+    cudaMemsetAsync(ws.group_counter, 0, sizeof(unsigned), s);
+    bh_kernel<ORDER, EPS0><<<(unsigned) blocks, kThreads, 0, s>>>(nodes, num_nodes, bodies, n_bodies, targets, nt, G,
+                                                                   eps, acc, counts, ws.stack, ws.group_counter, err,
+                                                                   gtab, (int) ngroups, inst_root, inst_counts);
+}
+
+}  // namespace
+
 int sm_count(int device) {
     static int cached[64] = {0};
     if (device < 0 || device >= 64) device = 0;
@@ -433,25 +468,11 @@ int sm_count(int device) {
     return cached[device];
 }
 
-template<int ORDER, bool EPS0>
-void launch_variant(const NodeArrays &nodes, const int *num_nodes, const float4 *bodies, int n_bodies,
-                    const float4 *targets, int nt, float G, float eps, float4 *acc, unsigned long long *counts,
-                    TraverseWorkspace &ws, uint32_t *err, cudaStream_t s, const int4 *gtab, int64_t ngroups,
-                    const int *inst_root) {
+int current_sm_count() {
     int device = 0;
     cudaGetDevice(&device);
-    int64_t blocks = (int64_t) sm_count(device) * blocks_per_sm<ORDER, EPS0>();
-    blocks = std::min<int64_t>(blocks, ws.warps / kWarps);
-    const int64_t groups = gtab ? ngroups : (nt + 31) / 32;
-    blocks = std::min<int64_t>(blocks, (groups + kWarps - 1) / kWarps);
-    if (blocks < 1) blocks = 1;
-    cudaMemsetAsync(ws.group_counter, 0, sizeof(unsigned), s);
-    bh_kernel<ORDER, EPS0><<<(unsigned) blocks, kThreads, 0, s>>>(nodes, num_nodes, bodies, n_bodies, targets, nt, G,
-                                                                   eps, acc, counts, ws.stack, ws.group_counter, err,
-                                                                   gtab, (int) ngroups, inst_root);
+    return sm_count(device);
 }
-
-}  // namespace
 
 int64_t traverse_resident_warps(int device) {
     int b = std::max(std::max(blocks_per_sm<1, false>(), blocks_per_sm<1, true>()),
@@ -462,15 +483,15 @@ int64_t traverse_resident_warps(int device) {
 void launch_bh_traverse(int order, const NodeArrays &nodes, const int *num_nodes, const float4 *bodies, int64_t n_bodies,
                         const float4 *targets, int64_t n_targets, float G, float eps, float4 *acc,
                         unsigned long long *counts, TraverseWorkspace &ws, uint32_t *err, cudaStream_t s,
-                        const int4 *gtab, int64_t ngroups, const int *inst_root) {
+                        const int4 *gtab, int64_t ngroups, const int *inst_root, unsigned long long *inst_counts) {
     if (n_targets <= 0) return;
     const int nb = (int) n_bodies, nt = (int) n_targets;
     if (order == 1) {
-        if (eps == 0.f) launch_variant<1, true>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s, gtab, ngroups, inst_root);
-        else launch_variant<1, false>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s, gtab, ngroups, inst_root);
+        if (eps == 0.f) launch_variant<1, true>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s, gtab, ngroups, inst_root, inst_counts);
+        else launch_variant<1, false>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s, gtab, ngroups, inst_root, inst_counts);
     } else {
-        if (eps == 0.f) launch_variant<2, true>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s, gtab, ngroups, inst_root);
-        else launch_variant<2, false>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s, gtab, ngroups, inst_root);
+        if (eps == 0.f) launch_variant<2, true>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s, gtab, ngroups, inst_root, inst_counts);
+        else launch_variant<2, false>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s, gtab, ngroups, inst_root, inst_counts);
     }
 }
 

@@ -138,6 +138,7 @@ SIGNATURES = {
     "nb_set_instances": (C.c_int, [_vp, _i32, _vp, _vp, _vp, _vp]),
     "nb_instance_count": (_i32, [_vp]),
     "nb_get_instance_roots": (C.c_int, [_vp, _vp]),
+    "nb_get_instance_counts": (C.c_int, [_vp, _i32, _vp, _vp]),
     "nb_enable_graphs": (C.c_int, [_vp, C.c_int]),
     "nb_set_fp64_summaries": (C.c_int, [_vp, C.c_int64]),
     "nb_server_create": (C.c_int, [C.POINTER(Config), C.c_uint64, C.POINTER(_vp)]),
@@ -338,6 +339,14 @@ class Solver:
 
     def instance_count(self) -> int:
         return int(lib().nb_instance_count(self._ctx))
+
+    def instance_counts(self) -> np.ndarray:
+        """(particle-particle, node-particle) counts of the last force pass per instance, shape (k, 2)."""
+        k = self.instance_count()
+        pp = np.zeros(max(k, 1), np.uint64)
+        npc = np.zeros(max(k, 1), np.uint64)
+        self._check(lib().nb_get_instance_counts(self._ctx, k, _ptr(pp), _ptr(npc)))
+        return np.stack([pp[:k], npc[:k]], axis=1)
 
     def autotune(self, cache=None, candidates=None, passes: int = 3, tolerance: float = 0.0):
         """Pick the leaf size for the current bodies by measurement (see autotune.py)."""

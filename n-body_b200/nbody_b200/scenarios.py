@@ -11,6 +11,8 @@ bodies as (x, y, z, m) and velocities as (vx, vy, vz, 0). G = 1 throughout.
                  distribution function by von Neumann rejection (Aarseth, Henon & Wielen 1974)
   hernquist      Hernquist sphere: r = a sqrt(X) / (1 - sqrt(X)), truncated at r_max; isotropic
                  speeds by rejection from the Hernquist (1990) ergodic distribution function
+  colliding_hernquist  two Hernquist spheres on a collision course (the dual-tree scene)
+  batched_plummer      many Plummer spheres of log-uniform sizes and uniform theta (the batch)
 """
 from __future__ import annotations
 
@@ -110,6 +112,34 @@ def hernquist(n: int, seed: int = 44, a: float = 1.0, M: float = 1.0, r_max: flo
     pos -= pos.mean(0)
     vel -= vel.mean(0)
     return _pack(pos, np.full(n, M / n), vel)
+
+
+def colliding_hernquist(half: int, seed: int = 46, separation: float = 20.0, approach: float = 0.5):
+    """Two Hernquist spheres of `half` bodies each (a = 1, total mass 1 each, truncated at 100 a),
+    centred at x = -separation/2 and +separation/2 and approaching at `approach` along x (half of
+    it each): the dual-tree precision-study scene."""
+    a, va = hernquist(half, seed=seed)
+    b, vb = hernquist(half, seed=seed + 1)
+    a[:, 0] -= np.float32(separation / 2)
+    b[:, 0] += np.float32(separation / 2)
+    va[:, 0] += np.float32(approach / 2)
+    vb[:, 0] -= np.float32(approach / 2)
+    return np.concatenate([a, b]), np.concatenate([va, vb])
+
+
+def batched_plummer(count: int, seed: int = 44, n_min: int = 1024, n_max: int = 200000,
+                    theta_range=(0.4, 0.7)):
+    """`count` independent Plummer spheres with N log-uniform in [n_min, n_max] (rounded) and theta
+    uniform in theta_range: (sizes int64[count], thetas float32[count], bodies list, velocities list)."""
+    rng = np.random.default_rng(seed)
+    sizes = np.round(np.exp(rng.uniform(np.log(n_min), np.log(n_max), count))).astype(np.int64)
+    thetas = rng.uniform(theta_range[0], theta_range[1], count).astype(np.float32)
+    bodies, vels = [], []
+    for k, n in enumerate(sizes):
+        pm, vel = plummer(int(n), seed=seed * 1000 + k)
+        bodies.append(pm)
+        vels.append(vel)
+    return sizes, thetas, bodies, vels
 
 
 def softening_to_epsilon(softening_length: float) -> float:

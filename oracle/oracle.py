@@ -33,44 +33,82 @@ def build() -> None:
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
 
+NATIVE_PATH = os.path.join(HERE, "_build", "libnbody_oracle_native.so")
+NATIVE_STAMP = NATIVE_PATH + ".host"
+_timing_lib = None
+
+
+def _host_cpu() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def timing_lib() -> C.CDLL:
+    """The timing build (-O3 -march=native) for the CPU baseline, compiled on first use for the
+    host it runs on (rebuilt when the host's CPU model differs from the one it was built for)."""
+    global _timing_lib
+    if _timing_lib is None:
+        cpu = _host_cpu()
+        stamp = open(NATIVE_STAMP).read() if os.path.exists(NATIVE_STAMP) else None
+        if stamp != cpu or not os.path.exists(NATIVE_PATH):
+            if os.path.exists(NATIVE_PATH):
+                os.remove(NATIVE_PATH)
+            subprocess.run(["make", "-s", "-C", HERE, "native"], check=True)
+            with open(NATIVE_STAMP, "w") as f:
+                f.write(cpu)
+        _timing_lib = _load(NATIVE_PATH)
+    return _timing_lib
+
+
 def lib() -> C.CDLL:
     global _lib
     if _lib is None:
         if not os.path.exists(LIB_PATH):
             build()
-        L = C.CDLL(LIB_PATH)
-        i64, i32, f32, f64 = C.c_int64, C.c_int32, C.c_float, C.c_double
-        sig = {
-            "or_bbox": (None, [i64, _f32p, _f32p]),
-            "or_morton": (None, [i64, _f32p, _f32p, _u64p]),
-            "or_sort": (None, [i64, _u64p, _u32p]),
-            "or_build": (i64, [i64, _u64p, i32, _i32p, _i32p, _i32p, _i32p]),
-            "or_summarize": (C.c_int, [i64, _i32p, _i32p, _i32p, _i32p, _f32p, i32, _f32p, _f32p, _f32p]),
-            "or_bh_accelerations": (i64, [i64, _f32p, f32, f32, f32, i32, i32, _f32p, _u64p, i32]),
-            "or_bh_targets": (i64, [i64, _f32p, i64, _f32p, f32, f32, f32, i32, i32, _f32p, _u64p, i32]),
-            "or_direct_f32": (None, [i64, _f32p, i64, C.c_void_p, f32, f32, _f32p, i32]),
-            "or_direct_f64": (None, [i64, _f32p, i64, C.c_void_p, f64, f64, _f64p, i32]),
-            "or_kick_drift": (None, [i64, _f32p, _f32p, _f32p, f32]),
-            "or_max_threads": (i32, []),
-            "or_particle_particle": (None, [f32, f32, _f32p, f32, _f32p, _f32p]),
-            "or_leaf_summary": (C.c_int, [i64, _f32p, i32, _f32p, _f32p, _f32p]),
-            "or_node_particle": (C.c_int, [i32, f32, f32, _f32p, _f32p, _f32p, _f32p]),
-            "or_particle_node": (C.c_int, [i32, f32, f32, _f32p, f32, _f32p, _f32p]),
-            "or_field_at": (C.c_int, [i32, _f32p, _f32p, _f32p]),
-            "or_field_translated": (C.c_int, [i32, _f32p, _f32p, _f32p]),
-            "or_dual_accelerations": (i64, [i64, _f32p, f32, f32, f32, i32, i32, _f32p, _u64p, i32]),
-            "or_tensor_linear_index": (i32, [i32, _i32p]),
-            "or_tensor_dimensional_index": (C.c_int, [i32, i32, _i32p]),
-            "or_tensor_lexicographic_index": (C.c_int, [i32, i32, _i32p]),
-            "or_tensor_cartesian_power": (C.c_int, [i32, _f32p, _f32p]),
-            "or_tensor2_times_vector": (None, [_f32p, _f32p, _f32p]),
-        }
-        for name, (res, args) in sig.items():
-            fn = getattr(L, name)
-            fn.restype = res
-            fn.argtypes = args
-        _lib = L
+        _lib = _load(LIB_PATH)
     return _lib
+
+
+def _load(path: str) -> C.CDLL:
+    """The library at `path` with every exported function's ctypes signature."""
+    L = C.CDLL(path)
+    i64, i32, f32, f64 = C.c_int64, C.c_int32, C.c_float, C.c_double
+    sig = {
+        "or_bbox": (None, [i64, _f32p, _f32p]),
+        "or_morton": (None, [i64, _f32p, _f32p, _u64p]),
+        "or_sort": (None, [i64, _u64p, _u32p]),
+        "or_build": (i64, [i64, _u64p, i32, _i32p, _i32p, _i32p, _i32p]),
+        "or_summarize": (C.c_int, [i64, _i32p, _i32p, _i32p, _i32p, _f32p, i32, _f32p, _f32p, _f32p]),
+        "or_bh_accelerations": (i64, [i64, _f32p, f32, f32, f32, i32, i32, _f32p, _u64p, i32]),
+        "or_bh_targets": (i64, [i64, _f32p, i64, _f32p, f32, f32, f32, i32, i32, _f32p, _u64p, i32]),
+        "or_direct_f32": (None, [i64, _f32p, i64, C.c_void_p, f32, f32, _f32p, i32]),
+        "or_direct_f64": (None, [i64, _f32p, i64, C.c_void_p, f64, f64, _f64p, i32]),
+        "or_kick_drift": (None, [i64, _f32p, _f32p, _f32p, f32]),
+        "or_max_threads": (i32, []),
+        "or_particle_particle": (None, [f32, f32, _f32p, f32, _f32p, _f32p]),
+        "or_leaf_summary": (C.c_int, [i64, _f32p, i32, _f32p, _f32p, _f32p]),
+        "or_node_particle": (C.c_int, [i32, f32, f32, _f32p, _f32p, _f32p, _f32p]),
+        "or_particle_node": (C.c_int, [i32, f32, f32, _f32p, f32, _f32p, _f32p]),
+        "or_field_at": (C.c_int, [i32, _f32p, _f32p, _f32p]),
+        "or_field_translated": (C.c_int, [i32, _f32p, _f32p, _f32p]),
+        "or_dual_accelerations": (i64, [i64, _f32p, f32, f32, f32, i32, i32, _f32p, _u64p, i32]),
+        "or_tensor_linear_index": (i32, [i32, _i32p]),
+        "or_tensor_dimensional_index": (C.c_int, [i32, i32, _i32p]),
+        "or_tensor_lexicographic_index": (C.c_int, [i32, i32, _i32p]),
+        "or_tensor_cartesian_power": (C.c_int, [i32, _f32p, _f32p]),
+        "or_tensor2_times_vector": (None, [_f32p, _f32p, _f32p]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    return L
 
 
 def _bodies(pm) -> np.ndarray:
@@ -124,13 +162,14 @@ def summarize(tree, pm_sorted, order: int):
     return bb[:nn], cm[:nn], mo[:nn]
 
 
-def bh_accelerations(pm, G=1.0, eps=1e-5, theta=0.5, leaf=16, order=1, threads=0):
+def bh_accelerations(pm, G=1.0, eps=1e-5, theta=0.5, leaf=16, order=1, threads=0, L=None):
     """ActiveTreeSolver (LinearBVH, DiagonalOverCenterDistance, Gravity) accelerations in input
-    order, and the (particle-particle, node-particle) interaction counts."""
+    order, and the (particle-particle, node-particle) interaction counts. L: the library to run
+    (default: the parity build; timing_lib() for the CPU baseline)."""
     pm = _bodies(pm)
     acc = np.zeros((len(pm), 4), np.float32)
     counts = np.zeros(2, np.uint64)
-    nn = lib().or_bh_accelerations(len(pm), pm, G, eps, theta, leaf, order, acc, counts, threads)
+    nn = (L or lib()).or_bh_accelerations(len(pm), pm, G, eps, theta, leaf, order, acc, counts, threads)
     assert nn >= 0
     return acc, counts
 
@@ -180,16 +219,16 @@ def direct_f64(pm, idx=None, G=1.0, eps=1e-5, threads=0) -> np.ndarray:
     return acc
 
 
-def kick_drift(pm, vel, acc, dt: float):
+def kick_drift(pm, vel, acc, dt: float, L=None):
     pm = _bodies(pm).copy()
     vel = _bodies(vel).copy()
     acc = _bodies(acc)
-    lib().or_kick_drift(len(pm), pm, vel, acc, dt)
+    (L or lib()).or_kick_drift(len(pm), pm, vel, acc, dt)
     return pm, vel
 
 
-def max_threads() -> int:
-    return int(lib().or_max_threads())
+def max_threads(L=None) -> int:
+    return int((L or lib()).or_max_threads())
 
 
 # ---- rule-level helpers ----

@@ -159,15 +159,13 @@ def test_cli_rejects_bad_arguments(tmp_path, nb):
     assert run("-i", "2", "--checkpoint-every", "-1", "--checkpoint-prefix", str(tmp_path / "c"), str(src)).returncode == 2
 
 
-REFERENCE_SCENARIOS = "/root/reference/scenarios"
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 @pytest.mark.parametrize("name", ["threebody.json", "test.json"])
 def test_reads_reference_scenario_files(tmp_path, nb, name):
-    """The reference's own scenario files (read in place when the reference tree is present)."""
-    src = os.path.join(REFERENCE_SCENARIOS, name)
-    if not os.path.exists(src):
-        pytest.skip("reference scenarios not present")
+    """The reference's own scenario files (scenarios/*.json), kept as fixtures in tests/golden."""
+    src = os.path.join(GOLDEN, name)
     out = tmp_path / "out.json"
     r = run("-i", "0", "-o", str(out), src)
     assert r.returncode == 0, r.stderr
