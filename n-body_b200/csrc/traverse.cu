@@ -21,12 +21,14 @@
 //      is exact for every target, not a heuristic.
 //   2. Mixed nodes are batched and resolved lane-parallel: each lane takes one node and tests the
 //      32 targets (broadcast from shared memory), producing accept and open masks.
-//   3. Nodes accepted by every target go to a shared list evaluated by all lanes with broadcast
-//      loads; nodes accepted by some targets only go to per-target private lists in shared memory,
-//      evaluated target-major (each lane walks its own list). Opened leaves go to a (leaf, mask)
-//      list evaluated with broadcast body loads. Opened internal nodes push both children.
-// The expensive terms thus run without traversal bookkeeping between them, and the per-node
-// traversal cost is spread over 32 nodes per instruction.
+//   3. Accepted nodes are staged in per-warp shared-memory slabs: the lane that accepted a node
+//      copies its payload there asynchronously (cp.async), so the payload crosses L2 once per
+//      group instead of once per target. Nodes accepted by every target go to the full slab and
+//      are evaluated by all lanes with broadcast reads; nodes accepted by some targets go to the
+//      partial slab with their target masks, and at evaluation a warp bit-matrix transpose of
+//      the masks gives every lane the set of slab entries it owns, which it walks on its own.
+//      Opened leaves go to a (leaf, mask) list evaluated with broadcast body loads; opened
+//      internal nodes push both children.
 //
 // Arithmetic: FP32, one MUFU rsqrt per interaction, G applied once per target. Pair term:
 // 20 flops by the usual direct-sum convention (12 FP32 instructions + rsqrt). Quadrupole node
@@ -44,29 +46,57 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kList = 64;          // capacity of each per-warp list; rounds append at most 32
+constexpr int kList = 64;   // leaf and mixed lists: each round appends at most 32, evaluated above 32
+constexpr int kFullSlab = 32;  // staged nodes accepted by the whole group
+constexpr int kPartSlab = 64;  // staged nodes accepted by some targets only (two 32-entry mask blocks)
 // Stack: kTraverseStack entries per warp. No bound below that size is proven for every tree, so a
 // round whose pushes would not fit abandons its group and sets kErrStackOverflow (the host turns it
 // into an error); every entry on the stack has been written, so no stale entry is ever popped.
-constexpr int kPriv = 32;          // per-target private list of partially accepted nodes
 constexpr unsigned kFull = 0xffffffffu;
 
 enum : int { kNone = 0, kAcceptAll = 1, kOpenAll = 2, kMixed = 3 };
 
-struct WarpLists {
+template<int PAY>
+struct WarpSmem {
     float4 tpos[32];
-    int approx_node[kList];       // nodes accepted by every target of the group
+    float4 full_pay[kFullSlab * PAY];  // payloads of group-wide accepted nodes
+    float4 part_pay[kPartSlab * PAY];  // payloads of partially accepted nodes
+    uint32_t part_mask[kPartSlab];     // their target masks
     int pp_begin[kList], pp_end[kList];
     uint32_t pp_mask[kList];
     int mixed_node[kList];
     uint32_t mixed_mask[kList];
-    int priv[kPriv][32];          // [slot][lane]: nodes accepted by some targets only
 };
+
+template<int ORDER>
+constexpr size_t block_smem_bytes() {
+    return sizeof(WarpSmem<NodeLayout<ORDER>::PAY>) * kWarps;
+}
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
     return m;
+}
+
+// 16-byte asynchronous global -> shared copy (completes at cp_async_wait_all).
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const uint32_t s = (uint32_t) __cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Transpose of the 32 x 32 bit matrix whose row r is lane r's word: afterwards bit r of lane c's
+// word is bit c of row r (five butterfly stages exchanging off-diagonal blocks).
+__device__ __forceinline__ uint32_t transpose32(uint32_t x, int lane) {
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        const uint32_t hi = s == 16 ? 0xFFFF0000u : s == 8 ? 0xFF00FF00u : s == 4 ? 0xF0F0F0F0u
+                          : s == 2 ? 0xCCCCCCCCu : 0xAAAAAAAAu;
+        const uint32_t y = __shfl_xor_sync(kFull, x, s);
+        x = (lane & s) ? ((x & hi) | ((y & hi) >> s)) : ((x & ~hi) | ((y & ~hi) << s));
+    }
+    return x;
 }
 
 // Squared distance in the reference's IEEE order: (dx*dx + dy*dy) + dz*dz, d = p - c.
@@ -110,79 +140,75 @@ __device__ __forceinline__ void quad_term(float4 p, float4 com, float4 q0, float
     az = fmaf(rz, sr, fmaf(qz, sq, az));
 }
 
-// Warp-wide ordered append: returns this lane's slot (valid where pred) and advances count.
-__device__ __forceinline__ int warp_append(bool pred, int &count, uint32_t lt) {
-    const uint32_t b = __ballot_sync(kFull, pred);
-    const int pos = count + __popc(b & lt);
-    count += __popc(b);
-    return pos;
-}
-
+// Node term from a staged payload (PAY float4 in shared memory).
 template<int ORDER, bool EPS0>
-__device__ __forceinline__ void node_term(const float4 *__restrict__ pay, int c, float4 p, float eps, float &ax,
-                                          float &ay, float &az) {
-    constexpr int PAY = NodeLayout<ORDER>::PAY;
-    const float4 *pc = pay + (int64_t) c * PAY;
+__device__ __forceinline__ void staged_term(const float4 *pc, float4 p, float eps, float &ax, float &ay, float &az) {
     if constexpr (ORDER == 1) {
-        pair_term<EPS0>(p, __ldg(pc), eps, ax, ay, az);
+        pair_term<EPS0>(p, pc[0], eps, ax, ay, az);
     } else {
-        quad_term<EPS0>(p, __ldg(pc), __ldg(pc + 1), __ldg(pc + 2), eps, ax, ay, az);
+        quad_term<EPS0>(p, pc[0], pc[1], pc[2], eps, ax, ay, az);
     }
 }
 
-// Nodes accepted by the whole group: every lane evaluates every entry (broadcast loads).
+template<int PAY>
+__device__ __forceinline__ void stage_node(float4 *dst, const float4 *__restrict__ pay, int c) {
+    const float4 *src = pay + (int64_t) c * PAY;
+#pragma unroll
+    for (int k = 0; k < PAY; ++k) cp_async16(dst + k, src + k);
+}
+
+// Nodes accepted by the whole group: every lane evaluates every staged entry (broadcast reads).
 template<int ORDER, bool EPS0>
-__device__ __forceinline__ void flush_approx(WarpLists &L, int &napprox, const float4 *__restrict__ pay, float4 p,
-                                             float eps, float &ax, float &ay, float &az, unsigned &cnp) {
+__device__ __forceinline__ void flush_full(WarpSmem<NodeLayout<ORDER>::PAY> &S, int &nfull, float4 p, float eps,
+                                           float &ax, float &ay, float &az, unsigned &cnp) {
+    constexpr int PAY = NodeLayout<ORDER>::PAY;
+    cp_async_wait_all();
+    __syncwarp();
     int j = 0;
-    for (; j + 1 < napprox; j += 2) {
-        const int c0 = L.approx_node[j], c1 = L.approx_node[j + 1];
-        node_term<ORDER, EPS0>(pay, c0, p, eps, ax, ay, az);
-        node_term<ORDER, EPS0>(pay, c1, p, eps, ax, ay, az);
+    for (; j + 1 < nfull; j += 2) {
+        staged_term<ORDER, EPS0>(S.full_pay + j * PAY, p, eps, ax, ay, az);
+        staged_term<ORDER, EPS0>(S.full_pay + (j + 1) * PAY, p, eps, ax, ay, az);
     }
-    if (j < napprox) node_term<ORDER, EPS0>(pay, L.approx_node[j], p, eps, ax, ay, az);
-    cnp += (unsigned) napprox;
-    napprox = 0;
+    if (j < nfull) staged_term<ORDER, EPS0>(S.full_pay + j * PAY, p, eps, ax, ay, az);
+    cnp += (unsigned) nfull;
+    nfull = 0;
     __syncwarp();
 }
 
-// Nodes accepted by some targets only: each lane walks its own list (target-major).
+// Nodes accepted by some targets only: the masks are transposed so that each lane holds the set
+// of entries it evaluates, then every lane walks its own set.
 template<int ORDER, bool EPS0>
-__device__ __forceinline__ void flush_private(WarpLists &L, int &npriv, const float4 *__restrict__ pay, float4 p,
-                                              float eps, int lane, float &ax, float &ay, float &az, unsigned &cnp) {
-    const int most = __reduce_max_sync(kFull, npriv);
-    for (int k = 0; k < most; ++k) {
-        if (k < npriv) node_term<ORDER, EPS0>(pay, L.priv[k][lane], p, eps, ax, ay, az);
+__device__ __forceinline__ void flush_part(WarpSmem<NodeLayout<ORDER>::PAY> &S, int &npart, float4 p, float eps,
+                                           int lane, float &ax, float &ay, float &az, unsigned &cnp) {
+    constexpr int PAY = NodeLayout<ORDER>::PAY;
+    cp_async_wait_all();
+    __syncwarp();
+    uint32_t b0 = transpose32(lane < npart ? S.part_mask[lane] : 0u, lane);
+    uint32_t b1 = npart > 32 ? transpose32(lane + 32 < npart ? S.part_mask[lane + 32] : 0u, lane) : 0u;
+    cnp += (unsigned) (__popc(b0) + __popc(b1));
+    while (__any_sync(kFull, (b0 | b1) != 0u)) {
+        if (b0 | b1) {
+            int j;
+            if (b0) {
+                j = __ffs(b0) - 1;
+                b0 &= b0 - 1;
+            } else {
+                j = 31 + __ffs(b1);
+                b1 &= b1 - 1;
+            }
+            staged_term<ORDER, EPS0>(S.part_pay + j * PAY, p, eps, ax, ay, az);
+        }
     }
-    cnp += (unsigned) npriv;
-    npriv = 0;
+    npart = 0;
     __syncwarp();
 }
 
-// Partially accepted entries (node c_i with target mask A_i in lane i) go to the private lists
-// of the targets in A_i; a full list is evaluated before it would overflow.
-template<int ORDER, bool EPS0>
-__device__ __forceinline__ void append_private(WarpLists &L, int &npriv, bool partial, int c, uint32_t A,
-                                               const float4 *__restrict__ pay, float4 p, float eps, int lane,
-                                               float &ax, float &ay, float &az, unsigned &cnp) {
-    uint32_t pend = __ballot_sync(kFull, partial);
-    while (pend) {
-        const int src = __ffs(pend) - 1;
-        pend &= pend - 1;
-        const int node = __shfl_sync(kFull, c, src);
-        const uint32_t mask = __shfl_sync(kFull, A, src);
-        if (__any_sync(kFull, npriv == kPriv)) flush_private<ORDER, EPS0>(L, npriv, pay, p, eps, lane, ax, ay, az, cnp);
-        if ((mask >> lane) & 1u) L.priv[npriv++][lane] = node;
-    }
-    __syncwarp();
-}
-
-template<bool EPS0>
-__device__ __forceinline__ void flush_pp(WarpLists &L, int &npp, const float4 *__restrict__ bodies, float4 p,
+template<bool EPS0, int PAY>
+__device__ __forceinline__ void flush_pp(WarpSmem<PAY> &S, int &npp, const float4 *__restrict__ bodies, float4 p,
                                          float eps, int lane, float &ax, float &ay, float &az, unsigned &cpp) {
     for (int j = 0; j < npp; ++j) {
-        const int b = L.pp_begin[j], e = L.pp_end[j];
-        const bool on = (L.pp_mask[j] >> lane) & 1u;
+        const int b = S.pp_begin[j], e = S.pp_end[j];
+        const bool on = (S.pp_mask[j] >> lane) & 1u;
         int k = b;
         for (; k + 3 < e; k += 4) {
             const float4 s0 = __ldg(bodies + k), s1 = __ldg(bodies + k + 1);
@@ -204,19 +230,84 @@ __device__ __forceinline__ void flush_pp(WarpLists &L, int &npp, const float4 *_
     __syncwarp();
 }
 
+// Classified entries of one round, appended to the slabs and lists (warp-uniform control flow):
+// acc / part are accepted nodes (target mask mk for part), leaf is an opened leaf (body range
+// l0..l1, mask mk), open an opened internal node (children c + 1 and l0, mask mk), mixed a node
+// still to be resolved per target.
 template<int ORDER, bool EPS0>
-__global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const int *__restrict__ num_nodes_p,
-                                                      const float4 *__restrict__ bodies, int n_bodies,
-                                                      const float4 *__restrict__ targets, int n_targets, float G,
-                                                      float eps, float4 *__restrict__ acc,
-                                                      unsigned long long *__restrict__ counts,
-                                                      int2 *__restrict__ stack_base, unsigned *__restrict__ group_counter,
-                                                      uint32_t *__restrict__ err, const int4 *__restrict__ groups,
-                                                      int num_group_tasks, const int *__restrict__ inst_root,
-                                                      unsigned long long *__restrict__ inst_counts) {
-    __shared__ WarpLists lists[kWarps];
+__device__ __forceinline__ bool dispatch(WarpSmem<NodeLayout<ORDER>::PAY> &S, const float4 *__restrict__ pay,
+                                         const float4 *__restrict__ bodies, int2 *stack, bool acc, bool part,
+                                         bool leaf, bool open, bool mixed, int c, uint32_t mk, int l0, int l1,
+                                         int n_bodies, uint32_t lt, int lane, int &nfull, int &npart, int &npp,
+                                         int &nmixed, int &top, float4 p, float eps, float &ax, float &ay, float &az,
+                                         unsigned &gnp, unsigned &gpp, uint32_t *err) {
+    constexpr int PAY = NodeLayout<ORDER>::PAY;
+    uint32_t b = __ballot_sync(kFull, acc);
+    if (b) {
+        if (nfull + __popc(b) > kFullSlab) flush_full<ORDER, EPS0>(S, nfull, p, eps, ax, ay, az, gnp);
+        if (acc) stage_node<PAY>(S.full_pay + (nfull + __popc(b & lt)) * PAY, pay, c);
+        nfull += __popc(b);
+    }
+    b = __ballot_sync(kFull, part);
+    if (b) {
+        if (npart + __popc(b) > kPartSlab) flush_part<ORDER, EPS0>(S, npart, p, eps, lane, ax, ay, az, gnp);
+        if (part) {
+            const int slot = npart + __popc(b & lt);
+            stage_node<PAY>(S.part_pay + slot * PAY, pay, c);
+            S.part_mask[slot] = mk;
+        }
+        npart += __popc(b);
+    }
+    b = __ballot_sync(kFull, leaf);
+    if (leaf) {
+        const int pos = npp + __popc(b & lt);
+        S.pp_begin[pos] = max(l0, 0);
+        S.pp_end[pos] = min(l1, n_bodies);
+        S.pp_mask[pos] = mk;
+    }
+    npp += __popc(b);
+    b = __ballot_sync(kFull, mixed);
+    if (mixed) {
+        const int pos = nmixed + __popc(b & lt);
+        S.mixed_node[pos] = c;
+        S.mixed_mask[pos] = mk;
+    }
+    nmixed += __popc(b);
+    b = __ballot_sync(kFull, open);
+    bool abandoned = false;
+    if (top + 2 * __popc(b) > kTraverseStack) {
+        // a push would not fit: the group is abandoned with an error (warp-uniform)
+        if (lane == 0) atomicOr(err, (uint32_t) kErrStackOverflow);
+        abandoned = true;
+    } else {
+        if (open) {
+            const int sp = top + 2 * __popc(b & lt);
+            stack[sp] = make_int2(l0, (int) mk);         // right child
+            stack[sp + 1] = make_int2(c + 1, (int) mk);  // left child, popped first
+        }
+        top += 2 * __popc(b);
+    }
+    __syncwarp();
+    // each round appends at most 32 leaves: evaluate before the next one could overflow the list
+    if (npp > kList - 32) flush_pp<EPS0>(S, npp, bodies, p, eps, lane, ax, ay, az, gpp);
+    return abandoned;
+}
+
+template<int ORDER, bool EPS0>
+__global__ void __launch_bounds__(kThreads, 4) bh_kernel(NodeArrays nodes, const int *__restrict__ num_nodes_p,
+                                                         const float4 *__restrict__ bodies, int n_bodies,
+                                                         const float4 *__restrict__ targets, int n_targets, float G,
+                                                         float eps, float4 *__restrict__ acc,
+                                                         unsigned long long *__restrict__ counts,
+                                                         int2 *__restrict__ stack_base,
+                                                         unsigned *__restrict__ group_counter,
+                                                         uint32_t *__restrict__ err, const int4 *__restrict__ groups,
+                                                         int num_group_tasks, const int *__restrict__ inst_root,
+                                                         unsigned long long *__restrict__ inst_counts) {
+    constexpr int PAY = NodeLayout<ORDER>::PAY;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    WarpLists &L = lists[warp];
+    WarpSmem<PAY> &S = reinterpret_cast<WarpSmem<PAY> *>(smem_raw)[warp];
     int2 *stack = stack_base + ((int64_t) blockIdx.x * kWarps + warp) * kTraverseStack;
     const float4 *__restrict__ mac = nodes.mac;
     const int2 *__restrict__ link = nodes.link;
@@ -256,8 +347,8 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
                 hi[k] = fmaxf(hi[k], __shfl_xor_sync(kFull, hi[k], o));
             }
         }
-        L.tpos[lane] = p;
-        int top = 0, napprox = 0, npp = 0, nmixed = 0, npriv = 0;
+        S.tpos[lane] = p;
+        int top = 0, nfull = 0, npart = 0, npp = 0, nmixed = 0;
         if (num_nodes > 0 && root >= 0 && root < num_nodes) {
             if (lane == 0) stack[0] = make_int2(root, (int) full);
             top = 1;
@@ -304,42 +395,16 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
                     else cls = kMixed;
                 }
                 __syncwarp();  // popped entries are read before children overwrite them
-                const bool is_acc = cls == kAcceptAll && m == full;
-                const bool is_acc_part = cls == kAcceptAll && m != full;
                 const bool is_leaf_open = cls == kOpenAll && l1 >= 0;
                 const bool is_int_open = cls == kOpenAll && l1 < 0 && l0 > c + 1 && l0 < num_nodes;
                 if (cls == kOpenAll && l1 < 0 && !is_int_open) atomicOr(err, (uint32_t) kErrTraverseLimit);
-                const bool is_mix = cls == kMixed;
-                int pos = warp_append(is_acc, napprox, lt);
-                if (is_acc) L.approx_node[pos] = c;
-                append_private<ORDER, EPS0>(L, npriv, is_acc_part, c, m, pay, p, eps, lane, ax, ay, az, gnp);
-                pos = warp_append(is_leaf_open, npp, lt);
-                if (is_leaf_open) {
-                    L.pp_begin[pos] = max(l0, 0);
-                    L.pp_end[pos] = min(l1, n_bodies);
-                    L.pp_mask[pos] = m;
-                }
-                pos = warp_append(is_mix, nmixed, lt);
-                if (is_mix) { L.mixed_node[pos] = c; L.mixed_mask[pos] = m; }
-                const uint32_t bi = __ballot_sync(kFull, is_int_open);
-                if (top + 2 * __popc(bi) > kTraverseStack) {
-                    // warp-uniform: a push would not fit, so the group is abandoned with an error
-                    // (every entry on the stack was written; nothing unwritten is ever popped)
-                    if (lane == 0) atomicOr(err, (uint32_t) kErrStackOverflow);
+                if (dispatch<ORDER, EPS0>(S, pay, bodies, stack, cls == kAcceptAll && m == full,
+                                          cls == kAcceptAll && m != full, is_leaf_open, is_int_open, cls == kMixed,
+                                          c, m, l0, l1, n_bodies, lt, lane, nfull, npart, npp, nmixed, top, p, eps,
+                                          ax, ay, az, gnp, gpp, err)) {
                     top = 0;
                     nmixed = 0;
-                } else {
-                    if (is_int_open) {
-                        const int sp = top + 2 * __popc(bi & lt);
-                        stack[sp] = make_int2(l0, (int) m);         // right child
-                        stack[sp + 1] = make_int2(c + 1, (int) m);  // left child, popped first
-                    }
-                    top += 2 * __popc(bi);
                 }
-                __syncwarp();
-                // each round appends at most 32 entries per list: evaluate before the next one
-                if (napprox > kList - 32) flush_approx<ORDER, EPS0>(L, napprox, pay, p, eps, ax, ay, az, gnp);
-                if (npp > kList - 32) flush_pp<EPS0>(L, npp, bodies, p, eps, lane, ax, ay, az, gpp);
             }
             if (nmixed >= 32 || (top == 0 && nmixed > 0)) {
                 // ---- 2. resolve up to 32 mixed nodes: per-target MAC, lane-parallel over nodes ----
@@ -349,8 +414,8 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
                 int c = 0, l0 = 0, l1 = -1;
                 uint32_t A = 0, O = 0;
                 if (lane < k) {
-                    c = L.mixed_node[base + lane];
-                    const uint32_t m = L.mixed_mask[base + lane];
+                    c = S.mixed_node[base + lane];
+                    const uint32_t m = S.mixed_mask[base + lane];
                     const float4 mc = __ldg(mac + c);
                     const int2 lk = __ldg(link + c);
                     l0 = lk.x;
@@ -358,48 +423,32 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
                     uint32_t bits = 0;
 #pragma unroll 8
                     for (int t = 0; t < 32; ++t) {
-                        const float4 tp = L.tpos[t];
+                        const float4 tp = S.tpos[t];
                         bits |= (ref_dist2(tp.x, tp.y, tp.z, mc) >= mc.w) ? (1u << t) : 0u;
                     }
                     A = bits & m;
                     O = m & ~A;
                 }
                 __syncwarp();
-                const bool is_acc = A != 0 && A == full;
-                const bool is_acc_part = A != 0 && A != full;
-                const bool is_leaf_open = O != 0 && l1 >= 0;
                 const bool is_int_open = O != 0 && l1 < 0 && l0 > c + 1 && l0 < num_nodes;
                 if (O != 0 && l1 < 0 && !is_int_open) atomicOr(err, (uint32_t) kErrTraverseLimit);
-                int pos = warp_append(is_acc, napprox, lt);
-                if (is_acc) L.approx_node[pos] = c;
-                append_private<ORDER, EPS0>(L, npriv, is_acc_part, c, A, pay, p, eps, lane, ax, ay, az, gnp);
-                pos = warp_append(is_leaf_open, npp, lt);
-                if (is_leaf_open) {
-                    L.pp_begin[pos] = max(l0, 0);
-                    L.pp_end[pos] = min(l1, n_bodies);
-                    L.pp_mask[pos] = O;
-                }
-                const uint32_t bi = __ballot_sync(kFull, is_int_open);
-                if (top + 2 * __popc(bi) > kTraverseStack) {
-                    if (lane == 0) atomicOr(err, (uint32_t) kErrStackOverflow);
+                const bool is_acc = A != 0 && A == full;
+                const bool is_part = A != 0 && A != full;
+                // an entry can be accepted by some targets and opened by others: append both parts
+                if (dispatch<ORDER, EPS0>(S, pay, bodies, stack, is_acc, is_part, false, false, false, c, A, l0,
+                                          l1, n_bodies, lt, lane, nfull, npart, npp, nmixed, top, p, eps, ax, ay,
+                                          az, gnp, gpp, err) ||
+                    dispatch<ORDER, EPS0>(S, pay, bodies, stack, false, false, O != 0 && l1 >= 0, is_int_open, false,
+                                          c, O, l0, l1, n_bodies, lt, lane, nfull, npart, npp, nmixed, top, p, eps,
+                                          ax, ay, az, gnp, gpp, err)) {
                     top = 0;
                     nmixed = 0;
-                } else {
-                    if (is_int_open) {
-                        const int sp = top + 2 * __popc(bi & lt);
-                        stack[sp] = make_int2(l0, (int) O);
-                        stack[sp + 1] = make_int2(c + 1, (int) O);
-                    }
-                    top += 2 * __popc(bi);
                 }
-                __syncwarp();
-                if (napprox > kList - 32) flush_approx<ORDER, EPS0>(L, napprox, pay, p, eps, ax, ay, az, gnp);
-                if (npp > kList - 32) flush_pp<EPS0>(L, npp, bodies, p, eps, lane, ax, ay, az, gpp);
             }
         }
-        flush_approx<ORDER, EPS0>(L, napprox, pay, p, eps, ax, ay, az, gnp);
-        flush_private<ORDER, EPS0>(L, npriv, pay, p, eps, lane, ax, ay, az, gnp);
-        flush_pp<EPS0>(L, npp, bodies, p, eps, lane, ax, ay, az, gpp);
+        flush_full<ORDER, EPS0>(S, nfull, p, eps, ax, ay, az, gnp);
+        flush_part<ORDER, EPS0>(S, npart, p, eps, lane, ax, ay, az, gnp);
+        flush_pp<EPS0>(S, npp, bodies, p, eps, lane, ax, ay, az, gpp);
         if (valid) acc[i] = make_float4(G * ax, G * ay, G * az, 0.f);
         if (valid) {
             cnp += gnp;
@@ -426,15 +475,21 @@ __global__ void __launch_bounds__(kThreads) bh_kernel(NodeArrays nodes, const in
 }
 
 // Occupancy and SM count are fixed per device and kernel: queried once (B200 parts are identical).
+// The kernel's dynamic shared memory (the warps' slabs and lists) is enabled on first use.
 template<int ORDER, bool EPS0>
-int blocks_per_sm() {
-    static int cached = 0;
-    if (cached == 0) {
+int blocks_per_sm(int device) {
+    static int cached[64] = {0};
+    if (device < 0 || device >= 64) device = 0;
+    if (cached[device] == 0) {
+        const size_t smem = block_smem_bytes<ORDER>();
+        cudaFuncSetAttribute(bh_kernel<ORDER, EPS0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+        cudaFuncSetAttribute(bh_kernel<ORDER, EPS0>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
         int b = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, bh_kernel<ORDER, EPS0>, kThreads, 0);
-        cached = b > 0 ? b : 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, bh_kernel<ORDER, EPS0>, kThreads, smem);
+        cached[device] = b > 0 ? b : 1;
     }
-    return cached;
+    return cached[device];
 }
 
 template<int ORDER, bool EPS0>
@@ -444,15 +499,15 @@ void launch_variant(const NodeArrays &nodes, const int *num_nodes, const float4 
                     const int *inst_root, unsigned long long *inst_counts) {
     int device = 0;
     cudaGetDevice(&device);
-    int64_t blocks = (int64_t) sm_count(device) * blocks_per_sm<ORDER, EPS0>();
+    int64_t blocks = (int64_t) sm_count(device) * blocks_per_sm<ORDER, EPS0>(device);
     blocks = std::min<int64_t>(blocks, ws.warps / kWarps);
     const int64_t groups = gtab ? ngroups : (nt + 31) / 32;
     blocks = std::min<int64_t>(blocks, (groups + kWarps - 1) / kWarps);
     if (blocks < 1) blocks = 1;
     cudaMemsetAsync(ws.group_counter, 0, sizeof(unsigned), s);
-    bh_kernel<ORDER, EPS0><<<(unsigned) blocks, kThreads, 0, s>>>(nodes, num_nodes, bodies, n_bodies, targets, nt, G,
-                                                                   eps, acc, counts, ws.stack, ws.group_counter, err,
-                                                                   gtab, (int) ngroups, inst_root, inst_counts);
+    bh_kernel<ORDER, EPS0><<<(unsigned) blocks, kThreads, block_smem_bytes<ORDER>(), s>>>(
+        nodes, num_nodes, bodies, n_bodies, targets, nt, G, eps, acc, counts, ws.stack, ws.group_counter, err, gtab,
+        (int) ngroups, inst_root, inst_counts);
 }
 
 }  // namespace
@@ -475,8 +530,8 @@ int current_sm_count() {
 }
 
 int64_t traverse_resident_warps(int device) {
-    int b = std::max(std::max(blocks_per_sm<1, false>(), blocks_per_sm<1, true>()),
-                     std::max(blocks_per_sm<2, false>(), blocks_per_sm<2, true>()));
+    int b = std::max(std::max(blocks_per_sm<1, false>(device), blocks_per_sm<1, true>(device)),
+                     std::max(blocks_per_sm<2, false>(device), blocks_per_sm<2, true>(device)));
     return (int64_t) sm_count(device) * b * kWarps;
 }
 
