@@ -319,6 +319,10 @@ def _run_ours_on_stream(args, torch, nb, pm, vel, eps, stream, world, rank, devi
     solver = nb.QuadrupoleLinearBVHSolver(bodies=pm, rule=nb.Gravity(1.0, eps), velocities=vel, theta=THETA,
                                           max_leaf_size=LEAF, time_step=DT, device=device)
     solver.set_stream(stream.cuda_stream)
+    # the traversal's launch shape at the configured leaf size, measured on these bodies
+    from nbody_b200 import autotune as at
+
+    shape, shape_ms = at.tune_shape(solver, passes=3)
     acc_info = accuracy(nb, solver, pm, eps, torch, torch.device("cuda", device))
     counts = solver.counts()
     solver.set_bodies(pm, vel)
@@ -396,6 +400,9 @@ def _run_ours_on_stream(args, torch, nb, pm, vel, eps, stream, world, rank, devi
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Plummer sphere)",
         "config": workload_config(args),
+        "autotune": {"traversal_shape": list(shape), "ms_per_force_pass_by_shape": shape_ms,
+                     "method": "force passes at each launch shape (threads per block x traversal tile) at the "
+                               "configured leaf size 16, fastest kept"},
         "e2e": {"value": e2e_value, "unit": "body-steps/s", "h2d_bytes_per_step": 32 * args.n,
                 "d2h_bytes_per_step": 32 * args.n, "steps": args.e2e_steps,
                 "path": "nb_set_bodies (pinned host) + nb_step + nb_get_bodies, wall clock"},
@@ -589,10 +596,12 @@ def run_batched(args):
                                          device=device)
         s.set_stream(stream.cuda_stream)
         s.set_instances(sizes, np.concatenate(bodies), np.concatenate(vels), thetas)
-        # leaf size measured on this batch (force passes only: the state does not change)
-        tuned = s.autotune(candidates=(4, 6, 8, 12, 16, 24), passes=2)
-        leaf = tuned.leaf
+        # leaf size and traversal launch shape measured on this batch (force passes only: the
+        # state does not change)
+        tuned = s.autotune(candidates=(4, 6, 8, 12, 16, 24), passes=2, tolerance=0.02)
+        leaf, shape = tuned.leaf, tuned.shape
         accuracy = batched_accuracy(nb, s, sizes, bodies, eps, torch, device)
+        batch_acc = s.update_accelerations()
         s.enable_graphs(True)
         s.step(max(args.warmup, 3))
         torch.cuda.synchronize(device)
@@ -608,13 +617,19 @@ def run_batched(args):
         s.step(2)
         phases = s.phase_times()
         s.close()
-        # the same instances, one after another, through the plain path (one context each)
+        # the same instances, one after another, through the plain path (one context each, same
+        # theta, leaf size and launch shape: every instance's accelerations are bit-identical to the
+        # batch's, so the two runs are at equal accuracy by construction; checked below)
         ctxs = []
+        starts = np.concatenate([[0], np.cumsum(sizes)])
+        identical = True
         for k in range(len(sizes)):
             c = nb.QuadrupoleLinearBVHSolver(bodies=bodies[k], velocities=vels[k], rule=nb.Gravity(1.0, eps),
                                              theta=float(thetas[k]), max_leaf_size=leaf, time_step=BATCH_DT,
                                              device=device)
             c.set_stream(stream.cuda_stream)
+            c.traversal_shape = shape
+            identical &= bool(np.array_equal(c.update_accelerations(), batch_acc[starts[k]:starts[k + 1]]))
             c.step(1)
             ctxs.append(c)
         seq_steps = max(1, min(args.steps, 5))
@@ -641,9 +656,15 @@ def run_batched(args):
                    "softening": BATCH_SOFTENING, "leaf_size": leaf, "order": ORDER, "dt": BATCH_DT,
                    "graphs": "two steps per CUDA graph", "l2": "flushed (256 MB write) before the timed steps"},
         "sequential_plain_path": {"value": seq_value, "unit": "body-steps/s", "steps": seq_steps,
-                                  "leaf_size": leaf, "ratio_batched_over_sequential": value / seq_value},
+                                  "leaf_size": leaf, "traversal_shape": list(shape),
+                                  "ratio_batched_over_sequential": value / seq_value,
+                                  "accelerations_bit_identical_to_batch": identical,
+                                  "accuracy": "equal: the same instances with the same theta, leaf size and launch "
+                                              "shape give bit-identical accelerations (force RMS as in accuracy)"},
         "autotune": {"leaf_size": leaf, "ms_per_force_pass": {str(k): v for k, v in tuned.timings_ms.items()},
-                     "method": "force passes of this batch at each candidate leaf size, fastest kept"},
+                     "traversal_shape": list(shape), "ms_per_force_pass_by_shape": tuned.shape_timings_ms,
+                     "method": "force passes of this batch at each candidate leaf size (default launch shape), "
+                               "then at each launch shape (threads per block x traversal tile), fastest kept"},
         "accuracy": accuracy,
         "phases_ms_per_step": {k: phases[k] / max(phases["passes"], 1) for k in
                                ("bbox_ms", "morton_ms", "sort_ms", "gather_ms", "build_ms", "traverse_ms",
@@ -694,7 +715,7 @@ def serving_pools(seed=45, n_max=1 << 21):
 
 
 def serve_run(nb, pools, rate, duration, rng, eps, steps_range=(10, 1000), n_range=(2048, 1 << 21),
-              budget=150 * 10 ** 9, drain=0.0, leaf=LEAF):
+              budget=150 * 10 ** 9, drain=0.0, leaf=LEAF, shape=(256, 64)):
     """Open-loop Poisson arrivals for `duration` seconds (then `drain` more seconds of ticks).
     Latency = completion time - arrival time, wall clock."""
     arrivals = []
@@ -707,6 +728,7 @@ def serve_run(nb, pools, rate, duration, rng, eps, steps_range=(10, 1000), n_ran
         arrivals.append((t, n, steps, theta, pm, vel))
         t += rng.exponential(1.0 / rate)
     sv = nb.Server(rule=nb.Gravity(1.0, eps), order=ORDER, max_leaf_size=leaf, time_step=DT, hbm_budget_bytes=budget)
+    sv.set_traversal_shape(shape)
     pending = {}  # id -> (arrival time, bodies)
     latencies = []
     t0 = time.perf_counter()
@@ -761,7 +783,7 @@ def serving_sample(pools, requests=64, seed=47):
 
 
 def serving_leaf(nb, sample, eps):
-    """Leaf size for the server, measured on the sample batch of requests."""
+    """Leaf size and traversal launch shape for the server, measured on the sample batch of requests."""
     sizes, bodies, thetas = sample
     with nb.QuadrupoleLinearBVHSolver(rule=nb.Gravity(1.0, eps), time_step=DT) as s:
         s.set_instances(sizes, np.concatenate([b[0] for b in bodies]), thetas=np.asarray(thetas, np.float32))
@@ -769,7 +791,7 @@ def serving_leaf(nb, sample, eps):
     return tuned.leaf, tuned
 
 
-def serving_sample_vs_sequential(nb, sample, eps, leaf, torch, steps=2):
+def serving_sample_vs_sequential(nb, sample, eps, leaf, torch, steps=2, shape=(256, 64)):
     """The sample batch advanced together (one batched step per tick, as the server runs it) against
     the same requests advanced one after another through the plain single-instance path, on the
     device clock. Both run the same steps of the same bodies, with identical results."""
@@ -780,6 +802,7 @@ def serving_sample_vs_sequential(nb, sample, eps, leaf, torch, steps=2):
     t1 = torch.cuda.Event(enable_timing=True)
     with nb.QuadrupoleLinearBVHSolver(rule=nb.Gravity(1.0, eps), max_leaf_size=leaf, time_step=DT) as s:
         s.set_stream(stream.cuda_stream)
+        s.traversal_shape = shape
         s.set_instances(sizes, np.concatenate([b[0] for b in bodies]), np.concatenate([b[1] for b in bodies]),
                         np.asarray(thetas, np.float32))
         s.step(3)
@@ -794,6 +817,7 @@ def serving_sample_vs_sequential(nb, sample, eps, leaf, torch, steps=2):
         with nb.QuadrupoleLinearBVHSolver(bodies=pm, velocities=vel, rule=nb.Gravity(1.0, eps), theta=theta,
                                           max_leaf_size=leaf, time_step=DT) as c:
             c.set_stream(stream.cuda_stream)
+            c.traversal_shape = shape
             c.step(1)
             torch.cuda.synchronize()
             t0.record(stream)
@@ -804,6 +828,7 @@ def serving_sample_vs_sequential(nb, sample, eps, leaf, torch, steps=2):
     batched = total * steps / (batched_ms / 1000.0)
     sequential = total * steps / (seq_ms / 1000.0)
     return {"requests": len(sizes), "total_bodies": total, "steps": steps, "leaf_size": leaf,
+            "traversal_shape": list(shape),
             "batched_body_steps_per_s": batched, "sequential_plain_body_steps_per_s": sequential,
             "ratio_batched_over_sequential": batched / sequential,
             "ratio_served_over_sequential": None}
@@ -821,15 +846,16 @@ def run_serving(args):
     rng = np.random.default_rng(46 + rank)
     sample = serving_sample(pools)
     leaf, tuned = serving_leaf(nb, sample, eps)
-    versus = serving_sample_vs_sequential(nb, sample, eps, leaf, torch)
-    overload = serve_run(nb, pools, args.rate, args.duration, rng, eps, leaf=leaf)
+    shape = tuned.shape
+    versus = serving_sample_vs_sequential(nb, sample, eps, leaf, torch, shape=shape)
+    overload = serve_run(nb, pools, args.rate, args.duration, rng, eps, leaf=leaf, shape=shape)
     # the server's own throughput (re-layouts, admission and retirement included) on the stream
     versus["ratio_served_over_sequential"] = (overload["throughput_body_steps_per_s"] /
                                               versus["sequential_plain_body_steps_per_s"])
     # calibrated run: arrival rate at 70 % of the measured capacity for the mean request size
     mean_work = np.mean([np.exp(rng.uniform(np.log(2048), np.log(1 << 21))) for _ in range(20000)]) * 505.0
     rate = max(0.7 * overload["throughput_body_steps_per_s"] / mean_work, 0.05)
-    calibrated = serve_run(nb, pools, rate, args.duration, rng, eps, drain=args.duration, leaf=leaf)
+    calibrated = serve_run(nb, pools, rate, args.duration, rng, eps, drain=args.duration, leaf=leaf, shape=shape)
     line = {
         "metric": "serving: aggregate body-steps/s and request latency p50/p99 (Poisson arrivals)",
         "value": overload["throughput_body_steps_per_s"], "unit": "body-steps/s", "n_gpus": world,
@@ -839,7 +865,9 @@ def run_serving(args):
                    "theta_range": [0.4, 0.7], "softening": BATCH_SOFTENING, "hbm_budget_bytes": 150 * 10 ** 9,
                    "order": ORDER, "leaf_size": leaf},
         "autotune": {"leaf_size": leaf, "ms_per_force_pass": {str(k): v for k, v in tuned.timings_ms.items()},
-                     "method": "force passes of a 64-request sample batch at each candidate leaf size"},
+                     "traversal_shape": list(shape), "ms_per_force_pass_by_shape": tuned.shape_timings_ms,
+                     "method": "force passes of a 64-request sample batch at each candidate leaf size, then at "
+                               "each launch shape"},
         "sample_batch_vs_sequential": versus,
         "overload_run": overload,
         "calibrated_run": calibrated,

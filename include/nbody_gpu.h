@@ -184,6 +184,15 @@ int nb_enable_graphs(nb_ctx *ctx, int enable);
  * of those nodes are no longer bit-identical to the reference's FP32 ones. */
 int nb_set_fp64_summaries(nb_ctx *ctx, int64_t min_bodies);
 
+/* Launch shape of the Barnes-Hut traversal (no counterpart in the reference, whose TBB loop has no
+ * such knob; LinearBVH::maxLeafSize, LinearBVH.h:135-137, is the one it has): block_threads
+ * threads per block (128 or 256) and slab_entries staged partially accepted nodes per warp (32 or
+ * 64); 0 selects the default (256, 64). Decisions and interaction counts do not depend on it;
+ * accelerations sum the same terms, possibly in another order. The autotuner
+ * (nbody_b200/autotune.py) picks it per workload. */
+int nb_set_traversal_shape(nb_ctx *ctx, int32_t block_threads, int32_t slab_entries);
+int nb_get_traversal_shape(const nb_ctx *ctx, int32_t *block_threads, int32_t *slab_entries);
+
 /* Target sharding of one instance over `world` processes, one GPU each (the path shards over
  * targets; every rank needs all sources). Every rank holds the same state.
  * A force pass still sorts and builds over all bodies, but evaluates accelerations, and nb_step

@@ -1209,6 +1209,25 @@ int nb_set_fp64_summaries(nb_ctx *ctx, int64_t min_bodies) {
     return NB_OK;
 }
 
+int nb_set_traversal_shape(nb_ctx *ctx, int32_t block_threads, int32_t slab_entries) {
+    if (!ctx) return NB_ERR_INVALID_ARGUMENT;
+    if (block_threads == 0) block_threads = 256;
+    if (slab_entries == 0) slab_entries = 64;
+    if (!traversal_shape_valid(block_threads, slab_entries))
+        return fail(ctx, NB_ERR_INVALID_ARGUMENT, "traversal shape: block of 128 or 256 threads, slab of 32 or 64");
+    ctx->trav.threads = block_threads;
+    ctx->trav.slab = slab_entries;
+    drop_graph(ctx);  // captured passes hold the old launch shape
+    return NB_OK;
+}
+
+int nb_get_traversal_shape(const nb_ctx *ctx, int32_t *block_threads, int32_t *slab_entries) {
+    if (!ctx || !block_threads || !slab_entries) return NB_ERR_INVALID_ARGUMENT;
+    *block_threads = ctx->trav.threads;
+    *slab_entries = ctx->trav.slab;
+    return NB_OK;
+}
+
 int nb_shard_range(int64_t n, int32_t rank, int32_t world, int64_t *chunk, int64_t *first, int64_t *count) {
     if (n < 0 || world < 1 || rank < 0 || rank >= world || !chunk || !first || !count)
         return NB_ERR_INVALID_ARGUMENT;

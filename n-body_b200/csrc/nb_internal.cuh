@@ -245,7 +245,11 @@ struct TraverseWorkspace {
     int2 *stack = nullptr;            // per resident warp: kTraverseStack entries of (node, target mask)
     unsigned *group_counter = nullptr;
     int64_t warps = 0;                // resident warps the stack memory was sized for
+    int threads = 256;                // launch shape: threads per block (128 or 256)
+    int slab = 64;                    // launch shape: partial-accept slab entries per warp (32 or 64)
 };
+// Whether (threads, slab) is one of the traversal's compiled launch shapes.
+bool traversal_shape_valid(int threads, int slab);
 constexpr int kTraverseStack = 4608;
 // Resident warps of the persistent traversal grid on `device` (for sizing TraverseWorkspace).
 int64_t traverse_resident_warps(int device);

@@ -44,11 +44,12 @@ namespace nbg {
 
 namespace {
 
-constexpr int kThreads = 256;
-constexpr int kWarps = kThreads / 32;
-constexpr int kList = 64;   // leaf and mixed lists: each round appends at most 32, evaluated above 32
+// Launch shapes (autotuned per workload, see nb_set_traversal_shape): THREADS threads per block
+// (128 or 256) and PART entries in the partial-accept slab (32 or 64). The launch bounds keep
+// 1024 threads per SM resident (64 registers per thread).
+constexpr int kResidentThreads = 1024;
+constexpr int kList = 64;      // leaf and mixed lists: each round appends at most 32, evaluated above 32
 constexpr int kFullSlab = 32;  // staged nodes accepted by the whole group
-constexpr int kPartSlab = 64;  // staged nodes accepted by some targets only (two 32-entry mask blocks)
 // Stack: kTraverseStack entries per warp. No bound below that size is proven for every tree, so a
 // round whose pushes would not fit abandons its group and sets kErrStackOverflow (the host turns it
 // into an error); every entry on the stack has been written, so no stale entry is ever popped.
@@ -56,21 +57,21 @@ constexpr unsigned kFull = 0xffffffffu;
 
 enum : int { kNone = 0, kAcceptAll = 1, kOpenAll = 2, kMixed = 3 };
 
-template<int PAY>
+template<int PAY, int PART>
 struct WarpSmem {
     float4 tpos[32];
     float4 full_pay[kFullSlab * PAY];  // payloads of group-wide accepted nodes
-    float4 part_pay[kPartSlab * PAY];  // payloads of partially accepted nodes
-    uint32_t part_mask[kPartSlab];     // their target masks
+    float4 part_pay[PART * PAY];       // payloads of partially accepted nodes
+    uint32_t part_mask[PART];          // their target masks
     int pp_begin[kList], pp_end[kList];
     uint32_t pp_mask[kList];
     int mixed_node[kList];
     uint32_t mixed_mask[kList];
 };
 
-template<int ORDER>
+template<int ORDER, int THREADS, int PART>
 constexpr size_t block_smem_bytes() {
-    return sizeof(WarpSmem<NodeLayout<ORDER>::PAY>) * kWarps;
+    return sizeof(WarpSmem<NodeLayout<ORDER>::PAY, PART>) * (THREADS / 32);
 }
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -158,8 +159,8 @@ __device__ __forceinline__ void stage_node(float4 *dst, const float4 *__restrict
 }
 
 // Nodes accepted by the whole group: every lane evaluates every staged entry (broadcast reads).
-template<int ORDER, bool EPS0>
-__device__ __forceinline__ void flush_full(WarpSmem<NodeLayout<ORDER>::PAY> &S, int &nfull, float4 p, float eps,
+template<int ORDER, bool EPS0, int PART>
+__device__ __forceinline__ void flush_full(WarpSmem<NodeLayout<ORDER>::PAY, PART> &S, int &nfull, float4 p, float eps,
                                            float &ax, float &ay, float &az, unsigned &cnp) {
     constexpr int PAY = NodeLayout<ORDER>::PAY;
     cp_async_wait_all();
@@ -177,14 +178,16 @@ __device__ __forceinline__ void flush_full(WarpSmem<NodeLayout<ORDER>::PAY> &S, 
 
 // Nodes accepted by some targets only: the masks are transposed so that each lane holds the set
 // of entries it evaluates, then every lane walks its own set.
-template<int ORDER, bool EPS0>
-__device__ __forceinline__ void flush_part(WarpSmem<NodeLayout<ORDER>::PAY> &S, int &npart, float4 p, float eps,
+template<int ORDER, bool EPS0, int PART>
+__device__ __forceinline__ void flush_part(WarpSmem<NodeLayout<ORDER>::PAY, PART> &S, int &npart, float4 p, float eps,
                                            int lane, float &ax, float &ay, float &az, unsigned &cnp) {
     constexpr int PAY = NodeLayout<ORDER>::PAY;
     cp_async_wait_all();
     __syncwarp();
     uint32_t b0 = transpose32(lane < npart ? S.part_mask[lane] : 0u, lane);
-    uint32_t b1 = npart > 32 ? transpose32(lane + 32 < npart ? S.part_mask[lane + 32] : 0u, lane) : 0u;
+    uint32_t b1 = 0u;
+    if constexpr (PART > 32)
+        b1 = npart > 32 ? transpose32(lane + 32 < npart ? S.part_mask[lane + 32] : 0u, lane) : 0u;
     cnp += (unsigned) (__popc(b0) + __popc(b1));
     while (__any_sync(kFull, (b0 | b1) != 0u)) {
         if (b0 | b1) {
@@ -203,8 +206,8 @@ __device__ __forceinline__ void flush_part(WarpSmem<NodeLayout<ORDER>::PAY> &S, 
     __syncwarp();
 }
 
-template<bool EPS0, int PAY>
-__device__ __forceinline__ void flush_pp(WarpSmem<PAY> &S, int &npp, const float4 *__restrict__ bodies, float4 p,
+template<bool EPS0, int PAY, int PART>
+__device__ __forceinline__ void flush_pp(WarpSmem<PAY, PART> &S, int &npp, const float4 *__restrict__ bodies, float4 p,
                                          float eps, int lane, float &ax, float &ay, float &az, unsigned &cpp) {
     for (int j = 0; j < npp; ++j) {
         const int b = S.pp_begin[j], e = S.pp_end[j];
@@ -234,8 +237,8 @@ __device__ __forceinline__ void flush_pp(WarpSmem<PAY> &S, int &npp, const float
 // acc / part are accepted nodes (target mask mk for part), leaf is an opened leaf (body range
 // l0..l1, mask mk), open an opened internal node (children c + 1 and l0, mask mk), mixed a node
 // still to be resolved per target.
-template<int ORDER, bool EPS0>
-__device__ __forceinline__ bool dispatch(WarpSmem<NodeLayout<ORDER>::PAY> &S, const float4 *__restrict__ pay,
+template<int ORDER, bool EPS0, int PART>
+__device__ __forceinline__ bool dispatch(WarpSmem<NodeLayout<ORDER>::PAY, PART> &S, const float4 *__restrict__ pay,
                                          const float4 *__restrict__ bodies, int2 *stack, bool acc, bool part,
                                          bool leaf, bool open, bool mixed, int c, uint32_t mk, int l0, int l1,
                                          int n_bodies, uint32_t lt, int lane, int &nfull, int &npart, int &npp,
@@ -244,13 +247,13 @@ __device__ __forceinline__ bool dispatch(WarpSmem<NodeLayout<ORDER>::PAY> &S, co
     constexpr int PAY = NodeLayout<ORDER>::PAY;
     uint32_t b = __ballot_sync(kFull, acc);
     if (b) {
-        if (nfull + __popc(b) > kFullSlab) flush_full<ORDER, EPS0>(S, nfull, p, eps, ax, ay, az, gnp);
+        if (nfull + __popc(b) > kFullSlab) flush_full<ORDER, EPS0, PART>(S, nfull, p, eps, ax, ay, az, gnp);
         if (acc) stage_node<PAY>(S.full_pay + (nfull + __popc(b & lt)) * PAY, pay, c);
         nfull += __popc(b);
     }
     b = __ballot_sync(kFull, part);
     if (b) {
-        if (npart + __popc(b) > kPartSlab) flush_part<ORDER, EPS0>(S, npart, p, eps, lane, ax, ay, az, gnp);
+        if (npart + __popc(b) > PART) flush_part<ORDER, EPS0, PART>(S, npart, p, eps, lane, ax, ay, az, gnp);
         if (part) {
             const int slot = npart + __popc(b & lt);
             stage_node<PAY>(S.part_pay + slot * PAY, pay, c);
@@ -289,12 +292,12 @@ __device__ __forceinline__ bool dispatch(WarpSmem<NodeLayout<ORDER>::PAY> &S, co
     }
     __syncwarp();
     // each round appends at most 32 leaves: evaluate before the next one could overflow the list
-    if (npp > kList - 32) flush_pp<EPS0>(S, npp, bodies, p, eps, lane, ax, ay, az, gpp);
+    if (npp > kList - 32) flush_pp<EPS0, NodeLayout<ORDER>::PAY, PART>(S, npp, bodies, p, eps, lane, ax, ay, az, gpp);
     return abandoned;
 }
 
-template<int ORDER, bool EPS0>
-__global__ void __launch_bounds__(kThreads, 4) bh_kernel(NodeArrays nodes, const int *__restrict__ num_nodes_p,
+template<int ORDER, bool EPS0, int THREADS, int PART>
+__global__ void __launch_bounds__(THREADS, kResidentThreads / THREADS) bh_kernel(NodeArrays nodes, const int *__restrict__ num_nodes_p,
                                                          const float4 *__restrict__ bodies, int n_bodies,
                                                          const float4 *__restrict__ targets, int n_targets, float G,
                                                          float eps, float4 *__restrict__ acc,
@@ -307,8 +310,8 @@ __global__ void __launch_bounds__(kThreads, 4) bh_kernel(NodeArrays nodes, const
     constexpr int PAY = NodeLayout<ORDER>::PAY;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    WarpSmem<PAY> &S = reinterpret_cast<WarpSmem<PAY> *>(smem_raw)[warp];
-    int2 *stack = stack_base + ((int64_t) blockIdx.x * kWarps + warp) * kTraverseStack;
+    WarpSmem<PAY, PART> &S = reinterpret_cast<WarpSmem<PAY, PART> *>(smem_raw)[warp];
+    int2 *stack = stack_base + ((int64_t) blockIdx.x * (THREADS / 32) + warp) * kTraverseStack;
     const float4 *__restrict__ mac = nodes.mac;
     const int2 *__restrict__ link = nodes.link;
     const float4 *__restrict__ pay = nodes.pay;
@@ -398,7 +401,7 @@ __global__ void __launch_bounds__(kThreads, 4) bh_kernel(NodeArrays nodes, const
                 const bool is_leaf_open = cls == kOpenAll && l1 >= 0;
                 const bool is_int_open = cls == kOpenAll && l1 < 0 && l0 > c + 1 && l0 < num_nodes;
                 if (cls == kOpenAll && l1 < 0 && !is_int_open) atomicOr(err, (uint32_t) kErrTraverseLimit);
-                if (dispatch<ORDER, EPS0>(S, pay, bodies, stack, cls == kAcceptAll && m == full,
+                if (dispatch<ORDER, EPS0, PART>(S, pay, bodies, stack, cls == kAcceptAll && m == full,
                                           cls == kAcceptAll && m != full, is_leaf_open, is_int_open, cls == kMixed,
                                           c, m, l0, l1, n_bodies, lt, lane, nfull, npart, npp, nmixed, top, p, eps,
                                           ax, ay, az, gnp, gpp, err)) {
@@ -435,10 +438,10 @@ __global__ void __launch_bounds__(kThreads, 4) bh_kernel(NodeArrays nodes, const
                 const bool is_acc = A != 0 && A == full;
                 const bool is_part = A != 0 && A != full;
                 // an entry can be accepted by some targets and opened by others: append both parts
-                if (dispatch<ORDER, EPS0>(S, pay, bodies, stack, is_acc, is_part, false, false, false, c, A, l0,
+                if (dispatch<ORDER, EPS0, PART>(S, pay, bodies, stack, is_acc, is_part, false, false, false, c, A, l0,
                                           l1, n_bodies, lt, lane, nfull, npart, npp, nmixed, top, p, eps, ax, ay,
                                           az, gnp, gpp, err) ||
-                    dispatch<ORDER, EPS0>(S, pay, bodies, stack, false, false, O != 0 && l1 >= 0, is_int_open, false,
+                    dispatch<ORDER, EPS0, PART>(S, pay, bodies, stack, false, false, O != 0 && l1 >= 0, is_int_open, false,
                                           c, O, l0, l1, n_bodies, lt, lane, nfull, npart, npp, nmixed, top, p, eps,
                                           ax, ay, az, gnp, gpp, err)) {
                     top = 0;
@@ -446,9 +449,9 @@ __global__ void __launch_bounds__(kThreads, 4) bh_kernel(NodeArrays nodes, const
                 }
             }
         }
-        flush_full<ORDER, EPS0>(S, nfull, p, eps, ax, ay, az, gnp);
-        flush_part<ORDER, EPS0>(S, npart, p, eps, lane, ax, ay, az, gnp);
-        flush_pp<EPS0>(S, npp, bodies, p, eps, lane, ax, ay, az, gpp);
+        flush_full<ORDER, EPS0, PART>(S, nfull, p, eps, ax, ay, az, gnp);
+        flush_part<ORDER, EPS0, PART>(S, npart, p, eps, lane, ax, ay, az, gnp);
+        flush_pp<EPS0, PAY, PART>(S, npp, bodies, p, eps, lane, ax, ay, az, gpp);
         if (valid) acc[i] = make_float4(G * ax, G * ay, G * az, 0.f);
         if (valid) {
             cnp += gnp;
@@ -476,38 +479,77 @@ __global__ void __launch_bounds__(kThreads, 4) bh_kernel(NodeArrays nodes, const
 
 // Occupancy and SM count are fixed per device and kernel: queried once (B200 parts are identical).
 // The kernel's dynamic shared memory (the warps' slabs and lists) is enabled on first use.
-template<int ORDER, bool EPS0>
+template<int ORDER, bool EPS0, int THREADS, int PART>
 int blocks_per_sm(int device) {
     static int cached[64] = {0};
     if (device < 0 || device >= 64) device = 0;
     if (cached[device] == 0) {
-        const size_t smem = block_smem_bytes<ORDER>();
-        cudaFuncSetAttribute(bh_kernel<ORDER, EPS0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-        cudaFuncSetAttribute(bh_kernel<ORDER, EPS0>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             cudaSharedmemCarveoutMaxShared);
+        const size_t smem = block_smem_bytes<ORDER, THREADS, PART>();
+        auto kernel = bh_kernel<ORDER, EPS0, THREADS, PART>;
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+        cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
         int b = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, bh_kernel<ORDER, EPS0>, kThreads, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, THREADS, smem);
         cached[device] = b > 0 ? b : 1;
     }
     return cached[device];
 }
 
-template<int ORDER, bool EPS0>
-void launch_variant(const NodeArrays &nodes, const int *num_nodes, const float4 *bodies, int n_bodies,
-                    const float4 *targets, int nt, float G, float eps, float4 *acc, unsigned long long *counts,
-                    TraverseWorkspace &ws, uint32_t *err, cudaStream_t s, const int4 *gtab, int64_t ngroups,
-                    const int *inst_root, unsigned long long *inst_counts) {
+template<int ORDER, bool EPS0, int THREADS, int PART>
+int resident_warps(int device) {
+    return sm_count(device) * blocks_per_sm<ORDER, EPS0, THREADS, PART>(device) * (THREADS / 32);
+}
+
+struct LaunchArgs {
+    const NodeArrays *nodes;
+    const int *num_nodes;
+    const float4 *bodies;
+    int n_bodies;
+    const float4 *targets;
+    int nt;
+    float G, eps;
+    float4 *acc;
+    unsigned long long *counts;
+    TraverseWorkspace *ws;
+    uint32_t *err;
+    cudaStream_t s;
+    const int4 *gtab;
+    int64_t ngroups;
+    const int *inst_root;
+    unsigned long long *inst_counts;
+};
+
+template<int ORDER, bool EPS0, int THREADS, int PART>
+void launch_variant(const LaunchArgs &a) {
+    constexpr int kWarps = THREADS / 32;
     int device = 0;
     cudaGetDevice(&device);
-    int64_t blocks = (int64_t) sm_count(device) * blocks_per_sm<ORDER, EPS0>(device);
-    blocks = std::min<int64_t>(blocks, ws.warps / kWarps);
-    const int64_t groups = gtab ? ngroups : (nt + 31) / 32;
+    int64_t blocks = (int64_t) sm_count(device) * blocks_per_sm<ORDER, EPS0, THREADS, PART>(device);
+    blocks = std::min<int64_t>(blocks, a.ws->warps / kWarps);
+    const int64_t groups = a.gtab ? a.ngroups : (a.nt + 31) / 32;
     blocks = std::min<int64_t>(blocks, (groups + kWarps - 1) / kWarps);
     if (blocks < 1) blocks = 1;
-    cudaMemsetAsync(ws.group_counter, 0, sizeof(unsigned), s);
-    bh_kernel<ORDER, EPS0><<<(unsigned) blocks, kThreads, block_smem_bytes<ORDER>(), s>>>(
-        nodes, num_nodes, bodies, n_bodies, targets, nt, G, eps, acc, counts, ws.stack, ws.group_counter, err, gtab,
-        (int) ngroups, inst_root, inst_counts);
+    cudaMemsetAsync(a.ws->group_counter, 0, sizeof(unsigned), a.s);
+    bh_kernel<ORDER, EPS0, THREADS, PART><<<(unsigned) blocks, THREADS, block_smem_bytes<ORDER, THREADS, PART>(), a.s>>>(
+        *a.nodes, a.num_nodes, a.bodies, a.n_bodies, a.targets, a.nt, a.G, a.eps, a.acc, a.counts, a.ws->stack,
+        a.ws->group_counter, a.err, a.gtab, (int) a.ngroups, a.inst_root, a.inst_counts);
+}
+
+template<int ORDER, bool EPS0>
+void launch_shape(const LaunchArgs &a, int threads, int part) {
+    if (threads == 128) {
+        if (part == 32) launch_variant<ORDER, EPS0, 128, 32>(a);
+        else launch_variant<ORDER, EPS0, 128, 64>(a);
+    } else {
+        if (part == 32) launch_variant<ORDER, EPS0, 256, 32>(a);
+        else launch_variant<ORDER, EPS0, 256, 64>(a);
+    }
+}
+
+template<int ORDER, bool EPS0>
+int max_resident_warps(int device) {
+    return std::max(std::max(resident_warps<ORDER, EPS0, 128, 32>(device), resident_warps<ORDER, EPS0, 128, 64>(device)),
+                    std::max(resident_warps<ORDER, EPS0, 256, 32>(device), resident_warps<ORDER, EPS0, 256, 64>(device)));
 }
 
 }  // namespace
@@ -530,23 +572,27 @@ int current_sm_count() {
 }
 
 int64_t traverse_resident_warps(int device) {
-    int b = std::max(std::max(blocks_per_sm<1, false>(device), blocks_per_sm<1, true>(device)),
-                     std::max(blocks_per_sm<2, false>(device), blocks_per_sm<2, true>(device)));
-    return (int64_t) sm_count(device) * b * kWarps;
+    return std::max(std::max(max_resident_warps<1, false>(device), max_resident_warps<1, true>(device)),
+                    std::max(max_resident_warps<2, false>(device), max_resident_warps<2, true>(device)));
 }
+
+bool traversal_shape_valid(int threads, int slab) { return (threads == 128 || threads == 256) && (slab == 32 || slab == 64); }
 
 void launch_bh_traverse(int order, const NodeArrays &nodes, const int *num_nodes, const float4 *bodies, int64_t n_bodies,
                         const float4 *targets, int64_t n_targets, float G, float eps, float4 *acc,
                         unsigned long long *counts, TraverseWorkspace &ws, uint32_t *err, cudaStream_t s,
                         const int4 *gtab, int64_t ngroups, const int *inst_root, unsigned long long *inst_counts) {
     if (n_targets <= 0) return;
-    const int nb = (int) n_bodies, nt = (int) n_targets;
+    const LaunchArgs a{&nodes, num_nodes, bodies, (int) n_bodies, targets, (int) n_targets, G, eps, acc, counts, &ws,
+                       err, s, gtab, ngroups, inst_root, inst_counts};
+    const bool ok = traversal_shape_valid(ws.threads, ws.slab);
+    const int threads = ok ? ws.threads : 256, part = ok ? ws.slab : 64;
     if (order == 1) {
-        if (eps == 0.f) launch_variant<1, true>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s, gtab, ngroups, inst_root, inst_counts);
-        else launch_variant<1, false>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s, gtab, ngroups, inst_root, inst_counts);
+        if (eps == 0.f) launch_shape<1, true>(a, threads, part);
+        else launch_shape<1, false>(a, threads, part);
     } else {
-        if (eps == 0.f) launch_variant<2, true>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s, gtab, ngroups, inst_root, inst_counts);
-        else launch_variant<2, false>(nodes, num_nodes, bodies, nb, targets, nt, G, eps, acc, counts, ws, err, s, gtab, ngroups, inst_root, inst_counts);
+        if (eps == 0.f) launch_shape<2, true>(a, threads, part);
+        else launch_shape<2, false>(a, threads, part);
     }
 }
 

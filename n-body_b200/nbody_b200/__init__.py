@@ -141,6 +141,8 @@ SIGNATURES = {
     "nb_get_instance_counts": (C.c_int, [_vp, _i32, _vp, _vp]),
     "nb_enable_graphs": (C.c_int, [_vp, C.c_int]),
     "nb_set_fp64_summaries": (C.c_int, [_vp, C.c_int64]),
+    "nb_set_traversal_shape": (C.c_int, [_vp, _i32, _i32]),
+    "nb_get_traversal_shape": (C.c_int, [_vp, C.POINTER(_i32), C.POINTER(_i32)]),
     "nb_server_create": (C.c_int, [C.POINTER(Config), C.c_uint64, C.POINTER(_vp)]),
     "nb_server_destroy": (C.c_int, [_vp]),
     "nb_server_last_error": (C.c_char_p, [_vp]),
@@ -362,6 +364,17 @@ class Solver:
         (nb_set_fp64_summaries; 0 turns it off)."""
         self._check(lib().nb_set_fp64_summaries(self._ctx, int(min_bodies)))
 
+    @property
+    def traversal_shape(self):
+        """(threads per block, partial-accept slab entries) of the traversal launch."""
+        t, e = C.c_int32(), C.c_int32()
+        self._check(lib().nb_get_traversal_shape(self._ctx, C.byref(t), C.byref(e)))
+        return int(t.value), int(e.value)
+
+    @traversal_shape.setter
+    def traversal_shape(self, shape):
+        self._check(lib().nb_set_traversal_shape(self._ctx, int(shape[0]), int(shape[1])))
+
     def body_count(self) -> int:
         return int(lib().nb_body_count(self._ctx))
 
@@ -534,6 +547,10 @@ class Server:
 
     def context(self):
         return lib().nb_server_context(self._h)
+
+    def set_traversal_shape(self, shape):
+        """Traversal launch shape (threads per block, tile) of the server's batched passes."""
+        self._check(lib().nb_set_traversal_shape(self.context(), int(shape[0]), int(shape[1])))
 
     def submit(self, bodies, velocities=None, theta: float = 0.5, steps: int = 1) -> int:
         pm = _bodies(bodies)

@@ -1,5 +1,6 @@
-"""Leaf-size autotuner (nbody_b200/autotune.py): selection, workload keys and the cache, driven
-by a fake solver on the CPU (the device path is exercised in test_gpu_autotune)."""
+"""Autotuner (nbody_b200/autotune.py): leaf size and traversal launch shape selection, workload keys
+and the cache, driven by a fake solver on the CPU (the device path is exercised in
+test_gpu_autotune)."""
 import json
 
 import pytest
@@ -8,8 +9,10 @@ import pytest
 class FakeSolver:
     """Solver-like object whose force-pass time depends on the leaf size."""
 
-    def __init__(self, cost, n=100000, instances=1, theta=0.5):
+    def __init__(self, cost, n=100000, instances=1, theta=0.5, shape_cost=None):
         self.cost, self.n, self.inst, self._theta = cost, n, instances, theta
+        self.shape_cost = shape_cost or (lambda shape: 0.0)
+        self.shape = (256, 64)
         self.max_leaf_size = 16
         self.sets = []
         self._passes = 0
@@ -29,6 +32,14 @@ class FakeSolver:
     def theta(self):
         return self._theta
 
+    @property
+    def traversal_shape(self):
+        return self.shape
+
+    @traversal_shape.setter
+    def traversal_shape(self, shape):
+        self.shape = (256, 64) if tuple(shape) == (0, 0) else tuple(shape)
+
     def __setattr__(self, k, v):
         if k == "max_leaf_size" and "sets" in self.__dict__:
             self.__dict__["sets"].append(v)
@@ -37,7 +48,7 @@ class FakeSolver:
     def update_accelerations_async(self):
         if self._timing:
             self._passes += 1
-            self._ms += self.cost(self.max_leaf_size)
+            self._ms += self.cost(self.max_leaf_size) + self.shape_cost(self.shape)
 
     def synchronize(self):
         pass
@@ -89,3 +100,24 @@ def test_cache_round_trip_and_reuse(nb, tmp_path):
     s2 = FakeSolver(lambda leaf: pytest.fail("a cached workload must not be measured again"))
     r2 = at.autotune(s2, at.TuningCache(path), candidates=(4, 8, 12, 16))
     assert r2.cached and r2.leaf == r.leaf and s2.max_leaf_size == r.leaf
+
+
+def test_shape_tuned_after_leaf(nb, tmp_path):
+    from nbody_b200 import autotune as at
+
+    s = FakeSolver(lambda leaf: abs(leaf - 12) + 10.0, shape_cost=lambda sh: {(128, 32): -1.0}.get(sh, 0.0))
+    cache = at.TuningCache(str(tmp_path / "t.json"))
+    r = at.autotune(s, cache, candidates=(8, 12, 16), passes=1)
+    assert r.leaf == 12 and r.shape == (128, 32) and s.traversal_shape == (128, 32)
+    assert set(r.shape_timings_ms) == {"256x64", "256x32", "128x64", "128x32"}
+    s2 = FakeSolver(lambda leaf: pytest.fail("cached"))
+    r2 = at.autotune(s2, at.TuningCache(str(tmp_path / "t.json")), candidates=(8, 12, 16))
+    assert r2.cached and r2.shape == (128, 32) and s2.traversal_shape == (128, 32) and s2.max_leaf_size == 12
+
+
+def test_cache_entry_without_shape_reads_default(nb, tmp_path):
+    from nbody_b200 import autotune as at
+
+    path = tmp_path / "old.json"
+    path.write_text(json.dumps({"k": {"leaf": 8, "timings_ms": {"8": 1.0}}}))
+    assert at.TuningCache(str(path)).lookup("k") == (8, (256, 64))
