@@ -266,7 +266,8 @@ void free_buffers(nb_ctx *ctx) {
     dev_free(ctx->sw.keys_alt); dev_free(ctx->sw.vals_alt); dev_free(ctx->sw.lookback);
     dev_free(ctx->tw.range); dev_free(ctx->tw.left); dev_free(ctx->tw.right); dev_free(ctx->tw.parent);
     dev_free(ctx->tw.splittable); dev_free(ctx->tw.visit); dev_free(ctx->tw.sbmin); dev_free(ctx->tw.sbmax);
-    dev_free(ctx->tw.scom); dev_free(ctx->tw.sq0); dev_free(ctx->tw.sq1); dev_free(ctx->tw.cnt);
+    dev_free(ctx->tw.scom); dev_free(ctx->tw.sq0); dev_free(ctx->tw.sq1); dev_free(ctx->tw.chain);
+    dev_free(ctx->tw.start); dev_free(ctx->tw.prefix); dev_free(ctx->tw.scan_part);
     dev_free(ctx->nodes.mac); dev_free(ctx->nodes.link); dev_free(ctx->nodes.pay);
     ctx->nodes.capacity = 0;
     ctx->cap = 0;
@@ -301,7 +302,10 @@ int ensure_capacity(nb_ctx *ctx, int64_t n) {
     NB_TRY(dev_alloc(&ctx->tw.scom, slots), "alloc summaries");
     NB_TRY(dev_alloc(&ctx->tw.sq0, slots), "alloc summaries");
     NB_TRY(dev_alloc(&ctx->tw.sq1, slots), "alloc summaries");
-    NB_TRY(dev_alloc(&ctx->tw.cnt, slots), "alloc summaries");
+    NB_TRY(dev_alloc(&ctx->tw.chain, c), "alloc tree");
+    NB_TRY(dev_alloc(&ctx->tw.start, c + 1), "alloc tree");
+    NB_TRY(dev_alloc(&ctx->tw.prefix, c + 1), "alloc tree");
+    NB_TRY(dev_alloc(&ctx->tw.scan_part, build_scan_tiles(c)), "alloc tree");
     ctx->tw.capacity = c;
     const int64_t node_cap = 2 * c;
     NB_TRY(dev_alloc(&ctx->nodes.mac, (size_t) node_cap), "alloc tree nodes");

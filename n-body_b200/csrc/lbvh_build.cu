@@ -21,10 +21,15 @@
 //                     sum follows libstdc++'s 4-way std::transform_reduce). All float operations
 //                     are single IEEE operations in the reference's order, so summaries are
 //                     bit-identical to the CPU restatement.
-//   emit_kernel       preorder index of every final node (walk to the root adding left-sibling
-//                     subtree sizes) and the node arrays the traversal reads: MAC data (centre and
-//                     exact MAC threshold), links (right child / leaf body range) and payload
-//                     (centre of mass, mass, quadrupole).
+//   scan kernels      exclusive prefix over body positions of the number of final nodes whose
+//                     range starts there (counted by karras_kernel)
+//   emit_kernel       the node arrays the traversal reads, each node at its preorder index: MAC data
+//                     (centre and exact MAC threshold), links (right child / leaf body range) and
+//                     payload (centre of mass, mass, quadrupole). The preorder index is closed-form:
+//                     for a node whose range starts at body f, the final nodes before it in preorder
+//                     are those starting before f (the prefix at f) and, among the internal nodes
+//                     starting at f (a chain of left children), the larger ones; a leaf starting at f
+//                     comes after that whole chain.
 #include <cfloat>
 
 #include "nb_internal.cuh"
@@ -48,11 +53,20 @@ __device__ __forceinline__ int prefix_delta(const uint64_t *__restrict__ codes, 
     return 32 + ((a != b) ? __clzll(a ^ b) : 64 + __clz(i ^ j));
 }
 
+// A node covering sorted positions [a, b] is split by the reference (a final internal node) iff it
+// holds more than `leaf` bodies with different end codes; a node spanning several instances only
+// connects their trees and is always split.
+__device__ __forceinline__ bool range_splittable(const uint64_t *__restrict__ codes, const int *__restrict__ inst_of,
+                                                 int leaf, int a, int b) {
+    if (inst_of && inst_of[a] != inst_of[b]) return true;
+    return (b - a + 1 > leaf) && (codes[a] != codes[b]);
+}
+
 __global__ void __launch_bounds__(kThreads) karras_kernel(const uint64_t *__restrict__ codes,
                                                           const int *__restrict__ inst_of, int n, int leaf,
                                                           int2 *__restrict__ range, int *__restrict__ left,
                                                           int *__restrict__ right, int *__restrict__ parent,
-                                                          uint8_t *__restrict__ splittable) {
+                                                          uint8_t *__restrict__ splittable, int *__restrict__ start) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
     const int dn = prefix_delta(codes, inst_of, n, i, i + 1);
@@ -80,10 +94,107 @@ __global__ void __launch_bounds__(kThreads) karras_kernel(const uint64_t *__rest
     range[i] = make_int2(first, last);
     if (lc >= 0) parent[lc] = i;
     if (rc >= 0) parent[rc] = i;
-    // A node spanning several instances only connects their trees: it is always split.
-    const bool spans = inst_of && inst_of[first] != inst_of[last];
-    splittable[i] = (uint8_t) (spans || ((last - first + 1 > leaf) && (codes[first] != codes[last])));
+    const bool split = range_splittable(codes, inst_of, leaf, first, last);
+    splittable[i] = (uint8_t) split;
+    if (split) {
+        // a final internal node starts at `first`; a child that is not split is a final leaf
+        atomicAdd(start + first, 2);
+        if (lc < 0 || !range_splittable(codes, inst_of, leaf, first, gamma)) atomicAdd(start + first, 1);
+        if (rc < 0 || !range_splittable(codes, inst_of, leaf, gamma + 1, last)) atomicAdd(start + gamma + 1, 1);
+    }
 }
+
+// Exclusive prefix over positions 0..n of the number of final nodes starting at each position,
+// in three steps: tile totals, a prefix over the tiles (one block), and the per-tile scan.
+constexpr int kScanTile = 2048;
+
+__device__ __forceinline__ int starts_at(const int *__restrict__ start, int64_t b) {
+    const int w = start[b];
+    return (w >> 1) + (w & 1);
+}
+
+__global__ void __launch_bounds__(kThreads) scan_tiles_kernel(const int *__restrict__ start, int64_t m,
+                                                              int *__restrict__ part) {
+    __shared__ int red[kThreads / 32];
+    const int64_t base = (int64_t) blockIdx.x * kScanTile;
+    int sum = 0;
+    for (int k = threadIdx.x; k < kScanTile; k += kThreads)
+        if (base + k < m) sum += starts_at(start, base + k);
+    sum = __reduce_add_sync(0xffffffffu, sum);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < kThreads / 32; ++w) t += red[w];
+        part[blockIdx.x] = t;
+    }
+}
+
+// One block: part[t] becomes the exclusive prefix of the tile totals; the total is the node count.
+__global__ void __launch_bounds__(1024) scan_parts_kernel(int *__restrict__ part, int tiles, int *__restrict__ total) {
+    __shared__ int warp_sum[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int base = 0; base < tiles; base += 1024) {
+        const int t = base + threadIdx.x;
+        const int v = t < tiles ? part[t] : 0;
+        int incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) warp_sum[warp] = incl;
+        __syncthreads();
+        int before = carry;
+        for (int w = 0; w < warp; ++w) before += warp_sum[w];
+        if (t < tiles) part[t] = before + incl - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = before + incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void __launch_bounds__(kThreads) scan_apply_kernel(const int *__restrict__ start, int64_t m,
+                                                              const int *__restrict__ part, int *__restrict__ prefix) {
+    constexpr int kPer = kScanTile / kThreads;  // consecutive positions per thread
+    __shared__ int warp_sum[kThreads / 32];
+    const int64_t base = (int64_t) blockIdx.x * kScanTile + (int64_t) threadIdx.x * kPer;
+    int v[kPer];
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        v[k] = base + k < m ? starts_at(start, base + k) : 0;
+        sum += v[k];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) warp_sum[warp] = incl;
+    __syncthreads();
+    int run = part[blockIdx.x] + incl - sum;
+    for (int w = 0; w < warp; ++w) run += warp_sum[w];
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+        if (base + k < m) prefix[base + k] = run;
+        run += v[k];
+    }
+}
+
+// Preorder index of a final node whose range starts at body f: after the final nodes starting
+// before f; an internal node follows the larger internal nodes of its chain at f (chain = final
+// internal nodes below it that share f), a leaf follows the whole chain.
+__device__ __forceinline__ int preorder_internal(const TreeWorkspace &tw, int f, int chain) {
+    return tw.prefix[f] + (tw.start[f] >> 1) - 1 - chain;
+}
+__device__ __forceinline__ int preorder_leaf(const TreeWorkspace &tw, int f) { return tw.prefix[f] + (tw.start[f] >> 1); }
 
 template<int ORDER>
 struct Summ {
@@ -333,6 +444,14 @@ __device__ Summ<ORDER> internal_summary_f64(const Summ<ORDER> &a, const Summ<ORD
 __device__ __forceinline__ bool is_final_leaf(const uint8_t *splittable, int c) { return c < 0 || !splittable[c]; }
 __device__ __forceinline__ int slot_of(int c, int n) { return c >= 0 ? c : (n - 1) + ~c; }
 
+// Arrival counter of the bottom-up climb with release-acquire ordering: the caller's summary
+// stores are visible before its arrival, and the second arriver sees the first one's stores.
+__device__ __forceinline__ int arrive_acq_rel(int *p) {
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(old) : "l"(p) : "memory");
+    return old;
+}
+
 template<int ORDER>
 __global__ void __launch_bounds__(kThreads) summarize_kernel(const float4 *__restrict__ bodies, int n, TreeWorkspace tw,
                                                              uint32_t *err) {
@@ -343,26 +462,33 @@ __global__ void __launch_bounds__(kThreads) summarize_kernel(const float4 *__res
         if (!is_final_leaf(tw.splittable, c)) continue;
         int b, e;
         if (c < 0) { b = e = ~c; } else { int2 r = tw.range[c]; b = r.x; e = r.y; }
-        const int slot = slot_of(c, n);
-        store_slot<ORDER>(tw, slot, leaf_summary<ORDER>(bodies, b, e));
-        tw.cnt[slot] = 1;
-        int p = i;
+        Summ<ORDER> mine = leaf_summary<ORDER>(bodies, b, e);
+        store_slot<ORDER>(tw, slot_of(c, n), mine);
+        int from = c, p = i, chain_from = -1;  // chain of the node we come from (-1: a leaf)
         for (int level = 0;; ++level) {
             if (level >= kMaxTreeDepth || p < 0 || p >= n - 1) {
                 atomicOr(err, (uint32_t) kErrTreeDepth);
                 break;
             }
-            __threadfence();
-            if (atomicAdd(&tw.visit[p], 1) == 0) break;  // the sibling's thread finishes p
-            __threadfence();
-            const int sl = slot_of(tw.left[p], n), sr = slot_of(tw.right[p], n);
+            if (arrive_acq_rel(&tw.visit[p]) == 0) break;  // the sibling's thread finishes p
+            const int lc = tw.left[p], rc = tw.right[p];
+            const bool from_left = (lc == from);
+            const Summ<ORDER> other = load_slot<ORDER>(tw, slot_of(from_left ? rc : lc, n));
             const int2 rg = tw.range[p];
-            if (tw.fp64_min_bodies > 0 && rg.y - rg.x + 1 >= tw.fp64_min_bodies)
-                store_slot<ORDER>(tw, p, internal_summary_f64<ORDER>(load_slot<ORDER>(tw, sl), load_slot<ORDER>(tw, sr)));
-            else
-                store_slot<ORDER>(tw, p, internal_summary<ORDER>(load_slot<ORDER>(tw, sl), load_slot<ORDER>(tw, sr)));
-            tw.cnt[p] = 1 + __ldcg(tw.cnt + sl) + __ldcg(tw.cnt + sr);
+            const Summ<ORDER> &l = from_left ? mine : other;
+            const Summ<ORDER> &r = from_left ? other : mine;
+            const Summ<ORDER> up = (tw.fp64_min_bodies > 0 && rg.y - rg.x + 1 >= tw.fp64_min_bodies)
+                                       ? internal_summary_f64<ORDER>(l, r)
+                                       : internal_summary<ORDER>(l, r);
+            store_slot<ORDER>(tw, p, up);
+            // final internal nodes below p that share its first body: its left child's chain
+            const int lchain = !is_final_leaf(tw.splittable, lc) ? (from_left ? chain_from : __ldcg(tw.chain + lc)) : -1;
+            const int ch = lchain + 1;
+            tw.chain[p] = ch;
             if (p == 0) break;
+            mine = up;
+            chain_from = ch;
+            from = p;
             p = tw.parent[p];
         }
     }
@@ -430,36 +556,26 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(int n, TreeWorkspace tw,
                                                         uint32_t *err, BatchSegments seg) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1 || !tw.splittable[i]) return;
-    int pre = 0;
-    int depth = 0;
-    for (int u = i; u != 0; ++depth) {
-        const int p = tw.parent[u];
-        if (depth >= kMaxTreeDepth || p < 0 || p >= n - 1) {
-            atomicOr(err, (uint32_t) kErrTreeDepth);
-            return;
-        }
-        pre += 1;
-        if (tw.right[p] == u) pre += tw.cnt[slot_of(tw.left[p], n)];
-        u = p;
-    }
     const int lc = tw.left[i], rc = tw.right[i];
-    const int lslot = slot_of(lc, n);
-    const int right_pre = pre + 1 + tw.cnt[lslot];
     const int2 ri = tw.range[i];
+    const int pre = preorder_internal(tw, ri.x, tw.chain[i]);
+    const int rfirst = rc < 0 ? ~rc : tw.range[rc].x;
+    const bool rleaf = is_final_leaf(tw.splittable, rc);
+    const int right_pre = rleaf ? preorder_leaf(tw, rfirst) : preorder_internal(tw, rfirst, tw.chain[rc]);
     write_record<ORDER>(nodes, pre, load_slot<ORDER>(tw, i), node_theta2(seg, t, ri.x), right_pre, -1, err);
     register_root(seg, pre, ri.x, ri.y);
     if (is_final_leaf(tw.splittable, lc)) {
         int2 r = lc < 0 ? make_int2(~lc, ~lc) : tw.range[lc];
-        write_record<ORDER>(nodes, pre + 1, load_slot<ORDER>(tw, lslot), node_theta2(seg, t, r.x), r.x, r.y + 1, err);
+        write_record<ORDER>(nodes, pre + 1, load_slot<ORDER>(tw, slot_of(lc, n)), node_theta2(seg, t, r.x), r.x, r.y + 1,
+                            err);
         register_root(seg, pre + 1, r.x, r.y);
     }
-    if (is_final_leaf(tw.splittable, rc)) {
+    if (rleaf) {
         int2 r = rc < 0 ? make_int2(~rc, ~rc) : tw.range[rc];
         write_record<ORDER>(nodes, right_pre, load_slot<ORDER>(tw, slot_of(rc, n)), node_theta2(seg, t, r.x), r.x,
                             r.y + 1, err);
         register_root(seg, right_pre, r.x, r.y);
     }
-    if (i == 0) *tw.num_nodes = tw.cnt[i];
 }
 
 // Smallest float s >= 0 with RN(sqrt(s)) >= b (sqrt is monotone, so the set is an up-set).
@@ -511,32 +627,21 @@ __global__ void __launch_bounds__(kThreads) emit_dual_kernel(int n, TreeWorkspac
                                                               uint32_t *err) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1 || !tw.splittable[i]) return;
-    int pre = 0;
-    int depth = 0;
-    for (int u = i; u != 0; ++depth) {
-        const int p = tw.parent[u];
-        if (depth >= kMaxTreeDepth || p < 0 || p >= n - 1) {
-            atomicOr(err, (uint32_t) kErrTreeDepth);
-            return;
-        }
-        pre += 1;
-        if (tw.right[p] == u) pre += tw.cnt[slot_of(tw.left[p], n)];
-        u = p;
-    }
     const int lc = tw.left[i], rc = tw.right[i];
-    const int lslot = slot_of(lc, n);
-    const int right_pre = pre + 1 + tw.cnt[lslot];
     const int2 ri = tw.range[i];
+    const int pre = preorder_internal(tw, ri.x, tw.chain[i]);
+    const int rfirst = rc < 0 ? ~rc : tw.range[rc].x;
+    const bool rleaf = is_final_leaf(tw.splittable, rc);
+    const int right_pre = rleaf ? preorder_leaf(tw, rfirst) : preorder_internal(tw, rfirst, tw.chain[rc]);
     write_dual_record(nodes, pre, load_slot<3>(tw, i), ri.x, ri.y, right_pre, -1 - ri.x, theta, err);
     if (is_final_leaf(tw.splittable, lc)) {
         int2 r = lc < 0 ? make_int2(~lc, ~lc) : tw.range[lc];
-        write_dual_record(nodes, pre + 1, load_slot<3>(tw, lslot), r.x, r.y, r.x, r.y + 1, theta, err);
+        write_dual_record(nodes, pre + 1, load_slot<3>(tw, slot_of(lc, n)), r.x, r.y, r.x, r.y + 1, theta, err);
     }
-    if (is_final_leaf(tw.splittable, rc)) {
+    if (rleaf) {
         int2 r = rc < 0 ? make_int2(~rc, ~rc) : tw.range[rc];
         write_dual_record(nodes, right_pre, load_slot<3>(tw, slot_of(rc, n)), r.x, r.y, r.x, r.y + 1, theta, err);
     }
-    if (i == 0) *tw.num_nodes = tw.cnt[i];
 }
 
 __global__ void root_leaf_dual_kernel(const float4 *__restrict__ bodies, int n, TreeWorkspace tw, DualNodes nodes,
@@ -557,7 +662,26 @@ __global__ void root_leaf_kernel(const float4 *__restrict__ bodies, int n, TreeW
     *tw.num_nodes = 1;
 }
 
+// Karras topology, the final nodes per start position and their exclusive prefix (which also
+// gives the node count); clears the climb's arrival counters.
+void launch_topology(const uint64_t *sorted_codes, const int *inst_of, int n, int leaf, TreeWorkspace &tw,
+                     cudaStream_t s) {
+    const int internal = n - 1;
+    const int blocks = (internal + kThreads - 1) / kThreads;
+    const int64_t m = (int64_t) n + 1;
+    const int tiles = (int) build_scan_tiles(n);
+    cudaMemsetAsync(tw.start, 0, (size_t) m * sizeof(int), s);
+    cudaMemsetAsync(tw.visit, 0, (size_t) internal * sizeof(int), s);
+    karras_kernel<<<blocks, kThreads, 0, s>>>(sorted_codes, inst_of, n, leaf, tw.range, tw.left, tw.right, tw.parent,
+                                              tw.splittable, tw.start);
+    scan_tiles_kernel<<<tiles, kThreads, 0, s>>>(tw.start, m, tw.scan_part);
+    scan_parts_kernel<<<1, 1024, 0, s>>>(tw.scan_part, tiles, tw.num_nodes);
+    scan_apply_kernel<<<tiles, kThreads, 0, s>>>(tw.start, m, tw.scan_part, tw.prefix);
+}
+
 }  // namespace
+
+int64_t build_scan_tiles(int64_t n) { return (n + 1 + kScanTile - 1) / kScanTile; }
 
 void launch_build_dual_tree(const uint64_t *sorted_codes, const float4 *bodies, int64_t n64, int leaf, float theta,
                             TreeWorkspace &tw, const DualNodes &nodes, uint32_t *err, cudaStream_t s) {
@@ -569,9 +693,7 @@ void launch_build_dual_tree(const uint64_t *sorted_codes, const float4 *bodies, 
     const int internal = n - 1;
     const int blocks = internal > 0 ? (internal + kThreads - 1) / kThreads : 1;
     if (internal > 0) {
-        karras_kernel<<<blocks, kThreads, 0, s>>>(sorted_codes, nullptr, n, leaf, tw.range, tw.left, tw.right,
-                                                  tw.parent, tw.splittable);
-        cudaMemsetAsync(tw.visit, 0, (size_t) internal * sizeof(int), s);
+        launch_topology(sorted_codes, nullptr, n, leaf, tw, s);
         summarize_kernel<3><<<blocks, kThreads, 0, s>>>(bodies, n, tw, err);
         emit_dual_kernel<<<blocks, kThreads, 0, s>>>(n, tw, nodes, theta, err);
     }
@@ -589,11 +711,7 @@ void launch_build_tree(const uint64_t *sorted_codes, const float4 *bodies, int64
     const float t = theta * theta;  // the reference compares against theta * theta in float
     const int internal = n - 1;
     const int blocks = internal > 0 ? (internal + kThreads - 1) / kThreads : 1;
-    if (internal > 0) {
-        karras_kernel<<<blocks, kThreads, 0, s>>>(sorted_codes, seg.inst_of, n, leaf, tw.range, tw.left, tw.right,
-                                                  tw.parent, tw.splittable);
-        cudaMemsetAsync(tw.visit, 0, (size_t) internal * sizeof(int), s);
-    }
+    if (internal > 0) launch_topology(sorted_codes, seg.inst_of, n, leaf, tw, s);
     if (order == 1) {
         if (internal > 0) {
             summarize_kernel<1><<<blocks, kThreads, 0, s>>>(bodies, n, tw, err);

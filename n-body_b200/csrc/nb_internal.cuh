@@ -166,13 +166,19 @@ struct TreeWorkspace {
     float4 *sbmin = nullptr, *sbmax = nullptr, *scom = nullptr;  // 2n-1 summary slots
     float4 *sq0 = nullptr, *sq1 = nullptr;                        // quadrupole slots (order >= 2)
     float4 *sq2 = nullptr, *sq3 = nullptr;                        // octupole slots (order 3)
-    int *cnt = nullptr;             // subtree node count per slot
+    int *chain = nullptr;           // per final internal node: final internal nodes below it that share its first body
+    int *start = nullptr;           // per body position (n + 1): 2 x (final internal nodes whose range starts
+                                    // there) + 1 if a final leaf starts there
+    int *prefix = nullptr;          // per body position (n + 1): final nodes starting before it (exclusive scan)
+    int *scan_part = nullptr;       // per scan tile: its total, then its exclusive prefix
     int *num_nodes = nullptr;       // device scalar: final node count
     int64_t capacity = 0;
     // Precision option (0: off, the reference's FP32 operations everywhere): internal nodes of at
     // least this many bodies combine their children's summaries in FP64, rounded once to FP32.
     int fp64_min_bodies = 0;
 };
+// Scan tiles of the preorder prefix over n + 1 body positions (sizes tw.scan_part).
+int64_t build_scan_tiles(int64_t n);
 void launch_build_tree(const uint64_t *sorted_codes, const float4 *bodies, int64_t n, int leaf, int order, float theta,
                        TreeWorkspace &tw, const NodeArrays &nodes, uint32_t *err, cudaStream_t s,
                        const BatchSegments &seg = BatchSegments());
