@@ -608,11 +608,13 @@ def run_batched(args):
         t0 = torch.cuda.Event(enable_timing=True)
         t1 = torch.cuda.Event(enable_timing=True)
         flush.zero_()
-        t0.record(stream)
-        s.step(args.steps)
-        t1.record(stream)
-        torch.cuda.synchronize(device)
+        with Clocks(device) as clk:
+            t0.record(stream)
+            s.step(args.steps)
+            t1.record(stream)
+            torch.cuda.synchronize(device)
         batch_ms = t0.elapsed_time(t1)
+        clocks = clk.summary()
         s.enable_timing(True)
         s.step(2)
         phases = s.phase_times()
@@ -666,6 +668,7 @@ def run_batched(args):
                      "method": "force passes of this batch at each candidate leaf size (default launch shape), "
                                "then at each launch shape (threads per block x traversal tile), fastest kept"},
         "accuracy": accuracy,
+        "clocks": clocks,
         "phases_ms_per_step": {k: phases[k] / max(phases["passes"], 1) for k in
                                ("bbox_ms", "morton_ms", "sort_ms", "gather_ms", "build_ms", "traverse_ms",
                                 "integrate_ms")},
@@ -848,14 +851,18 @@ def run_serving(args):
     leaf, tuned = serving_leaf(nb, sample, eps)
     shape = tuned.shape
     versus = serving_sample_vs_sequential(nb, sample, eps, leaf, torch, shape=shape)
-    overload = serve_run(nb, pools, args.rate, args.duration, rng, eps, leaf=leaf, shape=shape)
+    with Clocks(local) as clk:
+        overload = serve_run(nb, pools, args.rate, args.duration, rng, eps, leaf=leaf, shape=shape)
+    overload["clocks"] = clk.summary()
     # the server's own throughput (re-layouts, admission and retirement included) on the stream
     versus["ratio_served_over_sequential"] = (overload["throughput_body_steps_per_s"] /
                                               versus["sequential_plain_body_steps_per_s"])
     # calibrated run: arrival rate at 70 % of the measured capacity for the mean request size
     mean_work = np.mean([np.exp(rng.uniform(np.log(2048), np.log(1 << 21))) for _ in range(20000)]) * 505.0
     rate = max(0.7 * overload["throughput_body_steps_per_s"] / mean_work, 0.05)
-    calibrated = serve_run(nb, pools, rate, args.duration, rng, eps, drain=args.duration, leaf=leaf, shape=shape)
+    with Clocks(local) as clk:
+        calibrated = serve_run(nb, pools, rate, args.duration, rng, eps, drain=args.duration, leaf=leaf, shape=shape)
+    calibrated["clocks"] = clk.summary()
     line = {
         "metric": "serving: aggregate body-steps/s and request latency p50/p99 (Poisson arrivals)",
         "value": overload["throughput_body_steps_per_s"], "unit": "body-steps/s", "n_gpus": world,

@@ -184,6 +184,12 @@ int nb_enable_graphs(nb_ctx *ctx, int enable);
  * of those nodes are no longer bit-identical to the reference's FP32 ones. */
 int nb_set_fp64_summaries(nb_ctx *ctx, int64_t min_bodies);
 
+/* Self-test of the device-side bounded waits (no counterpart in the reference, which has no device
+ * waits): runs one radix-sort pass on `device` whose look-back can never complete (every index in
+ * bounds), with its wait limited to wait_ms (1..2000) milliseconds. Returns NB_ERR_DEVICE_TIMEOUT
+ * when the wait ended at its limit and reported it, as designed; the device stays usable. */
+int nb_selftest_bounded_wait(int32_t device, int32_t wait_ms);
+
 /* Launch shape of the Barnes-Hut traversal (no counterpart in the reference, whose TBB loop has no
  * such knob; LinearBVH::maxLeafSize, LinearBVH.h:135-137, is the one it has): block_threads
  * threads per block (128 or 256) and slab_entries staged partially accepted nodes per warp (32 or

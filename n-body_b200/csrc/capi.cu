@@ -1213,6 +1213,19 @@ int nb_set_fp64_summaries(nb_ctx *ctx, int64_t min_bodies) {
     return NB_OK;
 }
 
+int nb_selftest_bounded_wait(int32_t device, int32_t wait_ms) {
+    if (wait_ms < 1 || wait_ms > 2000) return NB_ERR_INVALID_ARGUMENT;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        cudaGetLastError();
+        return NB_ERR_CUDA;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) return NB_ERR_CUDA;
+    uint32_t e = 0;
+    if (lookback_timeout_selftest((unsigned long long) wait_ms * 1000000ull, &e) != cudaSuccess) return NB_ERR_CUDA;
+    return (e & kErrLookbackTimeout) ? NB_ERR_DEVICE_TIMEOUT : NB_OK;
+}
+
 int nb_set_traversal_shape(nb_ctx *ctx, int32_t block_threads, int32_t slab_entries) {
     if (!ctx) return NB_ERR_INVALID_ARGUMENT;
     if (block_threads == 0) block_threads = 256;

@@ -139,6 +139,9 @@ size_t sort_lookback_words(int64_t n);
 // cudaPeekAtLastError, which clears nothing).
 cudaError_t launch_radix_sort(uint64_t *keys, uint32_t *vals, int64_t n, SortWorkspace &ws, uint32_t *err,
                               cudaStream_t s);
+// Self-test of the bounded look-back wait: one pass that can never complete its look-back runs
+// with the given wait limit; the error word it leaves is returned (kErrLookbackTimeout expected).
+cudaError_t lookback_timeout_selftest(unsigned long long wait_limit_ns, uint32_t *err_word);
 // One stable one-sweep pass on digit `pass` (bits 8*pass .. 8*pass+7) of the keys. offsets holds
 // the exclusive digit prefixes at [pass*256 + d] and a trivial-pass flag at [8*256 + pass];
 // lookback (pass x tiles x 256 words) and tile_counter[pass] must be zero. Pass 0 ignores vals_in

@@ -80,7 +80,8 @@ __global__ void __launch_bounds__(kThreads) onesweep_kernel(const uint64_t *__re
                                                             const uint32_t *__restrict__ offsets,
                                                             uint32_t *__restrict__ lookback,
                                                             uint32_t *__restrict__ tile_counter,
-                                                            uint32_t *__restrict__ err) {
+                                                            uint32_t *__restrict__ err,
+                                                            unsigned long long wait_limit_ns) {
     __shared__ uint64_t s_keys[kTile];
     __shared__ uint32_t s_vals[kTile];
     __shared__ uint32_t s_whist[kWarps][256];
@@ -181,7 +182,7 @@ __global__ void __launch_bounds__(kThreads) onesweep_kernel(const uint64_t *__re
             uint32_t w = load_volatile(lookback + ((int64_t) pass * num_tiles + t) * 256 + d);
             uint32_t f = w & kFlagMask;
             if (f == 0u) {
-                if (global_timer_ns() - t0 > kWaitLimitNs) {
+                if (global_timer_ns() - t0 > wait_limit_ns) {
                     atomicOr(err, (uint32_t) kErrLookbackTimeout);
                     break;
                 }
@@ -229,7 +230,7 @@ void launch_radix_pass(const uint64_t *keys_in, const uint32_t *vals_in, uint64_
                        uint32_t *err, cudaStream_t s) {
     if (n <= 0) return;
     onesweep_kernel<<<(unsigned) sort_tiles(n), kThreads, 0, s>>>(keys_in, vals_in, keys_out, vals_out, n, pass,
-                                                                   offsets, lookback, tile_counter, err);
+                                                                   offsets, lookback, tile_counter, err, kWaitLimitNs);
 }
 
 cudaError_t launch_radix_sort(uint64_t *keys, uint32_t *vals, int64_t n, SortWorkspace &ws, uint32_t *err,
@@ -246,7 +247,7 @@ cudaError_t launch_radix_sort(uint64_t *keys, uint32_t *vals, int64_t n, SortWor
     uint32_t *vin = vals, *vout = ws.vals_alt;
     for (int p = 0; p < kPasses; ++p) {
         onesweep_kernel<<<(unsigned) tiles, kThreads, 0, s>>>(kin, vin, kout, vout, n, p, ws.offsets, ws.lookback,
-                                                               ws.tile_counter, err);
+                                                               ws.tile_counter, err, kWaitLimitNs);
         if ((e = cudaPeekAtLastError()) != cudaSuccess) return e;
         uint64_t *tk = kin; kin = kout; kout = tk;
         uint32_t *tv = vin; vin = vout; vout = tv;
@@ -254,6 +255,50 @@ cudaError_t launch_radix_sort(uint64_t *keys, uint32_t *vals, int64_t n, SortWor
     // An even number of passes leaves the result in (keys, vals).
     static_assert(kPasses % 2 == 0, "the sorted data must end in the caller's buffers");
     return cudaSuccess;
+}
+
+}  // namespace nbg
+
+namespace nbg {
+
+// One pass whose look-back can never complete, to check that the bounded wait ends: a single block
+// is launched with its tile ticket preset to 1, so it takes tile 1 of a two-tile input and waits on
+// tile 0's flags, which nothing ever publishes. Every index stays in bounds: keys and values hold
+// two tiles, the look-back buffer two tiles of 256 flags (the kernel indexes it with gridDim = 1),
+// and the tile's scatter writes within the first tile's positions. Returns the error word.
+cudaError_t lookback_timeout_selftest(unsigned long long wait_limit_ns, uint32_t *err_word) {
+    const int64_t n = 2 * kTile;
+    uint64_t *keys = nullptr, *keys_out = nullptr;
+    uint32_t *vals = nullptr, *vals_out = nullptr, *offsets = nullptr, *lookback = nullptr, *ticket = nullptr,
+             *err = nullptr;
+    cudaError_t e = cudaSuccess;
+    auto alloc = [&](void **p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(p, bytes);
+        if (e == cudaSuccess) e = cudaMemset(*p, 0, bytes);
+    };
+    alloc((void **) &keys, n * sizeof(uint64_t));
+    alloc((void **) &keys_out, n * sizeof(uint64_t));
+    alloc((void **) &vals, n * sizeof(uint32_t));
+    alloc((void **) &vals_out, n * sizeof(uint32_t));
+    alloc((void **) &offsets, (kPasses * 256 + kPasses) * sizeof(uint32_t));  // no pass is trivial
+    alloc((void **) &lookback, 2 * 256 * sizeof(uint32_t));
+    alloc((void **) &ticket, kPasses * sizeof(uint32_t));
+    alloc((void **) &err, sizeof(uint32_t));
+    if (e == cudaSuccess) {
+        const uint32_t one = 1;
+        e = cudaMemcpy(ticket, &one, sizeof(one), cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) {
+        onesweep_kernel<<<1, kThreads>>>(keys, vals, keys_out, vals_out, n, 0, offsets, lookback, ticket, err,
+                                         wait_limit_ns);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(err_word, err, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    for (void *p: {(void *) keys, (void *) keys_out, (void *) vals, (void *) vals_out, (void *) offsets,
+                   (void *) lookback, (void *) ticket, (void *) err})
+        if (p) cudaFree(p);
+    return e;
 }
 
 }  // namespace nbg

@@ -25,6 +25,14 @@ PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.path.join(PKG_ROOT, "lib", "libnbody_b200.so")
 
 NB_OK = 0
+# error codes of include/nbody_gpu.h
+NB_ERR_INVALID_ARGUMENT = -1
+NB_ERR_CUDA = -2
+NB_ERR_OUT_OF_MEMORY = -3
+NB_ERR_NO_BODIES = -4
+NB_ERR_DEVICE_TIMEOUT = -5
+NB_ERR_UNSUPPORTED = -6
+NB_ERR_DEVICE_CHECK = -7
 _STATUS = {
     -1: "invalid argument",
     -2: "CUDA error",
@@ -142,6 +150,7 @@ SIGNATURES = {
     "nb_enable_graphs": (C.c_int, [_vp, C.c_int]),
     "nb_set_fp64_summaries": (C.c_int, [_vp, C.c_int64]),
     "nb_set_traversal_shape": (C.c_int, [_vp, _i32, _i32]),
+    "nb_selftest_bounded_wait": (C.c_int, [_i32, _i32]),
     "nb_get_traversal_shape": (C.c_int, [_vp, C.POINTER(_i32), C.POINTER(_i32)]),
     "nb_server_create": (C.c_int, [C.POINTER(Config), C.c_uint64, C.POINTER(_vp)]),
     "nb_server_destroy": (C.c_int, [_vp]),
