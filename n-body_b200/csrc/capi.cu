@@ -268,6 +268,7 @@ void free_buffers(nb_ctx *ctx) {
     dev_free(ctx->tw.splittable); dev_free(ctx->tw.visit); dev_free(ctx->tw.sbmin); dev_free(ctx->tw.sbmax);
     dev_free(ctx->tw.scom); dev_free(ctx->tw.sq0); dev_free(ctx->tw.sq1); dev_free(ctx->tw.chain);
     dev_free(ctx->tw.start); dev_free(ctx->tw.prefix); dev_free(ctx->tw.scan_part);
+    dev_free(ctx->tw.leaf_parents); dev_free(ctx->tw.leaf_parents_count);
     dev_free(ctx->nodes.mac); dev_free(ctx->nodes.link); dev_free(ctx->nodes.pay);
     ctx->nodes.capacity = 0;
     ctx->cap = 0;
@@ -303,6 +304,8 @@ int ensure_capacity(nb_ctx *ctx, int64_t n) {
     NB_TRY(dev_alloc(&ctx->tw.sq0, slots), "alloc summaries");
     NB_TRY(dev_alloc(&ctx->tw.sq1, slots), "alloc summaries");
     NB_TRY(dev_alloc(&ctx->tw.chain, c), "alloc tree");
+    NB_TRY(dev_alloc(&ctx->tw.leaf_parents, c), "alloc tree");
+    NB_TRY(dev_alloc(&ctx->tw.leaf_parents_count, 1), "alloc tree");
     NB_TRY(dev_alloc(&ctx->tw.start, c + 1), "alloc tree");
     NB_TRY(dev_alloc(&ctx->tw.prefix, c + 1), "alloc tree");
     NB_TRY(dev_alloc(&ctx->tw.scan_part, build_scan_tiles(c)), "alloc tree");

@@ -30,6 +30,7 @@
 //                     are those starting before f (the prefix at f) and, among the internal nodes
 //                     starting at f (a chain of left children), the larger ones; a leaf starting at f
 //                     comes after that whole chain.
+#include <algorithm>
 #include <cfloat>
 
 #include "nb_internal.cuh"
@@ -66,7 +67,9 @@ __global__ void __launch_bounds__(kThreads) karras_kernel(const uint64_t *__rest
                                                           const int *__restrict__ inst_of, int n, int leaf,
                                                           int2 *__restrict__ range, int *__restrict__ left,
                                                           int *__restrict__ right, int *__restrict__ parent,
-                                                          uint8_t *__restrict__ splittable, int *__restrict__ start) {
+                                                          uint8_t *__restrict__ splittable, int *__restrict__ start,
+                                                          int *__restrict__ leaf_parents,
+                                                          int *__restrict__ leaf_parents_count) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
     const int dn = prefix_delta(codes, inst_of, n, i, i + 1);
@@ -99,8 +102,11 @@ __global__ void __launch_bounds__(kThreads) karras_kernel(const uint64_t *__rest
     if (split) {
         // a final internal node starts at `first`; a child that is not split is a final leaf
         atomicAdd(start + first, 2);
-        if (lc < 0 || !range_splittable(codes, inst_of, leaf, first, gamma)) atomicAdd(start + first, 1);
-        if (rc < 0 || !range_splittable(codes, inst_of, leaf, gamma + 1, last)) atomicAdd(start + gamma + 1, 1);
+        const bool lleaf = lc < 0 || !range_splittable(codes, inst_of, leaf, first, gamma);
+        const bool rleaf = rc < 0 || !range_splittable(codes, inst_of, leaf, gamma + 1, last);
+        if (lleaf) atomicAdd(start + first, 1);
+        if (rleaf) atomicAdd(start + gamma + 1, 1);
+        if (lleaf || rleaf) leaf_parents[atomicAdd(leaf_parents_count, 1)] = i;
     }
 }
 
@@ -452,11 +458,9 @@ __device__ __forceinline__ int arrive_acq_rel(int *p) {
     return old;
 }
 
+// Leaf summaries of final internal node i's final-leaf children, then the climb.
 template<int ORDER>
-__global__ void __launch_bounds__(kThreads) summarize_kernel(const float4 *__restrict__ bodies, int n, TreeWorkspace tw,
-                                                             uint32_t *err) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n - 1 || !tw.splittable[i]) return;
+__device__ void summarize_from(const float4 *__restrict__ bodies, int n, const TreeWorkspace &tw, uint32_t *err, int i) {
     for (int side = 0; side < 2; ++side) {
         const int c = side ? tw.right[i] : tw.left[i];
         if (!is_final_leaf(tw.splittable, c)) continue;
@@ -492,6 +496,16 @@ __global__ void __launch_bounds__(kThreads) summarize_kernel(const float4 *__res
             p = tw.parent[p];
         }
     }
+}
+
+// One thread per final internal node with leaf children (the compact list karras_kernel built), on
+// a grid of a few waves at most.
+template<int ORDER>
+__global__ void __launch_bounds__(kThreads) summarize_kernel(const float4 *__restrict__ bodies, int n, TreeWorkspace tw,
+                                                             uint32_t *err) {
+    const int count = *tw.leaf_parents_count;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x)
+        summarize_from<ORDER>(bodies, n, tw, err, tw.leaf_parents[idx]);
 }
 
 // Smallest float b such that RN(a / b) < t, i.e. d2 >= b <=> the reference's
@@ -662,6 +676,14 @@ __global__ void root_leaf_kernel(const float4 *__restrict__ bodies, int n, TreeW
     *tw.num_nodes = 1;
 }
 
+// Grid of the summary climb: enough threads for every possible leaf parent, capped at a few waves
+// (the kernel loops over the compact list).
+int summarize_blocks(int n) {
+    const int64_t need = ((int64_t) n - 1 + kThreads - 1) / kThreads;
+    const int64_t cap = (int64_t) current_sm_count() * 8;
+    return (int) std::max<int64_t>(1, std::min(need, cap));
+}
+
 // Karras topology, the final nodes per start position and their exclusive prefix (which also
 // gives the node count); clears the climb's arrival counters.
 void launch_topology(const uint64_t *sorted_codes, const int *inst_of, int n, int leaf, TreeWorkspace &tw,
@@ -672,8 +694,9 @@ void launch_topology(const uint64_t *sorted_codes, const int *inst_of, int n, in
     const int tiles = (int) build_scan_tiles(n);
     cudaMemsetAsync(tw.start, 0, (size_t) m * sizeof(int), s);
     cudaMemsetAsync(tw.visit, 0, (size_t) internal * sizeof(int), s);
+    cudaMemsetAsync(tw.leaf_parents_count, 0, sizeof(int), s);
     karras_kernel<<<blocks, kThreads, 0, s>>>(sorted_codes, inst_of, n, leaf, tw.range, tw.left, tw.right, tw.parent,
-                                              tw.splittable, tw.start);
+                                              tw.splittable, tw.start, tw.leaf_parents, tw.leaf_parents_count);
     scan_tiles_kernel<<<tiles, kThreads, 0, s>>>(tw.start, m, tw.scan_part);
     scan_parts_kernel<<<1, 1024, 0, s>>>(tw.scan_part, tiles, tw.num_nodes);
     scan_apply_kernel<<<tiles, kThreads, 0, s>>>(tw.start, m, tw.scan_part, tw.prefix);
@@ -694,7 +717,7 @@ void launch_build_dual_tree(const uint64_t *sorted_codes, const float4 *bodies, 
     const int blocks = internal > 0 ? (internal + kThreads - 1) / kThreads : 1;
     if (internal > 0) {
         launch_topology(sorted_codes, nullptr, n, leaf, tw, s);
-        summarize_kernel<3><<<blocks, kThreads, 0, s>>>(bodies, n, tw, err);
+        summarize_kernel<3><<<summarize_blocks(n), kThreads, 0, s>>>(bodies, n, tw, err);
         emit_dual_kernel<<<blocks, kThreads, 0, s>>>(n, tw, nodes, theta, err);
     }
     root_leaf_dual_kernel<<<1, 1, 0, s>>>(bodies, n, tw, nodes, theta, err);
@@ -714,13 +737,13 @@ void launch_build_tree(const uint64_t *sorted_codes, const float4 *bodies, int64
     if (internal > 0) launch_topology(sorted_codes, seg.inst_of, n, leaf, tw, s);
     if (order == 1) {
         if (internal > 0) {
-            summarize_kernel<1><<<blocks, kThreads, 0, s>>>(bodies, n, tw, err);
+            summarize_kernel<1><<<summarize_blocks(n), kThreads, 0, s>>>(bodies, n, tw, err);
             emit_kernel<1><<<blocks, kThreads, 0, s>>>(n, tw, t, nodes, err, seg);
         }
         root_leaf_kernel<1><<<1, 1, 0, s>>>(bodies, n, tw, t, nodes, err, seg);
     } else {
         if (internal > 0) {
-            summarize_kernel<2><<<blocks, kThreads, 0, s>>>(bodies, n, tw, err);
+            summarize_kernel<2><<<summarize_blocks(n), kThreads, 0, s>>>(bodies, n, tw, err);
             emit_kernel<2><<<blocks, kThreads, 0, s>>>(n, tw, t, nodes, err, seg);
         }
         root_leaf_kernel<2><<<1, 1, 0, s>>>(bodies, n, tw, t, nodes, err, seg);

@@ -174,6 +174,9 @@ struct TreeWorkspace {
                                     // there) + 1 if a final leaf starts there
     int *prefix = nullptr;          // per body position (n + 1): final nodes starting before it (exclusive scan)
     int *scan_part = nullptr;       // per scan tile: its total, then its exclusive prefix
+    int *leaf_parents = nullptr;    // final internal nodes with at least one final-leaf child (n - 1),
+                                    // in no particular order; the count is leaf_parents_count[0]
+    int *leaf_parents_count = nullptr;
     int *num_nodes = nullptr;       // device scalar: final node count
     int64_t capacity = 0;
     // Precision option (0: off, the reference's FP32 operations everywhere): internal nodes of at
