@@ -203,7 +203,9 @@ void free_dual(nb_ctx *ctx) {
     ctx->dws.arena_words = 0;
     NearPool &np = ctx->dws.near;
     dev_free(np.head); dev_free(np.items); dev_free(np.words); dev_free(np.units); dev_free(np.counters);
+    dev_free(np.walk_stack);
     np.head_cap = np.item_cap = np.word_cap = np.unit_cap = 0;
+    np.walk_warps = 0;
     SpillPool &sp = ctx->dws.spill;
     dev_free(sp.head); dev_free(sp.recs); dev_free(sp.rec_field); dev_free(sp.words); dev_free(sp.work);
     dev_free(sp.counters);
@@ -245,6 +247,8 @@ int ensure_dual(nb_ctx *ctx) {
     NB_TRY(dev_alloc(&np.units, (size_t) np.unit_cap), "alloc near-field pool");
     NB_TRY(dev_alloc(&np.counters, 4), "alloc near-field pool");
     if (ctx->dws.near_blocks == 0) ctx->dws.near_blocks = dual_near_blocks(ctx->cfg.device);
+    np.walk_warps = (int64_t) ctx->dws.near_blocks * dual_near_warps_per_block();
+    NB_TRY(dev_alloc(&np.walk_stack, (size_t) np.walk_warps * kNearWalkStack), "alloc near-field walk stacks");
     SpillPool &sp = ctx->dws.spill;
     sp.head_cap = (int64_t) slots;
     sp.work_cap = (int64_t) slots;

@@ -103,21 +103,25 @@ __device__ __forceinline__ float sep_box(const DNode &a, const DNode &b) {
 
 // sep(node, p) >= B, exactly, with the node's thresholds (B, S): when one of the two separation
 // vectors is zero, sep is RN(sqrt(|v|^2)) and the test is |v|^2 >= S; otherwise the double path.
-__device__ __forceinline__ bool sep_at_least(const DNode &n, const float p[3], float B, float S) {
-    const float ux = max0(fsub(n.mn[0], p[0])), uy = max0(fsub(n.mn[1], p[1])), uz = max0(fsub(n.mn[2], p[2]));
-    const float vx = max0(fsub(p[0], n.mx[0])), vy = max0(fsub(p[1], n.mx[1])), vz = max0(fsub(p[2], n.mx[2]));
-    const float su = fadd(fadd(fmul(ux, ux), fmul(uy, uy)), fmul(uz, uz));
-    const float sv = fadd(fadd(fmul(vx, vx), fmul(vy, vy)), fmul(vz, vz));
+// sep >= B from the squared lengths su, sv of the two separation vectors (non-decreasing in both).
+__device__ __forceinline__ bool sep_test(float su, float sv, float B, float S) {
     if (sv == 0.f) return su >= S;
     if (su == 0.f) return sv >= S;
     return sep_from(__fsqrt_rn(su), __fsqrt_rn(sv)) >= B;
 }
+// Squared length of the per-axis gaps (max0(a - b))_k, in the reference's operation order.
+__device__ __forceinline__ float gap2(float a0, float a1, float a2, float b0, float b1, float b2) {
+    const float x = max0(fsub(a0, b0)), y = max0(fsub(a1, b1)), z = max0(fsub(a2, b2));
+    return fadd(fadd(fmul(x, x), fmul(y, y)), fmul(z, z));
+}
+__device__ __forceinline__ bool sep_at_least(const DNode &n, const float p[3], float B, float S) {
+    return sep_test(gap2(n.mn[0], n.mn[1], n.mn[2], p[0], p[1], p[2]), gap2(p[0], p[1], p[2], n.mx[0], n.mx[1], n.mx[2]),
+                    B, S);
+}
 
 // DiagonalOverSeparation (DiagonalOverSeparation.h:29-49), (active node, point): approximate the
-// node for the point, RN(diag / sep) < theta and more than 32 bodies. thr = node thresholds.
-__device__ __forceinline__ bool approx_for_point(const DNode &a, float4 thr, const float p[3]) {
-    return a.size > 32 && sep_at_least(a, p, thr.x, thr.y);
-}
+// node for the point iff RN(diag / sep) < theta and it has more than 32 bodies; chunk_walk decides
+// it per target (sep_at_least with the node's thresholds) and for boxes of targets (classify_group).
 // (point, passive node): the active point is far from the passive node, RN(3 diag / sep) < theta
 __device__ __forceinline__ bool point_is_far(const float p[3], const DNode &P, float4 thr) {
     return sep_at_least(P, p, thr.z, thr.w);
@@ -908,13 +912,15 @@ __global__ void load_balanced_break_kernel(DualNodes nodes, const int *__restric
 
 constexpr int kNearThreads = 256;
 constexpr int kNearWarps = kNearThreads / 32;
-constexpr int kNearStack = kMaxTreeDepth + 4;  // (node, target mask) entries of one warp's walk
 constexpr int kPriv = 16;                      // queued M2P nodes per target
 
+constexpr int kNearLeaves = 64;  // opened leaves of a walk waiting for their pair tiles
+
 struct NearWarp {
-    int2 stack[kNearStack];
     int priv[kPriv][32];  // [slot][target]
     float4 tile[32];      // staged source bodies (16 interleaved pairs), then the replicas' partial sums
+    float4 tpos[32];      // the unit's targets (replica-0 lanes)
+    int4 leaf[kNearLeaves];  // opened leaves: (first body, end body, target mask, 0)
 };
 
 struct Lane {
@@ -1042,64 +1048,137 @@ __device__ void flush_priv(const Ctx &x, NearWarp &w, const Lane &L, int plen, c
     __syncwarp();
 }
 
-// activeTree (activeTree.h:24-79) from `root` for the unit's targets (bits of `tmask`): one stack
-// entry per node with the targets that still descend; approximated nodes are queued per target.
+enum : int { kGroupAccept = 1, kGroupOpen = 2, kGroupMixed = 3 };
+
+// The point criterion decided for every target in the box [lo, hi] at once: a target's separation
+// gaps are bounded below by the gaps to the box's nearest corner and above by those to its
+// farthest one, computed with the same IEEE operations, and sep_test is non-decreasing in both
+// squared lengths; so "all approximate" / "none approximates" are exact. A node of at most 32
+// bodies is never approximated.
+__device__ __forceinline__ int classify_group(const DNode &nd, float4 thr, const float lo[3], const float hi[3]) {
+    if (nd.size <= 32) return kGroupOpen;
+    const float su_lo = gap2(nd.mn[0], nd.mn[1], nd.mn[2], hi[0], hi[1], hi[2]);
+    const float sv_lo = gap2(lo[0], lo[1], lo[2], nd.mx[0], nd.mx[1], nd.mx[2]);
+    if (sep_test(su_lo, sv_lo, thr.x, thr.y)) return kGroupAccept;
+    const float su_hi = gap2(nd.mn[0], nd.mn[1], nd.mn[2], lo[0], lo[1], lo[2]);
+    const float sv_hi = gap2(hi[0], hi[1], hi[2], nd.mx[0], nd.mx[1], nd.mx[2]);
+    if (!sep_test(su_hi, sv_hi, thr.x, thr.y)) return kGroupOpen;
+    return kGroupMixed;
+}
+
+__device__ __forceinline__ uint32_t near_lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Pairs of the listed opened leaves with the targets that opened them (pair tiles, replicas split).
 template<bool EPS0>
-__device__ void warp_walk(const Ctx &x, NearWarp &w, const Lane &L, int root, unsigned tmask, const float p[3],
-                          float a[3], int &plen, unsigned long long &npp, unsigned long long &nnp, uint32_t *err) {
-    const int lane = threadIdx.x & 31;
-    const unsigned lead = L.T >= 32 ? 0xffffffffu : ((1u << L.T) - 1u);  // replica-0 lanes = target bits
-    int sp = 1;
-    if (lane == 0) w.stack[0] = make_int2(root, (int) tmask);
-    __syncwarp();
-    while (sp > 0) {
-        --sp;
-        const int2 e = w.stack[sp];
-        __syncwarp();
-        const int k = e.x;
-        const unsigned m = (unsigned) e.y;
-        const DNode nd = load_node(x.nodes, k);
-        const bool in = L.active && ((m >> L.t) & 1u);
-        const bool ap = in && approx_for_point(nd, __ldg(x.nodes.thr + k), p);
-        if (ap && L.r == 0) {
-            w.priv[plen][L.t] = k;
-            ++plen;
-            if (L.counted) ++nnp;
-        }
-        if (__any_sync(0xffffffffu, plen == kPriv)) {
-            __syncwarp();
-            flush_priv(x, w, L, plen, p, a);
-            plen = 0;
-        }
-        const unsigned need = m & ~(__ballot_sync(0xffffffffu, ap) & lead);
-        if (need == 0) continue;
-        if (nd.leaf()) {
-            if (!x.range_ok(nd.link0, nd.link1)) {
-                if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
-                continue;
-            }
-            const bool mine = L.active && ((need >> L.t) & 1u);
-            const int first = nd.link0;
-            pair_tile<EPS0>(w, L, nd.link1 - nd.link0, [&](int j) { return __ldg(x.bodies + first + j); }, mine, p,
-                            x.eps, a);
-            if (mine && L.counted) npp += (unsigned long long) (nd.link1 - nd.link0);
-        } else {
-            if (!x.left_ok(k) || !x.right_ok(k, nd.link0)) {
-                if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
-                continue;
-            }
-            if (sp + 2 > kNearStack) {
-                if (lane == 0) atomicOr(err, (uint32_t) kErrStackOverflow);
-                return;
-            }
-            if (lane == 0) {
-                w.stack[sp] = make_int2(nd.link0, (int) need);  // right child, second
-                w.stack[sp + 1] = make_int2(k + 1, (int) need);  // left child, first
-            }
-            sp += 2;
-            __syncwarp();
-        }
+__device__ void flush_leaves(const Ctx &x, NearWarp &w, const Lane &L, int &nleaf, const float p[3], float a[3],
+                             unsigned long long &npp) {
+    for (int j = 0; j < nleaf; ++j) {
+        const int4 lf = w.leaf[j];
+        const bool mine = L.active && (((unsigned) lf.z >> L.t) & 1u);
+        const int first = lf.x;
+        pair_tile<EPS0>(w, L, lf.y - lf.x, [&](int jj) { return __ldg(x.bodies + first + jj); }, mine, p, x.eps, a);
+        if (mine && L.counted) npp += (unsigned long long) (lf.y - lf.x);
     }
+    nleaf = 0;
+    __syncwarp();
+}
+
+// activeTree (activeTree.h:24-79) for the unit's targets from the `top` roots on the warp's stack,
+// walked 32 entries per round: each lane classifies one (node, target mask) entry for the whole
+// box of targets (classify_group), nodes left mixed are decided per target, approximated nodes are
+// queued per target (M2P), opened leaves are listed for pair tiles, and opened internal nodes push
+// both children with the targets that opened them. Every target takes exactly the reference's
+// decisions; a round whose pushes would not fit the stack ends the walk with kErrStackOverflow.
+template<bool EPS0>
+__device__ void chunk_walk(const Ctx &x, NearWarp &w, const Lane &L, int2 *stack, int top, const float lo[3],
+                           const float hi[3], const float p[3], float a[3], int &plen, unsigned long long &npp,
+                           unsigned long long &nnp, uint32_t *err) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = near_lanemask_lt();
+    int nleaf = 0;
+    int64_t rounds = 0;
+    const int64_t round_limit = 4 * (int64_t) x.nn + 64;
+    while (top > 0) {
+        if (++rounds > round_limit) {
+            if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
+            break;
+        }
+        const int k = min(32, top);
+        const int base = top - k;
+        top = base;
+        int c = 0, l0 = 0, l1 = -1;
+        unsigned A = 0, O = 0;
+        if (lane < k) {
+            const int2 e = stack[base + lane];
+            c = e.x;
+            const unsigned m = (unsigned) e.y;
+            const DNode nd = load_node(x.nodes, c);
+            const float4 thr = __ldg(x.nodes.thr + c);
+            l0 = nd.link0;
+            l1 = nd.link1;
+            const int cls = classify_group(nd, thr, lo, hi);
+            if (cls == kGroupAccept) {
+                A = m;
+            } else if (cls == kGroupOpen) {
+                O = m;
+            } else {
+                unsigned bits = 0;
+                for (int t = 0; t < L.T; ++t) {
+                    const float4 tp = w.tpos[t];
+                    const float pt[3] = {tp.x, tp.y, tp.z};
+                    if (sep_at_least(nd, pt, thr.x, thr.y)) bits |= 1u << t;
+                }
+                A = bits & m;
+                O = m & ~A;
+            }
+        }
+        __syncwarp();  // popped entries are read before children overwrite them
+        const bool is_leaf = O != 0 && l1 >= 0, is_inner = O != 0 && l1 < 0;
+        const bool leaf_ok = is_leaf && x.range_ok(l0, l1);
+        const bool inner_ok = is_inner && x.left_ok(c) && x.right_ok(c, l0);
+        if ((is_leaf && !leaf_ok) || (is_inner && !inner_ok)) atomicOr(err, (uint32_t) kErrTraverseLimit);
+        // approximated: queued per target (M2P), in lane order of the round
+        uint32_t pend = __ballot_sync(0xffffffffu, A != 0);
+        while (pend) {
+            const int src = __ffs(pend) - 1;
+            pend &= pend - 1;
+            const int node = __shfl_sync(0xffffffffu, c, src);
+            const unsigned am = __shfl_sync(0xffffffffu, A, src);
+            if (__any_sync(0xffffffffu, plen == kPriv)) {
+                flush_priv(x, w, L, plen, p, a);
+                plen = 0;
+            }
+            if (L.active && L.r == 0 && ((am >> L.t) & 1u)) {
+                w.priv[plen][L.t] = node;
+                ++plen;
+                if (L.counted) ++nnp;
+            }
+        }
+        // opened leaves: listed, pair tiles when the list could overflow
+        uint32_t b = __ballot_sync(0xffffffffu, leaf_ok);
+        if (nleaf + __popc(b) > kNearLeaves) flush_leaves<EPS0>(x, w, L, nleaf, p, a, npp);
+        if (leaf_ok) w.leaf[nleaf + __popc(b & lt)] = make_int4(l0, l1, (int) O, 0);
+        nleaf += __popc(b);
+        // opened internal nodes: both children, left popped first
+        b = __ballot_sync(0xffffffffu, inner_ok);
+        if (top + 2 * __popc(b) > kNearWalkStack) {
+            if (lane == 0) atomicOr(err, (uint32_t) kErrStackOverflow);
+            top = 0;
+        } else {
+            if (inner_ok) {
+                const int sp = top + 2 * __popc(b & lt);
+                stack[sp] = make_int2(l0, (int) O);
+                stack[sp + 1] = make_int2(c + 1, (int) O);
+            }
+            top += 2 * __popc(b);
+        }
+        __syncwarp();
+    }
+    flush_leaves<EPS0>(x, w, L, nleaf, p, a, npp);
 }
 
 template<bool EPS0>
@@ -1111,6 +1190,7 @@ __global__ void __launch_bounds__(kNearThreads, 4) near_kernel(DualNodes nodes, 
     __shared__ NearWarp s_warps[kNearWarps];
     const int lane = threadIdx.x & 31;
     NearWarp &w = s_warps[threadIdx.x >> 5];
+    int2 *wstack = pool.walk_stack + ((int64_t) blockIdx.x * kNearWarps + (threadIdx.x >> 5)) * kNearWalkStack;
     const Ctx x{nodes, bodies, G, eps, theta, *num_nodes, n};
     const unsigned long long nunits = min(pool.counters[2], (unsigned long long) pool.unit_cap);
     const unsigned long long nitems = min(pool.counters[0], (unsigned long long) pool.item_cap);
@@ -1146,9 +1226,23 @@ __global__ void __launch_bounds__(kNearThreads, 4) near_kernel(DualNodes nodes, 
         const float4 q = __ldg(bodies + t);
         const float p[3] = {q.x, q.y, q.z};
         const unsigned tmask = L.T >= 32 ? 0xffffffffu : ((1u << L.T) - 1u);
+        // the box of the unit's targets (every lane holds one of them) and their positions
+        float lo[3] = {p[0], p[1], p[2]}, hi[3] = {p[0], p[1], p[2]};
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+                hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+            }
+        }
+        if (lane < L.T) w.tpos[lane] = q;
+        __syncwarp();
         float a[3] = {0.f, 0.f, 0.f};
         int plen = 0;
         int guard = 0;
+        int top = 0;  // activeTree roots of the unit's items, walked together after the close bodies
+        bool overflow = false;
         for (int it = pool.head[leaf]; it >= 0; ++guard) {
             if ((unsigned long long) it >= nitems || guard > (1 << 24)) {
                 if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
@@ -1168,17 +1262,25 @@ __global__ void __launch_bounds__(kNearThreads, 4) near_kernel(DualNodes nodes, 
                     if (L.counted) npp += (unsigned long long) len;
                 }
             } else {
-                for (int r = 0; r < item.w; ++r) {
-                    const int root = words[r];
-                    if (root < 0 || root >= x.nn) {
-                        if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
+                for (int r0 = 0; r0 < item.w; r0 += 32) {
+                    const int r = r0 + lane;
+                    const int root = r < item.w ? words[r] : -1;
+                    const bool ok = r < item.w && root >= 0 && root < x.nn;
+                    if (r < item.w && !ok) atomicOr(err, (uint32_t) kErrTraverseLimit);
+                    const uint32_t b = __ballot_sync(0xffffffffu, ok);
+                    if (top + __popc(b) > kNearWalkStack) {
+                        overflow = true;
                         continue;
                     }
-                    warp_walk<EPS0>(x, w, L, root, tmask, p, a, plen, npp, nnp, err);
+                    if (ok) wstack[top + __popc(b & near_lanemask_lt())] = make_int2(root, (int) tmask);
+                    top += __popc(b);
                 }
             }
             it = item.x;
         }
+        if (overflow && lane == 0) atomicOr(err, (uint32_t) kErrStackOverflow);
+        __syncwarp();
+        if (top > 0) chunk_walk<EPS0>(x, w, L, wstack, top, lo, hi, p, a, plen, npp, nnp, err);
         if (__any_sync(0xffffffffu, plen > 0)) flush_priv(x, w, L, plen, p, a);
         // replicas' partial sums, added in replica order
         w.tile[lane] = make_float4(a[0], a[1], a[2], 0.f);
@@ -1211,6 +1313,12 @@ __global__ void __launch_bounds__(kNearThreads, 4) near_kernel(DualNodes nodes, 
 
 }  // namespace
 
+// Near-field grid: the resident blocks, never more than the walk stacks allocated (one per warp).
+unsigned near_grid(const DualWorkspace &ws) {
+    const int64_t by_stacks = ws.near.walk_warps / kNearWarps;
+    return (unsigned) std::max<int64_t>(1, std::min<int64_t>(ws.near_blocks, by_stacks));
+}
+
 void launch_dual_traverse(const DualNodes &nodes, const int *num_nodes, const float4 *bodies, int64_t n, float G,
                           float eps, float theta, float4 *acc, unsigned long long *counts, DualWorkspace &ws,
                           uint32_t *err, cudaStream_t s, int64_t t_lo, int64_t t_hi) {
@@ -1233,10 +1341,10 @@ void launch_dual_traverse(const DualNodes &nodes, const int *num_nodes, const fl
                                                               (int) ws.arena_words, ws.tasks, ws.near, ws.spill, -1,
                                                               lo, hi, err);
     if (eps == 0.f)
-        near_kernel<true><<<ws.near_blocks, kNearThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta,
+        near_kernel<true><<<near_grid(ws), kNearThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta,
                                                                   acc, counts, ws.near, lo, hi, err);
     else
-        near_kernel<false><<<ws.near_blocks, kNearThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta,
+        near_kernel<false><<<near_grid(ws), kNearThreads, 0, s>>>(nodes, num_nodes, bodies, (int) n, G, eps, theta,
                                                                    acc, counts, ws.near, lo, hi, err);
 }
 
@@ -1256,6 +1364,8 @@ int dual_frontier_blocks(int device) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dual_kernel<true>, kThreads, 0);
     return std::max(1, sms * std::max(per_sm, 1));
 }
+
+int dual_near_warps_per_block() { return kNearWarps; }
 
 int dual_near_blocks(int device) {
     int sms = 0, per_sm = 0;

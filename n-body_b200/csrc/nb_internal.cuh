@@ -216,7 +216,10 @@ struct NearPool {
     int2 *units = nullptr;                // (passive leaf, first target) per 32-target unit
     unsigned long long *counters = nullptr;  // items, words, units, unit cursor
     int64_t head_cap = 0, item_cap = 0, word_cap = 0, unit_cap = 0;
+    int2 *walk_stack = nullptr;           // per warp of the near-field grid: kNearWalkStack (node, mask)
+    int64_t walk_warps = 0;               // warps the walk stacks were sized for
 };
+constexpr int kNearWalkStack = 4608;
 // Tasks handed from the first traversal kernel (above the frontier of passive nodes with at
 // most `frontier` bodies) to the second one, which takes frontier nodes from a work list.
 struct SpillPool {
@@ -245,6 +248,7 @@ int64_t dual_arena_words(int64_t n);
 void dual_near_sizes(int64_t n, int64_t *item_cap, int64_t *word_cap);
 void dual_spill_sizes(int64_t n, int64_t *rec_cap, int64_t *word_cap);
 int dual_near_blocks(int device);
+int dual_near_warps_per_block();
 int dual_frontier_blocks(int device);
 // Accelerations of the targets in [t_lo, t_hi) of the Morton-ordered bodies (all sources act);
 // [0, n) for an unsharded pass.
