@@ -910,14 +910,21 @@ __global__ void load_balanced_break_kernel(DualNodes nodes, const int *__restric
 // between the replicas, whose partial sums are added in replica order at the end of the unit. So
 // short leaves still keep the whole warp busy. Terms are summed without G; G is applied once.
 
-constexpr int kNearThreads = 256;
+constexpr int kNearThreads = 128;  // 4 warps: their slabs and lists fit in 48 KB of static shared memory
 constexpr int kNearWarps = kNearThreads / 32;
-constexpr int kPriv = 16;                      // queued M2P nodes per target
+// A round of the walk adds at most 32 entries to each slab and list, which therefore hold 32.
+constexpr int kM2pFull = 32;  // staged nodes approximated for every target of the unit
+constexpr int kM2pPart = 32;  // staged nodes approximated for some targets (one 32-entry mask block)
+constexpr int kM2pRec = 5;    // float4 per staged node: (com, mass), quadrupole and octupole
 
-constexpr int kNearLeaves = 64;  // opened leaves of a walk waiting for their pair tiles
+constexpr int kNearLeaves = 32;  // opened leaves of a walk waiting for their pair tiles
+
+static_assert(kM2pFull >= 32 && kM2pPart >= 32 && kNearLeaves >= 32, "a round adds up to 32 entries");
 
 struct NearWarp {
-    int priv[kPriv][32];  // [slot][target]
+    float4 m2p_full[kM2pFull * kM2pRec];  // node records approximated for every target
+    float4 m2p_part[kM2pPart * kM2pRec];  // node records approximated for some targets
+    unsigned part_mask[kM2pPart];         // their target masks
     float4 tile[32];      // staged source bodies (16 interleaved pairs), then the replicas' partial sums
     float4 tpos[32];      // the unit's targets (replica-0 lanes)
     int4 leaf[kNearLeaves];  // opened leaves: (first body, end body, target mask, 0)
@@ -935,15 +942,14 @@ struct Lane {
 //   (D3 : Q2)_i = g3 R_i (R.Q2.R) + g2 (2 (Q2 R)_i + R_i tr Q2)
 //   (D4 : Q3)_i = g4 R_i (Q3 : RRR) + 3 g3 ((Q3 : RR)_i + R_i (t.R)) + 3 g2 t_i,  t_i = Q3_ikk,
 // which is the same sum over index tuples, grouped (about 100 flops instead of about 550).
-__device__ __forceinline__ void m2p_nog(const Ctx &x, int k, const float p[3], float a[3]) {
-    const float4 c4 = __ldg(x.nodes.com + k);
+// c4 = (centre of mass, mass), qa..qd = packed quadrupole (6) and octupole (10), as stored.
+__device__ __forceinline__ void m2p_term(float4 c4, float4 qa, float4 qb, float4 qc, float4 qd, float eps,
+                                         const float p[3], float a[3]) {
     const float rx = p[0] - c4.x, ry = p[1] - c4.y, rz = p[2] - c4.z;
     if (rx == 0.f && ry == 0.f && rz == 0.f) return;
-    const float inv = rsqrtf(fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, x.eps))));
+    const float inv = rsqrtf(fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps))));
     const float i2 = inv * inv, i3 = inv * i2, i5 = i3 * i2, i7 = i5 * i2, i9 = i7 * i2;
     const float g2 = 3.0f * i5, g3 = -15.0f * i7, g4 = 105.0f * i9;
-    const float4 *q = x.nodes.q + (int64_t) k * 4;
-    const float4 qa = __ldg(q), qb = __ldg(q + 1), qc = __ldg(q + 2), qd = __ldg(q + 3);
     // quadrupole xx xy xz yy yz zz; octupole xxx xxy xxz xyy xyz xzz yyy yyz yzz zzz
     const float Qxx = qa.x, Qxy = qa.y, Qxz = qa.z, Qyy = qa.w, Qyz = qb.x, Qzz = qb.y;
     const float Oxxx = qb.z, Oxxy = qb.w, Oxxz = qc.x, Oxyy = qc.y, Oxyz = qc.z, Oxzz = qc.w;
@@ -969,6 +975,11 @@ __device__ __forceinline__ void m2p_nog(const Ctx &x, int k, const float p[3], f
     a[0] += fmaf(rx, sr, fmaf(qrx, s2q, -fmaf(ox, s4o, tx * s4t)));
     a[1] += fmaf(ry, sr, fmaf(qry, s2q, -fmaf(oy, s4o, ty * s4t)));
     a[2] += fmaf(rz, sr, fmaf(qrz, s2q, -fmaf(oz, s4o, tz * s4t)));
+}
+
+// The node term from a node record staged in shared memory: (com, mass) then the four moment float4.
+__device__ __forceinline__ void m2p_staged(const float4 *pc, float eps, const float p[3], float a[3]) {
+    m2p_term(pc[0], pc[1], pc[2], pc[3], pc[4], eps, p, a);
 }
 
 // Gravity::particleParticle (Gravity.h:199-209) without G for two sources against one target, in
@@ -1036,15 +1047,66 @@ __device__ __forceinline__ void pair_tile(NearWarp &w, const Lane &L, int m, Src
     a[2] += az.x + az.y;
 }
 
-// The M2P terms queued per target (by its replica 0), split between the target's replicas.
-__device__ void flush_priv(const Ctx &x, NearWarp &w, const Lane &L, int plen, const float p[3], float a[3]) {
-    __syncwarp();  // queue entries written by the targets' first replicas
-    const int len = __shfl_sync(0xffffffffu, plen, L.t);  // the target's queue length
-    const int most = (int) __reduce_max_sync(0xffffffffu, (unsigned) len);
-    for (int i0 = 0; i0 < most; i0 += L.G) {
-        const int i = i0 + L.r;
-        if (L.active && i < len) m2p_nog(x, w.priv[i][L.t], p, a);
+__device__ __forceinline__ void near_cp_async16(void *smem, const void *gmem) {
+    const uint32_t a = (uint32_t) __cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void near_cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Copies node k's record (centre of mass and mass, then the four moment float4) into a slab slot.
+__device__ __forceinline__ void stage_m2p(float4 *dst, const DualNodes &N, int k) {
+    near_cp_async16(dst, N.com + k);
+    const float4 *q = N.q + (int64_t) k * 4;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) near_cp_async16(dst + 1 + i, q + i);
+}
+
+// Transpose of the 32 x 32 bit matrix whose row r is lane r's word: afterwards bit r of lane c's
+// word is bit c of row r.
+__device__ __forceinline__ uint32_t near_transpose32(uint32_t v, int lane) {
+#pragma unroll
+    for (int sh = 16; sh > 0; sh >>= 1) {
+        const uint32_t hi = sh == 16 ? 0xFFFF0000u : sh == 8 ? 0xFF00FF00u : sh == 4 ? 0xF0F0F0F0u
+                          : sh == 2 ? 0xCCCCCCCCu : 0xAAAAAAAAu;
+        const uint32_t y = __shfl_xor_sync(0xffffffffu, v, sh);
+        v = (lane & sh) ? ((v & hi) | ((y & hi) >> sh)) : ((v & ~hi) | ((y & ~hi) << sh));
     }
+    return v;
+}
+
+// M2P of the nodes approximated for every target: each target's replicas split the entries.
+__device__ void flush_m2p_full(const Ctx &x, NearWarp &w, const Lane &L, int &nfull, const float p[3], float a[3],
+                               unsigned long long &nnp) {
+    near_cp_async_wait_all();
+    __syncwarp();
+    if (L.active)
+        for (int j = L.r; j < nfull; j += L.G) m2p_staged(w.m2p_full + j * kM2pRec, x.eps, p, a);
+    if (L.counted) nnp += (unsigned long long) nfull;
+    nfull = 0;
+    __syncwarp();
+}
+
+// M2P of the nodes approximated for some targets: the masks are transposed so that each target
+// holds the set of entries it takes; its replicas split that set.
+__device__ void flush_m2p_part(const Ctx &x, NearWarp &w, const Lane &L, int &npart, const float p[3], float a[3],
+                               unsigned long long &nnp) {
+    const int lane = threadIdx.x & 31;
+    near_cp_async_wait_all();
+    __syncwarp();
+    const uint32_t mine_t = near_transpose32(lane < npart ? w.part_mask[lane] : 0u, lane);  // lane = target
+    uint32_t bits = __shfl_sync(0xffffffffu, mine_t, L.t);
+    if (!L.active) bits = 0u;
+    if (L.counted) nnp += (unsigned long long) __popc(bits);
+    int idx = 0;
+    while (__any_sync(0xffffffffu, bits != 0u)) {
+        if (bits) {
+            const int j = __ffs(bits) - 1;
+            bits &= bits - 1;
+            if (idx % L.G == L.r) m2p_staged(w.m2p_part + j * kM2pRec, x.eps, p, a);
+            ++idx;
+        }
+    }
+    npart = 0;
     __syncwarp();
 }
 
@@ -1095,11 +1157,12 @@ __device__ void flush_leaves(const Ctx &x, NearWarp &w, const Lane &L, int &nlea
 // decisions; a round whose pushes would not fit the stack ends the walk with kErrStackOverflow.
 template<bool EPS0>
 __device__ void chunk_walk(const Ctx &x, NearWarp &w, const Lane &L, int2 *stack, int top, const float lo[3],
-                           const float hi[3], const float p[3], float a[3], int &plen, unsigned long long &npp,
+                           const float hi[3], const float p[3], float a[3], unsigned long long &npp,
                            unsigned long long &nnp, uint32_t *err) {
     const int lane = threadIdx.x & 31;
     const uint32_t lt = near_lanemask_lt();
-    int nleaf = 0;
+    const unsigned tmask = L.T >= 32 ? 0xffffffffu : ((1u << L.T) - 1u);
+    int nleaf = 0, nfull = 0, npart = 0;
     int64_t rounds = 0;
     const int64_t round_limit = 4 * (int64_t) x.nn + 64;
     while (top > 0) {
@@ -1141,25 +1204,27 @@ __device__ void chunk_walk(const Ctx &x, NearWarp &w, const Lane &L, int2 *stack
         const bool leaf_ok = is_leaf && x.range_ok(l0, l1);
         const bool inner_ok = is_inner && x.left_ok(c) && x.right_ok(c, l0);
         if ((is_leaf && !leaf_ok) || (is_inner && !inner_ok)) atomicOr(err, (uint32_t) kErrTraverseLimit);
-        // approximated: queued per target (M2P), in lane order of the round
-        uint32_t pend = __ballot_sync(0xffffffffu, A != 0);
-        while (pend) {
-            const int src = __ffs(pend) - 1;
-            pend &= pend - 1;
-            const int node = __shfl_sync(0xffffffffu, c, src);
-            const unsigned am = __shfl_sync(0xffffffffu, A, src);
-            if (__any_sync(0xffffffffu, plen == kPriv)) {
-                flush_priv(x, w, L, plen, p, a);
-                plen = 0;
+        // approximated: node records staged once per unit (cp.async); every target's, or some
+        // targets' with their mask
+        const bool acc_all = A != 0 && A == tmask, acc_some = A != 0 && A != tmask;
+        uint32_t b = __ballot_sync(0xffffffffu, acc_all);
+        if (b) {
+            if (nfull + __popc(b) > kM2pFull) flush_m2p_full(x, w, L, nfull, p, a, nnp);
+            if (acc_all) stage_m2p(w.m2p_full + (nfull + __popc(b & lt)) * kM2pRec, x.nodes, c);
+            nfull += __popc(b);
+        }
+        b = __ballot_sync(0xffffffffu, acc_some);
+        if (b) {
+            if (npart + __popc(b) > kM2pPart) flush_m2p_part(x, w, L, npart, p, a, nnp);
+            if (acc_some) {
+                const int slot = npart + __popc(b & lt);
+                stage_m2p(w.m2p_part + slot * kM2pRec, x.nodes, c);
+                w.part_mask[slot] = A;
             }
-            if (L.active && L.r == 0 && ((am >> L.t) & 1u)) {
-                w.priv[plen][L.t] = node;
-                ++plen;
-                if (L.counted) ++nnp;
-            }
+            npart += __popc(b);
         }
         // opened leaves: listed, pair tiles when the list could overflow
-        uint32_t b = __ballot_sync(0xffffffffu, leaf_ok);
+        b = __ballot_sync(0xffffffffu, leaf_ok);
         if (nleaf + __popc(b) > kNearLeaves) flush_leaves<EPS0>(x, w, L, nleaf, p, a, npp);
         if (leaf_ok) w.leaf[nleaf + __popc(b & lt)] = make_int4(l0, l1, (int) O, 0);
         nleaf += __popc(b);
@@ -1179,10 +1244,12 @@ __device__ void chunk_walk(const Ctx &x, NearWarp &w, const Lane &L, int2 *stack
         __syncwarp();
     }
     flush_leaves<EPS0>(x, w, L, nleaf, p, a, npp);
+    flush_m2p_full(x, w, L, nfull, p, a, nnp);
+    flush_m2p_part(x, w, L, npart, p, a, nnp);
 }
 
 template<bool EPS0>
-__global__ void __launch_bounds__(kNearThreads, 4) near_kernel(DualNodes nodes, const int *__restrict__ num_nodes,
+__global__ void __launch_bounds__(kNearThreads, 8) near_kernel(DualNodes nodes, const int *__restrict__ num_nodes,
                                                                const float4 *__restrict__ bodies, int n, float G,
                                                                float eps, float theta, float4 *__restrict__ acc,
                                                                unsigned long long *__restrict__ counts, NearPool pool,
@@ -1239,7 +1306,6 @@ __global__ void __launch_bounds__(kNearThreads, 4) near_kernel(DualNodes nodes, 
         if (lane < L.T) w.tpos[lane] = q;
         __syncwarp();
         float a[3] = {0.f, 0.f, 0.f};
-        int plen = 0;
         int guard = 0;
         int top = 0;  // activeTree roots of the unit's items, walked together after the close bodies
         bool overflow = false;
@@ -1280,8 +1346,7 @@ __global__ void __launch_bounds__(kNearThreads, 4) near_kernel(DualNodes nodes, 
         }
         if (overflow && lane == 0) atomicOr(err, (uint32_t) kErrStackOverflow);
         __syncwarp();
-        if (top > 0) chunk_walk<EPS0>(x, w, L, wstack, top, lo, hi, p, a, plen, npp, nnp, err);
-        if (__any_sync(0xffffffffu, plen > 0)) flush_priv(x, w, L, plen, p, a);
+        if (top > 0) chunk_walk<EPS0>(x, w, L, wstack, top, lo, hi, p, a, npp, nnp, err);
         // replicas' partial sums, added in replica order
         w.tile[lane] = make_float4(a[0], a[1], a[2], 0.f);
         __syncwarp();
