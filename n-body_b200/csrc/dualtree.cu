@@ -1011,35 +1011,95 @@ __device__ __forceinline__ void pair2_nog(float2 npx, float2 npy, float2 npz, fl
 // Pairs of the unit's targets with sources src(0..m) for lanes in `mine`. 32 sources at a time are
 // staged in shared memory as 16 interleaved pairs (sources 2j and 2j+1 in one 32-byte record, so
 // that each 16-byte load yields two register pairs); replica r takes pairs r, r + G, ...
+// Pairs of the unit's targets with the c sources staged in the warp's tile, for lanes in `mine`;
+// replica r takes pairs r, r + G, ...
+template<bool EPS0>
+__device__ __forceinline__ void tile_pairs(NearWarp &w, const Lane &L, int c, bool mine, float2 npx, float2 npy,
+                                           float2 npz, float2 eps2, float2 &ax, float2 &ay, float2 &az) {
+    if (!mine) return;
+    const int np = (c + 1) >> 1;
+    const int G = L.G;
+    int k = L.r;
+    for (; k + G < np; k += 2 * G) {
+        const float4 u0 = w.tile[2 * k], v0 = w.tile[2 * k + 1];
+        const float4 u1 = w.tile[2 * (k + G)], v1 = w.tile[2 * (k + G) + 1];
+        pair2_nog<EPS0>(npx, npy, npz, eps2, u0, v0, ax, ay, az);
+        pair2_nog<EPS0>(npx, npy, npz, eps2, u1, v1, ax, ay, az);
+    }
+    if (k < np) pair2_nog<EPS0>(npx, npy, npz, eps2, w.tile[2 * k], w.tile[2 * k + 1], ax, ay, az);
+}
+
+// Stages one source per lane (a zero-mass source at the origin past the end) as 16 interleaved
+// pairs: sources 2j and 2j+1 in one 32-byte record, so that each 16-byte load yields two register
+// pairs.
+__device__ __forceinline__ void stage_tile(NearWarp &w, float4 b) {
+    const int lane = threadIdx.x & 31;
+    float *tf = reinterpret_cast<float *>(w.tile);
+    const int slot = (lane >> 1) * 8 + (lane & 1);
+    tf[slot] = b.x;
+    tf[slot + 2] = b.y;
+    tf[slot + 4] = b.z;
+    tf[slot + 6] = b.w;
+}
+
+// Pairs of the unit's targets with sources src(0..m) for lanes in `mine`, 32 sources per tile.
 template<bool EPS0, typename Src>
 __device__ __forceinline__ void pair_tile(NearWarp &w, const Lane &L, int m, Src src, bool mine, const float p[3],
                                           float eps, float a[3]) {
     const int lane = threadIdx.x & 31;
-    float *tf = reinterpret_cast<float *>(w.tile);
-    const int slot = (lane >> 1) * 8 + (lane & 1);
     const float2 npx = make_float2(-p[0], -p[0]), npy = make_float2(-p[1], -p[1]), npz = make_float2(-p[2], -p[2]);
     const float2 eps2 = make_float2(eps, eps);
     float2 ax = make_float2(0.f, 0.f), ay = ax, az = ax;
     for (int j0 = 0; j0 < m; j0 += 32) {
         const int c = min(32, m - j0);
-        const float4 b = lane < c ? src(j0 + lane) : make_float4(0.f, 0.f, 0.f, 0.f);
-        tf[slot] = b.x;
-        tf[slot + 2] = b.y;
-        tf[slot + 4] = b.z;
-        tf[slot + 6] = b.w;
+        stage_tile(w, lane < c ? src(j0 + lane) : make_float4(0.f, 0.f, 0.f, 0.f));
         __syncwarp();
-        if (mine) {
-            const int np = (c + 1) >> 1;
-            const int G = L.G;
-            int k = L.r;
-            for (; k + G < np; k += 2 * G) {
-                const float4 u0 = w.tile[2 * k], v0 = w.tile[2 * k + 1];
-                const float4 u1 = w.tile[2 * (k + G)], v1 = w.tile[2 * (k + G) + 1];
-                pair2_nog<EPS0>(npx, npy, npz, eps2, u0, v0, ax, ay, az);
-                pair2_nog<EPS0>(npx, npy, npz, eps2, u1, v1, ax, ay, az);
+        tile_pairs<EPS0>(w, L, c, mine, npx, npy, npz, eps2, ax, ay, az);
+        __syncwarp();
+    }
+    a[0] += ax.x + ax.y;
+    a[1] += ay.x + ay.y;
+    a[2] += az.x + az.y;
+}
+
+// Pairs of the unit's targets with the close bodies of one item, given as runs of consecutive
+// bodies ((first body, length) pairs): the runs are packed back to back into 32-source tiles, so a
+// short run does not cost a whole tile. Invalid runs are skipped with kErrTraverseLimit.
+template<bool EPS0>
+__device__ void run_tiles(const Ctx &x, NearWarp &w, const Lane &L, const int *words, int nwords, const float p[3],
+                          float a[3], unsigned long long &npp, uint32_t *err) {
+    const int lane = threadIdx.x & 31;
+    const float2 npx = make_float2(-p[0], -p[0]), npy = make_float2(-p[1], -p[1]), npz = make_float2(-p[2], -p[2]);
+    const float2 eps2 = make_float2(x.eps, x.eps);
+    float2 ax = make_float2(0.f, 0.f), ay = ax, az = ax;
+    int r = 0, first = 0, len = 0, o = 0;  // next word, current run, offset in it
+    for (;;) {
+        int fill = 0;
+        float4 b = make_float4(0.f, 0.f, 0.f, 0.f);
+        while (fill < 32) {
+            if (o == len) {  // the current run is used up: take the next valid one
+                if (r + 1 >= nwords) break;
+                first = words[r];
+                len = words[r + 1];
+                r += 2;
+                o = 0;
+                if (len < 0 || len > x.n || !x.range_ok(first, first + len)) {
+                    if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
+                    len = 0;
+                    continue;
+                }
+                if (L.counted) npp += (unsigned long long) len;
+                continue;
             }
-            if (k < np) pair2_nog<EPS0>(npx, npy, npz, eps2, w.tile[2 * k], w.tile[2 * k + 1], ax, ay, az);
+            const int take = min(len - o, 32 - fill);
+            if (lane >= fill && lane < fill + take) b = __ldg(x.bodies + first + o + (lane - fill));
+            fill += take;
+            o += take;
         }
+        if (fill == 0) break;
+        stage_tile(w, b);
+        __syncwarp();
+        tile_pairs<EPS0>(w, L, fill, L.active, npx, npy, npz, eps2, ax, ay, az);
         __syncwarp();
     }
     a[0] += ax.x + ax.y;
@@ -1317,16 +1377,8 @@ __global__ void __launch_bounds__(kNearThreads, 8) near_kernel(DualNodes nodes, 
             const int4 item = pool.items[it];
             const int *words = pool.words + item.z;
             if (item.y == kItemBodies) {
-                // runs of consecutive close bodies: (first body, length) pairs
-                for (int r = 0; r + 1 < item.w; r += 2) {
-                    const int b0 = words[r], len = words[r + 1];
-                    if (len < 0 || len > x.n || !x.range_ok(b0, b0 + len)) {
-                        if (lane == 0) atomicOr(err, (uint32_t) kErrTraverseLimit);
-                        continue;
-                    }
-                    pair_tile<EPS0>(w, L, len, [&](int j) { return __ldg(bodies + b0 + j); }, L.active, p, eps, a);
-                    if (L.counted) npp += (unsigned long long) len;
-                }
+                // runs of consecutive close bodies: (first body, length) pairs, packed into tiles
+                run_tiles<EPS0>(x, w, L, words, item.w, p, a, npp, err);
             } else {
                 for (int r0 = 0; r0 < item.w; r0 += 32) {
                     const int r = r0 + lane;
