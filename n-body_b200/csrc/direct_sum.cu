@@ -32,7 +32,7 @@ __global__ void __launch_bounds__(kThreads) direct_f32_kernel(const float4 *__re
             const float rx = p.x - b.x, ry = p.y - b.y, rz = p.z - b.z;
             const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps)));
             if (EPS0 && r2 == 0.f) continue;
-            const float inv = rsqrtf(r2);
+            const float inv = rsqrt_hw(r2);
             const float s = b.w * (inv * inv * inv);
             ax = fmaf(-rx, s, ax);
             ay = fmaf(-ry, s, ay);

@@ -158,7 +158,7 @@ __device__ __forceinline__ void load_q(const DualNodes &N, int k, float q2[6], f
 
 // 1 / sqrt(|R|^2 + eps) (the reference's r is sqrt(|R|^2 + eps), Gravity.h:207)
 __device__ __forceinline__ float soft_inv_r(const float R[3], float eps) {
-    return rsqrtf(fmaf(R[0], R[0], fmaf(R[1], R[1], fmaf(R[2], R[2], eps))));
+    return rsqrt_hw(fmaf(R[0], R[0], fmaf(R[1], R[1], fmaf(R[2], R[2], eps))));
 }
 
 // Gravity::nodeNode for MultipoleMassSummary<3> -> MultipoleAccelerationSummary<4> (M2L,
@@ -947,7 +947,7 @@ __device__ __forceinline__ void m2p_term(float4 c4, float4 qa, float4 qb, float4
                                          const float p[3], float a[3]) {
     const float rx = p[0] - c4.x, ry = p[1] - c4.y, rz = p[2] - c4.z;
     if (rx == 0.f && ry == 0.f && rz == 0.f) return;
-    const float inv = rsqrtf(fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps))));
+    const float inv = rsqrt_hw(fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps))));
     const float i2 = inv * inv, i3 = inv * i2, i5 = i3 * i2, i7 = i5 * i2, i9 = i7 * i2;
     const float g2 = 3.0f * i5, g3 = -15.0f * i7, g4 = 105.0f * i9;
     // quadrupole xx xy xz yy yz zz; octupole xxx xxy xxz xyy xyz xzz yyy yyz yzz zzz
@@ -996,8 +996,8 @@ __device__ __forceinline__ void pair2_nog(float2 npx, float2 npy, float2 npz, fl
     const float2 dz = __fadd2_rn(make_float2(v.x, v.y), npz);
     const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
     float2 inv;
-    inv.x = rsqrtf(r2.x);
-    inv.y = rsqrtf(r2.y);
+    inv.x = rsqrt_hw(r2.x);
+    inv.y = rsqrt_hw(r2.y);
     float2 s = __fmul2_rn(make_float2(v.z, v.w), __fmul2_rn(__fmul2_rn(inv, inv), inv));
     if (EPS0) {
         if (r2.x == 0.f) s.x = 0.f;

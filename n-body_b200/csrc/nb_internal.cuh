@@ -18,6 +18,17 @@ __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b)
 __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+// Reciprocal square root of the hardware special-function unit without the denormal-input fixup
+// that rsqrtf carries (a compare and two multiplies per call). At the interaction sites the
+// argument is |R|^2 + epsilon, a normal float for every pair that is evaluated (an exact zero is
+// skipped first), and for a normal argument the result equals rsqrtf's; a denormal argument is
+// flushed to zero (1/sqrt then overflows to infinity either way).
+__device__ __forceinline__ float rsqrt_hw(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // glm::min / glm::max semantics: min(x, y) = (y < x) ? y : x, max(x, y) = (x < y) ? y : x
 __device__ __forceinline__ float gmin(float x, float y) { return (y < x) ? y : x; }
 __device__ __forceinline__ float gmax(float x, float y) { return (x < y) ? y : x; }

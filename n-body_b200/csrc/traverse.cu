@@ -111,7 +111,7 @@ __device__ __forceinline__ void pair_term(float4 p, float4 b, float eps, float &
     const float rx = p.x - b.x, ry = p.y - b.y, rz = p.z - b.z;
     const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps)));
     if (EPS0 && r2 == 0.f) return;  // equal positions contribute nothing (Gravity.h:203)
-    const float inv = rsqrtf(r2);
+    const float inv = rsqrt_hw(r2);
     const float s = b.w * (inv * inv * inv);
     ax = fmaf(-rx, s, ax);
     ay = fmaf(-ry, s, ay);
@@ -124,7 +124,7 @@ __device__ __forceinline__ void quad_term(float4 p, float4 com, float4 q0, float
     const float rx = p.x - com.x, ry = p.y - com.y, rz = p.z - com.z;
     const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps)));
     if (EPS0 && r2 == 0.f) return;
-    const float inv = rsqrtf(r2);
+    const float inv = rsqrt_hw(r2);
     const float inv2 = inv * inv;
     const float inv3 = inv2 * inv;
     const float inv5 = inv3 * inv2;
