@@ -195,7 +195,7 @@ void drop_graph(nb_ctx *ctx) {
 }
 
 void free_dual(nb_ctx *ctx) {
-    dev_free(ctx->tw.sq2); dev_free(ctx->tw.sq3);
+    dev_free(ctx->tw.slot3);
     dev_free(ctx->dnodes.bmin); dev_free(ctx->dnodes.bmax); dev_free(ctx->dnodes.com); dev_free(ctx->dnodes.q);
     dev_free(ctx->dnodes.link); dev_free(ctx->dnodes.thr);
     ctx->dnodes.capacity = 0;
@@ -220,8 +220,7 @@ int ensure_dual(nb_ctx *ctx) {
     free_dual(ctx);
     const int64_t c = ctx->cap;
     const size_t slots = (size_t) (2 * c);
-    NB_TRY(dev_alloc(&ctx->tw.sq2, slots), "alloc octupole summaries");
-    NB_TRY(dev_alloc(&ctx->tw.sq3, slots), "alloc octupole summaries");
+    NB_TRY(dev_alloc(&ctx->tw.slot3, 8 * slots), "alloc octupole summaries");
     NB_TRY(dev_alloc(&ctx->dnodes.bmin, slots), "alloc dual nodes");
     NB_TRY(dev_alloc(&ctx->dnodes.bmax, slots), "alloc dual nodes");
     NB_TRY(dev_alloc(&ctx->dnodes.com, slots), "alloc dual nodes");
@@ -268,10 +267,9 @@ void free_buffers(nb_ctx *ctx) {
     dev_free(ctx->pos); dev_free(ctx->vel); dev_free(ctx->acc); dev_free(ctx->pos2); dev_free(ctx->vel2);
     dev_free(ctx->id); dev_free(ctx->id2); dev_free(ctx->keys); dev_free(ctx->vals);
     dev_free(ctx->sw.keys_alt); dev_free(ctx->sw.vals_alt); dev_free(ctx->sw.lookback);
-    dev_free(ctx->tw.range); dev_free(ctx->tw.left); dev_free(ctx->tw.right); dev_free(ctx->tw.parent);
-    dev_free(ctx->tw.splittable); dev_free(ctx->tw.visit); dev_free(ctx->tw.sbmin); dev_free(ctx->tw.sbmax);
-    dev_free(ctx->tw.scom); dev_free(ctx->tw.sq0); dev_free(ctx->tw.sq1); dev_free(ctx->tw.chain);
-    dev_free(ctx->tw.start); dev_free(ctx->tw.prefix); dev_free(ctx->tw.scan_part);
+    dev_free(ctx->tw.topo); dev_free(ctx->tw.parent); dev_free(ctx->tw.flags); dev_free(ctx->tw.visit);
+    dev_free(ctx->tw.slot); dev_free(ctx->tw.chain);
+    dev_free(ctx->tw.start); dev_free(ctx->tw.pre_base); dev_free(ctx->tw.scan_part);
     dev_free(ctx->tw.leaf_parents); dev_free(ctx->tw.leaf_parents_count);
     dev_free(ctx->nodes.mac); dev_free(ctx->nodes.link); dev_free(ctx->nodes.pay);
     ctx->nodes.capacity = 0;
@@ -296,22 +294,16 @@ int ensure_capacity(nb_ctx *ctx, int64_t n) {
     NB_TRY(dev_alloc(&ctx->sw.vals_alt, c), "alloc sort values");
     NB_TRY(dev_alloc(&ctx->sw.lookback, sort_lookback_words(c)), "alloc sort look-back");
     ctx->sw.capacity = c;
-    NB_TRY(dev_alloc(&ctx->tw.range, c), "alloc tree ranges");
-    NB_TRY(dev_alloc(&ctx->tw.left, c), "alloc tree");
-    NB_TRY(dev_alloc(&ctx->tw.right, c), "alloc tree");
+    NB_TRY(dev_alloc(&ctx->tw.topo, c), "alloc tree");
     NB_TRY(dev_alloc(&ctx->tw.parent, c), "alloc tree");
-    NB_TRY(dev_alloc(&ctx->tw.splittable, c), "alloc tree");
+    NB_TRY(dev_alloc(&ctx->tw.flags, c), "alloc tree");
     NB_TRY(dev_alloc(&ctx->tw.visit, c), "alloc tree");
-    NB_TRY(dev_alloc(&ctx->tw.sbmin, slots), "alloc summaries");
-    NB_TRY(dev_alloc(&ctx->tw.sbmax, slots), "alloc summaries");
-    NB_TRY(dev_alloc(&ctx->tw.scom, slots), "alloc summaries");
-    NB_TRY(dev_alloc(&ctx->tw.sq0, slots), "alloc summaries");
-    NB_TRY(dev_alloc(&ctx->tw.sq1, slots), "alloc summaries");
+    NB_TRY(dev_alloc(&ctx->tw.slot, 4 * slots), "alloc summaries");
     NB_TRY(dev_alloc(&ctx->tw.chain, c), "alloc tree");
     NB_TRY(dev_alloc(&ctx->tw.leaf_parents, c), "alloc tree");
     NB_TRY(dev_alloc(&ctx->tw.leaf_parents_count, 1), "alloc tree");
     NB_TRY(dev_alloc(&ctx->tw.start, c + 1), "alloc tree");
-    NB_TRY(dev_alloc(&ctx->tw.prefix, c + 1), "alloc tree");
+    NB_TRY(dev_alloc(&ctx->tw.pre_base, c + 1), "alloc tree");
     NB_TRY(dev_alloc(&ctx->tw.scan_part, build_scan_tiles(c)), "alloc tree");
     ctx->tw.capacity = c;
     const int64_t node_cap = 2 * c;

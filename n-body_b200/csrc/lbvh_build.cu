@@ -12,24 +12,24 @@
 //   - a final leaf is a non-splittable child of a final internal node (or the root itself).
 //
 // Kernels:
-//   karras_kernel     one thread per Karras internal node: range, split, children, parent,
-//                     splittable flag (reads ~2 log n codes per node, L2-resident)
+//   karras_kernel     one thread per Karras internal node: children, range, parent, the final
+//                     internal / final leaf flags (reads ~2 log n codes per node, L2-resident),
+//                     and the number of final nodes starting at each body position
+//   scan kernels      exclusive prefix over body positions of those counts: the preorder index of
+//                     the final leaf starting at each position
 //   summarize_kernel  one thread per final internal node with leaf children: sequential leaf
 //                     summaries over the leaf's bodies, then an atomic climb in which the second
 //                     child to arrive summarises the parent (CenterOfMassSummary.h:30-55,
 //                     BoundingBoxSummary.h:30-68, MultipoleMassSummary.h:37-97; the leaf moment
 //                     sum follows libstdc++'s 4-way std::transform_reduce). All float operations
 //                     are single IEEE operations in the reference's order, so summaries are
-//                     bit-identical to the CPU restatement.
-//   scan kernels      exclusive prefix over body positions of the number of final nodes whose
-//                     range starts there (counted by karras_kernel)
-//   emit_kernel       the node arrays the traversal reads, each node at its preorder index: MAC data
-//                     (centre and exact MAC threshold), links (right child / leaf body range) and
-//                     payload (centre of mass, mass, quadrupole). The preorder index is closed-form:
-//                     for a node whose range starts at body f, the final nodes before it in preorder
-//                     are those starting before f (the prefix at f) and, among the internal nodes
-//                     starting at f (a chain of left children), the larger ones; a leaf starting at f
-//                     comes after that whole chain.
+//                     bit-identical to the CPU restatement. Every node's record (the arrays the
+//                     traversal reads: MAC data, links, payload) is written by the thread that
+//                     finishes the node, at the node's preorder index. That index is closed-form:
+//                     for a node whose range starts at body f, the final nodes before it in
+//                     preorder are those starting before f and, among the internal nodes starting
+//                     at f (a chain of left children), the larger ones; a leaf starting at f comes
+//                     after that whole chain.
 #include <algorithm>
 #include <cfloat>
 
@@ -63,13 +63,13 @@ __device__ __forceinline__ bool range_splittable(const uint64_t *__restrict__ co
     return (b - a + 1 > leaf) && (codes[a] != codes[b]);
 }
 
+// Karras node flags: bit 0 a final internal node (the reference splits it); bits 1 and 2 its left /
+// right child is a final leaf (set for final internal nodes only).
+constexpr uint8_t kFinal = 1, kLeftLeaf = 2, kRightLeaf = 4;
+
 __global__ void __launch_bounds__(kThreads) karras_kernel(const uint64_t *__restrict__ codes,
                                                           const int *__restrict__ inst_of, int n, int leaf,
-                                                          int2 *__restrict__ range, int *__restrict__ left,
-                                                          int *__restrict__ right, int *__restrict__ parent,
-                                                          uint8_t *__restrict__ splittable, int *__restrict__ start,
-                                                          int *__restrict__ leaf_parents,
-                                                          int *__restrict__ leaf_parents_count) {
+                                                          TreeWorkspace tw) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
     const int dn = prefix_delta(codes, inst_of, n, i, i + 1);
@@ -92,22 +92,23 @@ __global__ void __launch_bounds__(kThreads) karras_kernel(const uint64_t *__rest
     const int first = min(i, j), last = max(i, j);
     const int lc = (first == gamma) ? ~gamma : gamma;
     const int rc = (last == gamma + 1) ? ~(gamma + 1) : gamma + 1;
-    left[i] = lc;
-    right[i] = rc;
-    range[i] = make_int2(first, last);
-    if (lc >= 0) parent[lc] = i;
-    if (rc >= 0) parent[rc] = i;
+    tw.topo[i] = make_int4(lc, rc, first, last);
+    tw.visit[i] = 0;
+    if (lc >= 0) tw.parent[lc] = i;
+    if (rc >= 0) tw.parent[rc] = i;
     const bool split = range_splittable(codes, inst_of, leaf, first, last);
-    splittable[i] = (uint8_t) split;
+    uint8_t f = (uint8_t) split;
     if (split) {
         // a final internal node starts at `first`; a child that is not split is a final leaf
-        atomicAdd(start + first, 2);
+        atomicAdd(tw.start + first, 2);
         const bool lleaf = lc < 0 || !range_splittable(codes, inst_of, leaf, first, gamma);
         const bool rleaf = rc < 0 || !range_splittable(codes, inst_of, leaf, gamma + 1, last);
-        if (lleaf) atomicAdd(start + first, 1);
-        if (rleaf) atomicAdd(start + gamma + 1, 1);
-        if (lleaf || rleaf) leaf_parents[atomicAdd(leaf_parents_count, 1)] = i;
+        if (lleaf) atomicAdd(tw.start + first, 1);
+        if (rleaf) atomicAdd(tw.start + gamma + 1, 1);
+        if (lleaf || rleaf) tw.leaf_parents[atomicAdd(tw.leaf_parents_count, 1)] = i;
+        f |= (uint8_t) ((lleaf ? kLeftLeaf : 0) | (rleaf ? kRightLeaf : 0));
     }
+    tw.flags[i] = f;
 }
 
 // Exclusive prefix over positions 0..n of the number of final nodes starting at each position,
@@ -164,16 +165,19 @@ __global__ void __launch_bounds__(1024) scan_parts_kernel(int *__restrict__ part
     if (threadIdx.x == 0) *total = carry;
 }
 
+// Writes pre_base[f] = (final nodes starting before f) + (final internal nodes starting at f): the
+// preorder index of the final leaf starting at f, one past the smallest internal node starting there.
 __global__ void __launch_bounds__(kThreads) scan_apply_kernel(const int *__restrict__ start, int64_t m,
-                                                              const int *__restrict__ part, int *__restrict__ prefix) {
+                                                              const int *__restrict__ part, int *__restrict__ pre_base) {
     constexpr int kPer = kScanTile / kThreads;  // consecutive positions per thread
     __shared__ int warp_sum[kThreads / 32];
     const int64_t base = (int64_t) blockIdx.x * kScanTile + (int64_t) threadIdx.x * kPer;
-    int v[kPer];
+    int v[kPer], w[kPer];
     int sum = 0;
 #pragma unroll
     for (int k = 0; k < kPer; ++k) {
-        v[k] = base + k < m ? starts_at(start, base + k) : 0;
+        w[k] = base + k < m ? start[base + k] : 0;
+        v[k] = (w[k] >> 1) + (w[k] & 1);
         sum += v[k];
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -189,7 +193,7 @@ __global__ void __launch_bounds__(kThreads) scan_apply_kernel(const int *__restr
     for (int w = 0; w < warp; ++w) run += warp_sum[w];
 #pragma unroll
     for (int k = 0; k < kPer; ++k) {
-        if (base + k < m) prefix[base + k] = run;
+        if (base + k < m) pre_base[base + k] = run + (w[k] >> 1);
         run += v[k];
     }
 }
@@ -198,9 +202,9 @@ __global__ void __launch_bounds__(kThreads) scan_apply_kernel(const int *__restr
 // before f; an internal node follows the larger internal nodes of its chain at f (chain = final
 // internal nodes below it that share f), a leaf follows the whole chain.
 __device__ __forceinline__ int preorder_internal(const TreeWorkspace &tw, int f, int chain) {
-    return tw.prefix[f] + (tw.start[f] >> 1) - 1 - chain;
+    return tw.pre_base[f] - 1 - chain;
 }
-__device__ __forceinline__ int preorder_leaf(const TreeWorkspace &tw, int f) { return tw.prefix[f] + (tw.start[f] >> 1); }
+__device__ __forceinline__ int preorder_leaf(const TreeWorkspace &tw, int f) { return tw.pre_base[f]; }
 
 template<int ORDER>
 struct Summ {
@@ -209,38 +213,51 @@ struct Summ {
     float q3[ORDER >= 3 ? 10 : 1];
 };
 
+// Summary slots, one record per node (Karras internal index, or n - 1 + body index for a leaf):
+// 4 float4 (64 bytes) for orders 1 and 2, 8 float4 (128 bytes) for order 3:
+//   [0] bmin.xyz, bmax.x  [1] bmax.yz, com.xy  [2] com.z, M, Q2[0..1]  [3] Q2[2..5]
+//   [4] Q3[0..3]  [5] Q3[4..7]  [6] Q3[8..9]
+template<int ORDER>
+__device__ __forceinline__ float4 *slot_ptr(const TreeWorkspace &tw, int slot) {
+    return ORDER >= 3 ? tw.slot3 + (int64_t) slot * 8 : tw.slot + (int64_t) slot * 4;
+}
+
 template<int ORDER>
 __device__ __forceinline__ void store_slot(const TreeWorkspace &tw, int slot, const Summ<ORDER> &s) {
-    tw.sbmin[slot] = make_float4(s.bmin[0], s.bmin[1], s.bmin[2], 0.f);
-    tw.sbmax[slot] = make_float4(s.bmax[0], s.bmax[1], s.bmax[2], 0.f);
-    tw.scom[slot] = make_float4(s.com[0], s.com[1], s.com[2], s.M);
+    float4 *d = slot_ptr<ORDER>(tw, slot);
+    d[0] = make_float4(s.bmin[0], s.bmin[1], s.bmin[2], s.bmax[0]);
+    d[1] = make_float4(s.bmax[1], s.bmax[2], s.com[0], s.com[1]);
     if constexpr (ORDER >= 2) {
-        tw.sq0[slot] = make_float4(s.q[0], s.q[1], s.q[2], s.q[3]);
-        tw.sq1[slot] = make_float4(s.q[4], s.q[5], ORDER >= 3 ? s.q3[0] : 0.f, ORDER >= 3 ? s.q3[1] : 0.f);
+        d[2] = make_float4(s.com[2], s.M, s.q[0], s.q[1]);
+        d[3] = make_float4(s.q[2], s.q[3], s.q[4], s.q[5]);
+    } else {
+        d[2] = make_float4(s.com[2], s.M, 0.f, 0.f);
     }
     if constexpr (ORDER >= 3) {
-        tw.sq2[slot] = make_float4(s.q3[2], s.q3[3], s.q3[4], s.q3[5]);
-        tw.sq3[slot] = make_float4(s.q3[6], s.q3[7], s.q3[8], s.q3[9]);
+        d[4] = make_float4(s.q3[0], s.q3[1], s.q3[2], s.q3[3]);
+        d[5] = make_float4(s.q3[4], s.q3[5], s.q3[6], s.q3[7]);
+        d[6] = make_float4(s.q3[8], s.q3[9], 0.f, 0.f);
     }
 }
 
-// Loads bypass L1: the slot may have been written by another block moments ago.
+// Loads bypass L1: the slot was written by another thread, possibly of another block, moments ago.
 template<int ORDER>
 __device__ __forceinline__ Summ<ORDER> load_slot(const TreeWorkspace &tw, int slot) {
     Summ<ORDER> s;
-    float4 a = __ldcg(tw.sbmin + slot), b = __ldcg(tw.sbmax + slot), c = __ldcg(tw.scom + slot);
-    s.bmin[0] = a.x; s.bmin[1] = a.y; s.bmin[2] = a.z;
-    s.bmax[0] = b.x; s.bmax[1] = b.y; s.bmax[2] = b.z;
-    s.com[0] = c.x; s.com[1] = c.y; s.com[2] = c.z; s.M = c.w;
+    const float4 *d = slot_ptr<ORDER>(tw, slot);
+    const float4 a = __ldcg(d), b = __ldcg(d + 1), c = __ldcg(d + 2);
+    s.bmin[0] = a.x; s.bmin[1] = a.y; s.bmin[2] = a.z; s.bmax[0] = a.w;
+    s.bmax[1] = b.x; s.bmax[2] = b.y; s.com[0] = b.z; s.com[1] = b.w;
+    s.com[2] = c.x; s.M = c.y;
     if constexpr (ORDER >= 2) {
-        float4 q0 = __ldcg(tw.sq0 + slot), q1 = __ldcg(tw.sq1 + slot);
-        s.q[0] = q0.x; s.q[1] = q0.y; s.q[2] = q0.z; s.q[3] = q0.w; s.q[4] = q1.x; s.q[5] = q1.y;
-        if constexpr (ORDER >= 3) {
-            float4 q2 = __ldcg(tw.sq2 + slot), q3 = __ldcg(tw.sq3 + slot);
-            s.q3[0] = q1.z; s.q3[1] = q1.w;
-            s.q3[2] = q2.x; s.q3[3] = q2.y; s.q3[4] = q2.z; s.q3[5] = q2.w;
-            s.q3[6] = q3.x; s.q3[7] = q3.y; s.q3[8] = q3.z; s.q3[9] = q3.w;
-        }
+        const float4 e = __ldcg(d + 3);
+        s.q[0] = c.z; s.q[1] = c.w; s.q[2] = e.x; s.q[3] = e.y; s.q[4] = e.z; s.q[5] = e.w;
+    }
+    if constexpr (ORDER >= 3) {
+        const float4 f = __ldcg(d + 4), g = __ldcg(d + 5), h = __ldcg(d + 6);
+        s.q3[0] = f.x; s.q3[1] = f.y; s.q3[2] = f.z; s.q3[3] = f.w;
+        s.q3[4] = g.x; s.q3[5] = g.y; s.q3[6] = g.z; s.q3[7] = g.w;
+        s.q3[8] = h.x; s.q3[9] = h.y;
     }
     return s;
 }
@@ -447,67 +464,6 @@ __device__ Summ<ORDER> internal_summary_f64(const Summ<ORDER> &a, const Summ<ORD
     return s;
 }
 
-__device__ __forceinline__ bool is_final_leaf(const uint8_t *splittable, int c) { return c < 0 || !splittable[c]; }
-__device__ __forceinline__ int slot_of(int c, int n) { return c >= 0 ? c : (n - 1) + ~c; }
-
-// Arrival counter of the bottom-up climb with release-acquire ordering: the caller's summary
-// stores are visible before its arrival, and the second arriver sees the first one's stores.
-__device__ __forceinline__ int arrive_acq_rel(int *p) {
-    int old;
-    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(old) : "l"(p) : "memory");
-    return old;
-}
-
-// Leaf summaries of final internal node i's final-leaf children, then the climb.
-template<int ORDER>
-__device__ void summarize_from(const float4 *__restrict__ bodies, int n, const TreeWorkspace &tw, uint32_t *err, int i) {
-    for (int side = 0; side < 2; ++side) {
-        const int c = side ? tw.right[i] : tw.left[i];
-        if (!is_final_leaf(tw.splittable, c)) continue;
-        int b, e;
-        if (c < 0) { b = e = ~c; } else { int2 r = tw.range[c]; b = r.x; e = r.y; }
-        Summ<ORDER> mine = leaf_summary<ORDER>(bodies, b, e);
-        store_slot<ORDER>(tw, slot_of(c, n), mine);
-        int from = c, p = i, chain_from = -1;  // chain of the node we come from (-1: a leaf)
-        for (int level = 0;; ++level) {
-            if (level >= kMaxTreeDepth || p < 0 || p >= n - 1) {
-                atomicOr(err, (uint32_t) kErrTreeDepth);
-                break;
-            }
-            if (arrive_acq_rel(&tw.visit[p]) == 0) break;  // the sibling's thread finishes p
-            const int lc = tw.left[p], rc = tw.right[p];
-            const bool from_left = (lc == from);
-            const Summ<ORDER> other = load_slot<ORDER>(tw, slot_of(from_left ? rc : lc, n));
-            const int2 rg = tw.range[p];
-            const Summ<ORDER> &l = from_left ? mine : other;
-            const Summ<ORDER> &r = from_left ? other : mine;
-            const Summ<ORDER> up = (tw.fp64_min_bodies > 0 && rg.y - rg.x + 1 >= tw.fp64_min_bodies)
-                                       ? internal_summary_f64<ORDER>(l, r)
-                                       : internal_summary<ORDER>(l, r);
-            store_slot<ORDER>(tw, p, up);
-            // final internal nodes below p that share its first body: its left child's chain
-            const int lchain = !is_final_leaf(tw.splittable, lc) ? (from_left ? chain_from : __ldcg(tw.chain + lc)) : -1;
-            const int ch = lchain + 1;
-            tw.chain[p] = ch;
-            if (p == 0) break;
-            mine = up;
-            chain_from = ch;
-            from = p;
-            p = tw.parent[p];
-        }
-    }
-}
-
-// One thread per final internal node with leaf children (the compact list karras_kernel built), on
-// a grid of a few waves at most.
-template<int ORDER>
-__global__ void __launch_bounds__(kThreads) summarize_kernel(const float4 *__restrict__ bodies, int n, TreeWorkspace tw,
-                                                             uint32_t *err) {
-    const int count = *tw.leaf_parents_count;
-    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x)
-        summarize_from<ORDER>(bodies, n, tw, err, tw.leaf_parents[idx]);
-}
-
 // Smallest float b such that RN(a / b) < t, i.e. d2 >= b <=> the reference's
 // diag^2 / d2 < theta^2 (DiagonalOverCenterDistance.h:18-22). RN(a / b) is monotone in b, so the
 // threshold is exact; NaN means "never approximate" (every comparison with NaN is false).
@@ -565,33 +521,6 @@ __device__ __forceinline__ void register_root(const BatchSegments &seg, int pre,
     if (r.x == first && r.y == last) seg.inst_root[k] = pre;
 }
 
-template<int ORDER>
-__global__ void __launch_bounds__(kThreads) emit_kernel(int n, TreeWorkspace tw, float t, NodeArrays nodes,
-                                                        uint32_t *err, BatchSegments seg) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n - 1 || !tw.splittable[i]) return;
-    const int lc = tw.left[i], rc = tw.right[i];
-    const int2 ri = tw.range[i];
-    const int pre = preorder_internal(tw, ri.x, tw.chain[i]);
-    const int rfirst = rc < 0 ? ~rc : tw.range[rc].x;
-    const bool rleaf = is_final_leaf(tw.splittable, rc);
-    const int right_pre = rleaf ? preorder_leaf(tw, rfirst) : preorder_internal(tw, rfirst, tw.chain[rc]);
-    write_record<ORDER>(nodes, pre, load_slot<ORDER>(tw, i), node_theta2(seg, t, ri.x), right_pre, -1, err);
-    register_root(seg, pre, ri.x, ri.y);
-    if (is_final_leaf(tw.splittable, lc)) {
-        int2 r = lc < 0 ? make_int2(~lc, ~lc) : tw.range[lc];
-        write_record<ORDER>(nodes, pre + 1, load_slot<ORDER>(tw, slot_of(lc, n)), node_theta2(seg, t, r.x), r.x, r.y + 1,
-                            err);
-        register_root(seg, pre + 1, r.x, r.y);
-    }
-    if (rleaf) {
-        int2 r = rc < 0 ? make_int2(~rc, ~rc) : tw.range[rc];
-        write_record<ORDER>(nodes, right_pre, load_slot<ORDER>(tw, slot_of(rc, n)), node_theta2(seg, t, r.x), r.x,
-                            r.y + 1, err);
-        register_root(seg, right_pre, r.x, r.y);
-    }
-}
-
 // Smallest float s >= 0 with RN(sqrt(s)) >= b (sqrt is monotone, so the set is an up-set).
 __device__ float sqrt_threshold(float b) {
     if (isnan(b)) return b;
@@ -637,30 +566,150 @@ __device__ void write_dual_record(const DualNodes &nodes, int pre, const Summ<3>
     nodes.link[pre] = make_int2(link0, link1);
 }
 
-__global__ void __launch_bounds__(kThreads) emit_dual_kernel(int n, TreeWorkspace tw, DualNodes nodes, float theta,
-                                                              uint32_t *err) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n - 1 || !tw.splittable[i]) return;
-    const int lc = tw.left[i], rc = tw.right[i];
-    const int2 ri = tw.range[i];
-    const int pre = preorder_internal(tw, ri.x, tw.chain[i]);
-    const int rfirst = rc < 0 ? ~rc : tw.range[rc].x;
-    const bool rleaf = is_final_leaf(tw.splittable, rc);
-    const int right_pre = rleaf ? preorder_leaf(tw, rfirst) : preorder_internal(tw, rfirst, tw.chain[rc]);
-    write_dual_record(nodes, pre, load_slot<3>(tw, i), ri.x, ri.y, right_pre, -1 - ri.x, theta, err);
-    if (is_final_leaf(tw.splittable, lc)) {
-        int2 r = lc < 0 ? make_int2(~lc, ~lc) : tw.range[lc];
-        write_dual_record(nodes, pre + 1, load_slot<3>(tw, slot_of(lc, n)), r.x, r.y, r.x, r.y + 1, theta, err);
+__device__ __forceinline__ int slot_of(int c, int n) { return c >= 0 ? c : (n - 1) + ~c; }
+
+// Arrival counter of the bottom-up climb with release-acquire ordering: the caller's summary
+// stores are visible before its arrival, and the second arriver sees the first one's stores.
+__device__ __forceinline__ int arrive_acq_rel(int *p) {
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(old) : "l"(p) : "memory");
+    return old;
+}
+
+// Node record writers of the two node formats, called by the thread that finishes a node.
+template<int ORDER>
+struct BhRecords {
+    NodeArrays nodes;
+    float t;  // RN(theta * theta)
+    BatchSegments seg;
+    __device__ void leaf(int pre, const Summ<ORDER> &s, int first, int last, uint32_t *err) const {
+        write_record<ORDER>(nodes, pre, s, node_theta2(seg, t, first), first, last + 1, err);
+        register_root(seg, pre, first, last);
     }
-    if (rleaf) {
-        int2 r = rc < 0 ? make_int2(~rc, ~rc) : tw.range[rc];
-        write_dual_record(nodes, right_pre, load_slot<3>(tw, slot_of(rc, n)), r.x, r.y, r.x, r.y + 1, theta, err);
+    __device__ void internal(int pre, const Summ<ORDER> &s, int first, int last, int right_pre, uint32_t *err) const {
+        write_record<ORDER>(nodes, pre, s, node_theta2(seg, t, first), right_pre, -1, err);
+        register_root(seg, pre, first, last);
     }
+};
+
+struct DualRecords {
+    DualNodes nodes;
+    float theta;
+    __device__ void leaf(int pre, const Summ<3> &s, int first, int last, uint32_t *err) const {
+        write_dual_record(nodes, pre, s, first, last, first, last + 1, theta, err);
+    }
+    __device__ void internal(int pre, const Summ<3> &s, int first, int last, int right_pre, uint32_t *err) const {
+        write_dual_record(nodes, pre, s, first, last, right_pre, -1 - first, theta, err);
+    }
+};
+
+// Summary of a final internal node covering bodies [first, last] from its children's.
+template<int ORDER>
+__device__ __forceinline__ Summ<ORDER> combine(const TreeWorkspace &tw, const Summ<ORDER> &l, const Summ<ORDER> &r,
+                                               int first, int last) {
+    return (tw.fp64_min_bodies > 0 && last - first + 1 >= tw.fp64_min_bodies) ? internal_summary_f64<ORDER>(l, r)
+                                                                              : internal_summary<ORDER>(l, r);
+}
+
+// Final internal node i's final-leaf children: leaf summaries and records, then the climb. A node
+// whose children are both final leaves is finished at once, without an arrival. The topology of
+// the next node up is loaded while the current level computes, so a level waits for its arrival
+// and the sibling's summary only.
+template<int ORDER, class Records>
+__device__ void summarize_from(const float4 *__restrict__ bodies, int n, const TreeWorkspace &tw, uint32_t *err,
+                               const Records &rec, int i) {
+    int4 tp = tw.topo[i];  // (left child, right child, first body, last body) of the node p below
+    uint8_t fl = tw.flags[i];
+    int par = tw.parent[i];  // not written for the root, and read only below a non-root node
+    const int gamma = tp.x >= 0 ? tp.x : ~tp.x;  // the left child's last body
+    Summ<ORDER> mine;
+    int from, p, chain_from;  // the finished child and its chain (-1: a leaf), the node above it
+    if ((fl & kLeftLeaf) && (fl & kRightLeaf)) {
+        const Summ<ORDER> l = leaf_summary<ORDER>(bodies, tp.z, gamma);
+        const Summ<ORDER> r = leaf_summary<ORDER>(bodies, gamma + 1, tp.w);
+        rec.leaf(preorder_leaf(tw, tp.z), l, tp.z, gamma, err);
+        const int right_pre = preorder_leaf(tw, gamma + 1);
+        rec.leaf(right_pre, r, gamma + 1, tp.w, err);
+        mine = combine<ORDER>(tw, l, r, tp.z, tp.w);
+        store_slot<ORDER>(tw, i, mine);
+        tw.chain[i] = 0;
+        rec.internal(preorder_internal(tw, tp.z, 0), mine, tp.z, tp.w, right_pre, err);
+        if (i == 0) return;
+        from = i;
+        chain_from = 0;
+        p = par;
+        if (p < 0 || p >= n - 1) {
+            atomicOr(err, (uint32_t) kErrTreeDepth);
+            return;
+        }
+        tp = tw.topo[p];
+        fl = tw.flags[p];
+        par = tw.parent[p];
+    } else {
+        const bool left = (fl & kLeftLeaf) != 0;  // exactly one child is a final leaf
+        const int b = left ? tp.z : gamma + 1, e = left ? gamma : tp.w;
+        mine = leaf_summary<ORDER>(bodies, b, e);
+        from = left ? tp.x : tp.y;
+        store_slot<ORDER>(tw, slot_of(from, n), mine);
+        rec.leaf(preorder_leaf(tw, b), mine, b, e, err);
+        chain_from = -1;
+        p = i;
+    }
+    for (int level = 0;; ++level) {
+        if (level >= kMaxTreeDepth || p < 0 || p >= n - 1) {
+            atomicOr(err, (uint32_t) kErrTreeDepth);
+            return;
+        }
+        if (arrive_acq_rel(&tw.visit[p]) == 0) return;  // the sibling's thread finishes p
+        const int lc = tp.x, rc = tp.y;
+        const bool from_left = (lc == from);
+        const bool lfin = (fl & kLeftLeaf) != 0, rfin = (fl & kRightLeaf) != 0;
+        const int sib = from_left ? rc : lc;
+        const Summ<ORDER> other = load_slot<ORDER>(tw, slot_of(sib, n));
+        const int sib_chain = (from_left ? rfin : lfin) ? -1 : __ldcg(tw.chain + sib);
+        int4 ntp = make_int4(0, 0, 0, 0);
+        uint8_t nfl = 0;
+        int npar = -1;
+        if (p != 0 && par >= 0 && par < n - 1) {
+            ntp = tw.topo[par];
+            nfl = tw.flags[par];
+            npar = tw.parent[par];
+        }
+        const Summ<ORDER> up = from_left ? combine<ORDER>(tw, mine, other, tp.z, tp.w)
+                                         : combine<ORDER>(tw, other, mine, tp.z, tp.w);
+        store_slot<ORDER>(tw, p, up);
+        // final internal nodes below p that share its first body: its left child's chain
+        const int lchain = lfin ? -1 : (from_left ? chain_from : sib_chain);
+        const int rchain = rfin ? -1 : (from_left ? sib_chain : chain_from);
+        const int ch = lchain + 1;
+        tw.chain[p] = ch;
+        const int rfirst = (lc >= 0 ? lc : ~lc) + 1;
+        const int right_pre = rfin ? preorder_leaf(tw, rfirst) : preorder_internal(tw, rfirst, rchain);
+        rec.internal(preorder_internal(tw, tp.z, ch), up, tp.z, tp.w, right_pre, err);
+        if (p == 0) return;
+        mine = up;
+        chain_from = ch;
+        from = p;
+        p = par;
+        tp = ntp;
+        fl = nfl;
+        par = npar;
+    }
+}
+
+// One thread per final internal node with leaf children (the compact list karras_kernel built), on
+// a grid of a few waves at most.
+template<int ORDER, class Records>
+__global__ void __launch_bounds__(kThreads) summarize_kernel(const float4 *__restrict__ bodies, int n, TreeWorkspace tw,
+                                                             uint32_t *err, Records rec) {
+    const int count = *tw.leaf_parents_count;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x)
+        summarize_from<ORDER, Records>(bodies, n, tw, err, rec, tw.leaf_parents[idx]);
 }
 
 __global__ void root_leaf_dual_kernel(const float4 *__restrict__ bodies, int n, TreeWorkspace tw, DualNodes nodes,
                                       float theta, uint32_t *err) {
-    if (n > 1 && tw.splittable[0]) return;
+    if (n > 1 && (tw.flags[0] & kFinal)) return;
     write_dual_record(nodes, 0, leaf_summary<3>(bodies, 0, n - 1), 0, n - 1, 0, n, theta, err);
     *tw.num_nodes = 1;
 }
@@ -670,7 +719,7 @@ __global__ void root_leaf_dual_kernel(const float4 *__restrict__ bodies, int n, 
 template<int ORDER>
 __global__ void root_leaf_kernel(const float4 *__restrict__ bodies, int n, TreeWorkspace tw, float t,
                                  NodeArrays nodes, uint32_t *err, BatchSegments seg) {
-    if (n > 1 && tw.splittable[0]) return;
+    if (n > 1 && (tw.flags[0] & kFinal)) return;
     write_record<ORDER>(nodes, 0, leaf_summary<ORDER>(bodies, 0, n - 1), node_theta2(seg, t, 0), 0, n, err);
     register_root(seg, 0, 0, n - 1);
     *tw.num_nodes = 1;
@@ -685,7 +734,7 @@ int summarize_blocks(int n) {
 }
 
 // Karras topology, the final nodes per start position and their exclusive prefix (which also
-// gives the node count); clears the climb's arrival counters.
+// gives the node count); the topology kernel also clears the climb's arrival counters.
 void launch_topology(const uint64_t *sorted_codes, const int *inst_of, int n, int leaf, TreeWorkspace &tw,
                      cudaStream_t s) {
     const int internal = n - 1;
@@ -693,13 +742,11 @@ void launch_topology(const uint64_t *sorted_codes, const int *inst_of, int n, in
     const int64_t m = (int64_t) n + 1;
     const int tiles = (int) build_scan_tiles(n);
     cudaMemsetAsync(tw.start, 0, (size_t) m * sizeof(int), s);
-    cudaMemsetAsync(tw.visit, 0, (size_t) internal * sizeof(int), s);
     cudaMemsetAsync(tw.leaf_parents_count, 0, sizeof(int), s);
-    karras_kernel<<<blocks, kThreads, 0, s>>>(sorted_codes, inst_of, n, leaf, tw.range, tw.left, tw.right, tw.parent,
-                                              tw.splittable, tw.start, tw.leaf_parents, tw.leaf_parents_count);
+    karras_kernel<<<blocks, kThreads, 0, s>>>(sorted_codes, inst_of, n, leaf, tw);
     scan_tiles_kernel<<<tiles, kThreads, 0, s>>>(tw.start, m, tw.scan_part);
     scan_parts_kernel<<<1, 1024, 0, s>>>(tw.scan_part, tiles, tw.num_nodes);
-    scan_apply_kernel<<<tiles, kThreads, 0, s>>>(tw.start, m, tw.scan_part, tw.prefix);
+    scan_apply_kernel<<<tiles, kThreads, 0, s>>>(tw.start, m, tw.scan_part, tw.pre_base);
 }
 
 }  // namespace
@@ -713,12 +760,10 @@ void launch_build_dual_tree(const uint64_t *sorted_codes, const float4 *bodies, 
         cudaMemsetAsync(tw.num_nodes, 0, sizeof(int), s);
         return;
     }
-    const int internal = n - 1;
-    const int blocks = internal > 0 ? (internal + kThreads - 1) / kThreads : 1;
-    if (internal > 0) {
+    if (n > 1) {
         launch_topology(sorted_codes, nullptr, n, leaf, tw, s);
-        summarize_kernel<3><<<summarize_blocks(n), kThreads, 0, s>>>(bodies, n, tw, err);
-        emit_dual_kernel<<<blocks, kThreads, 0, s>>>(n, tw, nodes, theta, err);
+        summarize_kernel<3, DualRecords>
+            <<<summarize_blocks(n), kThreads, 0, s>>>(bodies, n, tw, err, DualRecords{nodes, theta});
     }
     root_leaf_dual_kernel<<<1, 1, 0, s>>>(bodies, n, tw, nodes, theta, err);
 }
@@ -732,20 +777,16 @@ void launch_build_tree(const uint64_t *sorted_codes, const float4 *bodies, int64
         return;
     }
     const float t = theta * theta;  // the reference compares against theta * theta in float
-    const int internal = n - 1;
-    const int blocks = internal > 0 ? (internal + kThreads - 1) / kThreads : 1;
-    if (internal > 0) launch_topology(sorted_codes, seg.inst_of, n, leaf, tw, s);
+    if (n > 1) launch_topology(sorted_codes, seg.inst_of, n, leaf, tw, s);
     if (order == 1) {
-        if (internal > 0) {
-            summarize_kernel<1><<<summarize_blocks(n), kThreads, 0, s>>>(bodies, n, tw, err);
-            emit_kernel<1><<<blocks, kThreads, 0, s>>>(n, tw, t, nodes, err, seg);
-        }
+        if (n > 1)
+            summarize_kernel<1, BhRecords<1>>
+                <<<summarize_blocks(n), kThreads, 0, s>>>(bodies, n, tw, err, BhRecords<1>{nodes, t, seg});
         root_leaf_kernel<1><<<1, 1, 0, s>>>(bodies, n, tw, t, nodes, err, seg);
     } else {
-        if (internal > 0) {
-            summarize_kernel<2><<<summarize_blocks(n), kThreads, 0, s>>>(bodies, n, tw, err);
-            emit_kernel<2><<<blocks, kThreads, 0, s>>>(n, tw, t, nodes, err, seg);
-        }
+        if (n > 1)
+            summarize_kernel<2, BhRecords<2>>
+                <<<summarize_blocks(n), kThreads, 0, s>>>(bodies, n, tw, err, BhRecords<2>{nodes, t, seg});
         root_leaf_kernel<2><<<1, 1, 0, s>>>(bodies, n, tw, t, nodes, err, seg);
     }
 }

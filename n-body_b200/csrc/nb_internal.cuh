@@ -172,18 +172,18 @@ struct BatchSegments {
 
 // lbvh_build.cu
 struct TreeWorkspace {
-    int2 *range = nullptr;          // n-1 internal Karras nodes: first, last
-    int *left = nullptr, *right = nullptr;  // child encoding: internal i >= 0, Karras leaf j as ~j
+    int4 *topo = nullptr;           // n-1 Karras internal nodes: (left child, right child, first body, last body);
+                                    // child encoding: internal i >= 0, Karras leaf j as ~j
     int *parent = nullptr;          // parent of internal node
-    uint8_t *splittable = nullptr;  // n-1
-    int *visit = nullptr;           // n-1 arrival counters
-    float4 *sbmin = nullptr, *sbmax = nullptr, *scom = nullptr;  // 2n-1 summary slots
-    float4 *sq0 = nullptr, *sq1 = nullptr;                        // quadrupole slots (order >= 2)
-    float4 *sq2 = nullptr, *sq3 = nullptr;                        // octupole slots (order 3)
+    uint8_t *flags = nullptr;       // n-1: final internal node, left / right child a final leaf (lbvh_build.cu)
+    int *visit = nullptr;           // n-1 arrival counters of the summary climb
+    float4 *slot = nullptr;         // 2n summary slots of 4 float4 (orders 1 and 2)
+    float4 *slot3 = nullptr;        // 2n summary slots of 8 float4 (order 3, dual tree)
     int *chain = nullptr;           // per final internal node: final internal nodes below it that share its first body
     int *start = nullptr;           // per body position (n + 1): 2 x (final internal nodes whose range starts
                                     // there) + 1 if a final leaf starts there
-    int *prefix = nullptr;          // per body position (n + 1): final nodes starting before it (exclusive scan)
+    int *pre_base = nullptr;        // per body position (n + 1): preorder index of the final leaf starting there
+                                    // (final nodes starting before it plus final internal nodes starting at it)
     int *scan_part = nullptr;       // per scan tile: its total, then its exclusive prefix
     int *leaf_parents = nullptr;    // final internal nodes with at least one final-leaf child (n - 1),
                                     // in no particular order; the count is leaf_parents_count[0]
