@@ -104,9 +104,21 @@ __device__ __forceinline__ float sep_box(const DNode &a, const DNode &b) {
 // sep(node, p) >= B, exactly, with the node's thresholds (B, S): when one of the two separation
 // vectors is zero, sep is RN(sqrt(|v|^2)) and the test is |v|^2 >= S; otherwise the double path.
 // sep >= B from the squared lengths su, sv of the two separation vectors (non-decreasing in both).
+//
+// With both vectors nonzero, the exact sum lu^2 + lv^2 of the rounded lengths lies within a
+// relative 1.5 * 2^-23 of q = RN(su + sv), and sep (its double root rounded to float) is >= B
+// whenever that sum is >= B^2 (1 + 2^-21) and < B^2 whenever it is <= B^2 (1 - 2^-21). So
+// q >= RN(B^2) (1 + 2^-18) decides "yes" and q < RN(B^2) (1 - 2^-18) decides "no" exactly (for
+// RN(B^2) in [1e-30, 1e30], where no term is denormal or overflows); only the cases in between
+// take the double path.
 __device__ __forceinline__ bool sep_test(float su, float sv, float B, float S) {
     if (sv == 0.f) return su >= S;
     if (su == 0.f) return sv >= S;
+    const float b2 = B * B, q = su + sv;
+    if (b2 >= 1e-30f && b2 <= 1e30f) {
+        if (q >= b2 * (1.0f + 0x1p-18f)) return true;
+        if (q < b2 * (1.0f - 0x1p-18f)) return false;
+    }
     return sep_from(__fsqrt_rn(su), __fsqrt_rn(sv)) >= B;
 }
 // Squared length of the per-axis gaps (max0(a - b))_k, in the reference's operation order.
@@ -189,26 +201,36 @@ __device__ void m2l(const Ctx &x, int k, const DNode &n, const float pc[3], floa
     for (int a = 0; a < 15; ++a) f[19 + a] += d4[a] * mg * (1.0f / 6.0f);
 }
 
-// Gravity::particleNode into MultipoleAccelerationSummary<4> (P2L, Gravity.h:282-306)
+// Gravity::particleNode into MultipoleAccelerationSummary<4> (P2L, Gravity.h:282-306). The
+// expansion factors (m G for D2, m G / 2 for D3, m G / 6 for D4) are folded into the derivative
+// coefficients, so each field component takes one product sum.
+__device__ __forceinline__ st::Coef scaled(const st::Coef &c, float s) {
+    st::Coef o;
+    o.g1 = c.g1 * s;
+    o.g2 = c.g2 * s;
+    o.g3 = c.g3 * s;
+    o.g4 = c.g4 * s;
+    return o;
+}
 __device__ void p2l(const Ctx &x, float4 b, const float pc[3], float *f) {
     const float R[3] = {pc[0] - b.x, pc[1] - b.y, pc[2] - b.z};
     if (R[0] == 0.f && R[1] == 0.f && R[2] == 0.f) return;
     const float inv = soft_inv_r(R, x.eps);
     const st::Coef c = st::Coef::from_inverse(inv);
-    float d2[6], d3[10], d4[15];
-    st::D2(R, c, d2);
-    st::D3(R, c, d3);
-    st::D4(R, c, d4);
     const float mg = b.w * x.G;
-    const float inv3 = inv * inv * inv;
+    float d[15];
+    const float m1 = c.g1 * mg;  // -m G / r^3
 #pragma unroll
-    for (int i = 0; i < 3; ++i) f[i] -= R[i] * inv3 * mg;
+    for (int i = 0; i < 3; ++i) f[i] = fmaf(R[i], m1, f[i]);
+    st::D2(R, scaled(c, mg), d);
 #pragma unroll
-    for (int a = 0; a < 6; ++a) f[3 + a] += d2[a] * mg;
+    for (int a = 0; a < 6; ++a) f[3 + a] += d[a];
+    st::D3(R, scaled(c, mg * 0.5f), d);
 #pragma unroll
-    for (int a = 0; a < 10; ++a) f[9 + a] += d3[a] * mg * 0.5f;
+    for (int a = 0; a < 10; ++a) f[9 + a] += d[a];
+    st::D4(R, scaled(c, mg * (1.0f / 6.0f)), d);
 #pragma unroll
-    for (int a = 0; a < 15; ++a) f[19 + a] += d4[a] * mg * (1.0f / 6.0f);
+    for (int a = 0; a < 15; ++a) f[19 + a] += d[a];
 }
 
 struct Scan3 {
@@ -248,61 +270,65 @@ __device__ int stable_rank(int cls, Scan3 &s) {
 }
 
 // Stable block-wide partition of list[0..len) into classes 0, 1, 2 (c0, c1, c2; -1 drops the
-// entry), appending after the counts already in s.base. Each thread takes 4 consecutive entries
-// per round, so their loads overlap and one prefix sum serves 4 * kThreads entries. Every thread
+// entry), appending after the counts already in s.base. A round covers kPartK x kThreads entries:
+// warp w takes the w-th run of 32 kPartK consecutive entries, lane l its entries l, l + 32, ...
+// (coalesced loads, kPartK classifications in flight per thread). Ranks come from ballots within
+// the warp and one prefix over the warps' class totals: two block barriers per round. Every thread
 // of the block must call it.
+constexpr int kPartK = 4;
 template<typename Classify>
-__device__ void stable_partition4(const int *list, int len, int *c0, int *c1, int *c2, Scan3 &s, Classify classify) {
+__device__ void stable_partition(const int *list, int len, int *c0, int *c1, int *c2, Scan3 &s, Classify classify) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int i0 = 0; i0 < len; i0 += 4 * kThreads) {
-        const int b = i0 + 4 * (int) threadIdx.x;
-        int e[4], cls[4];
+    const unsigned lt = (1u << lane) - 1u;
+    for (int i0 = 0; i0 < len; i0 += kPartK * kThreads) {
+        const int wb = i0 + warp * (32 * kPartK) + lane;
+        int e[kPartK], cls[kPartK];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) e[j] = b + j < len ? list[b + j] : -1;
+        for (int j = 0; j < kPartK; ++j) e[j] = wb + 32 * j < len ? list[wb + 32 * j] : -1;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) cls[j] = b + j < len ? classify(e[j]) : -1;
-        int v[3] = {0, 0, 0};
+        for (int j = 0; j < kPartK; ++j) cls[j] = wb + 32 * j < len ? classify(e[j]) : -1;
+        int tot[3] = {0, 0, 0};
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            v[0] += cls[j] == 0;
-            v[1] += cls[j] == 1;
-            v[2] += cls[j] == 2;
+        for (int j = 0; j < kPartK; ++j) {
+            tot[0] += __popc(__ballot_sync(0xffffffffu, cls[j] == 0));
+            tot[1] += __popc(__ballot_sync(0xffffffffu, cls[j] == 1));
+            tot[2] += __popc(__ballot_sync(0xffffffffu, cls[j] == 2));
         }
-        int x[3] = {v[0], v[1], v[2]};
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const int y = __shfl_up_sync(0xffffffffu, x[k], o);
-                if (lane >= o) x[k] += y;
-            }
-        }
-        if (lane == 31) {
-            s.wcnt[0][warp] = x[0];
-            s.wcnt[1][warp] = x[1];
-            s.wcnt[2][warp] = x[2];
+        if (lane == 0) {
+            s.wcnt[0][warp] = tot[0];
+            s.wcnt[1][warp] = tot[1];
+            s.wcnt[2][warp] = tot[2];
         }
         __syncthreads();
-        int off[3];
+        int off[3], next[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            int pre = s.base[k];
-            for (int w = 0; w < warp; ++w) pre += s.wcnt[k][w];
-            off[k] = pre + x[k] - v[k];
+            int pre = s.base[k], all = s.base[k];
+            for (int w = 0; w < kWarps; ++w) {
+                const int c = s.wcnt[k][w];
+                if (w < warp) pre += c;
+                all += c;
+            }
+            off[k] = pre;
+            next[k] = all;
         }
+        // every thread has read the bases and the counts before the bases change and before the
+        // next round's counts overwrite them; the next round reads the new bases after its first
+        // barrier
         __syncthreads();
-        if (threadIdx.x < 3) {
-            int t = 0;
-            for (int w = 0; w < kWarps; ++w) t += s.wcnt[threadIdx.x][w];
-            s.base[threadIdx.x] += t;
-        }
+        if (threadIdx.x < 3) s.base[threadIdx.x] = threadIdx.x == 0 ? next[0] : (threadIdx.x == 1 ? next[1] : next[2]);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            if (cls[j] == 0) c0[off[0]++] = e[j];
-            else if (cls[j] == 1) c1[off[1]++] = e[j];
-            else if (cls[j] == 2) c2[off[2]++] = e[j];
+        for (int j = 0; j < kPartK; ++j) {
+            const unsigned b0 = __ballot_sync(0xffffffffu, cls[j] == 0);
+            const unsigned b1 = __ballot_sync(0xffffffffu, cls[j] == 1);
+            const unsigned b2 = __ballot_sync(0xffffffffu, cls[j] == 2);
+            if (cls[j] == 0) c0[off[0] + __popc(b0 & lt)] = e[j];
+            else if (cls[j] == 1) c1[off[1] + __popc(b1 & lt)] = e[j];
+            else if (cls[j] == 2) c2[off[2] + __popc(b2 & lt)] = e[j];
+            off[0] += __popc(b0);
+            off[1] += __popc(b1);
+            off[2] += __popc(b2);
         }
-        __syncthreads();
     }
 }
 
@@ -540,7 +566,7 @@ __global__ void __launch_bounds__(kThreads, 4) dual_kernel(DualNodes nodes, cons
 
         // ---- classify the list (stable compaction): far c0, leaf / close c1, non-leaf c2 ----
         if (type == kLockstep) {
-            stable_partition4(list, len, c0, c1, c2, s_scan, [&](int e) {
+            stable_partition(list, len, c0, c1, c2, s_scan, [&](int e) {
                 const DNode A = load_node(nodes, e);
                 int cls;
                 if (node_node(A, P, theta) == 0) cls = 0;
@@ -550,7 +576,7 @@ __global__ void __launch_bounds__(kThreads, 4) dual_kernel(DualNodes nodes, cons
                 return cls;
             });
         } else {
-            stable_partition4(list, len, c0, c1, c2, s_scan, [&](int e) {
+            stable_partition(list, len, c0, c1, c2, s_scan, [&](int e) {
                 const float4 q = __ldg(bodies + e);
                 const float pe[3] = {q.x, q.y, q.z};
                 return point_is_far(pe, P, pthr) ? 0 : 1;
@@ -1020,13 +1046,17 @@ __device__ __forceinline__ void tile_pairs(NearWarp &w, const Lane &L, int c, bo
     const int np = (c + 1) >> 1;
     const int G = L.G;
     int k = L.r;
-    for (; k + G < np; k += 2 * G) {
+    for (; k + 3 * G < np; k += 4 * G) {
         const float4 u0 = w.tile[2 * k], v0 = w.tile[2 * k + 1];
         const float4 u1 = w.tile[2 * (k + G)], v1 = w.tile[2 * (k + G) + 1];
+        const float4 u2 = w.tile[2 * (k + 2 * G)], v2 = w.tile[2 * (k + 2 * G) + 1];
+        const float4 u3 = w.tile[2 * (k + 3 * G)], v3 = w.tile[2 * (k + 3 * G) + 1];
         pair2_nog<EPS0>(npx, npy, npz, eps2, u0, v0, ax, ay, az);
         pair2_nog<EPS0>(npx, npy, npz, eps2, u1, v1, ax, ay, az);
+        pair2_nog<EPS0>(npx, npy, npz, eps2, u2, v2, ax, ay, az);
+        pair2_nog<EPS0>(npx, npy, npz, eps2, u3, v3, ax, ay, az);
     }
-    if (k < np) pair2_nog<EPS0>(npx, npy, npz, eps2, w.tile[2 * k], w.tile[2 * k + 1], ax, ay, az);
+    for (; k < np; k += G) pair2_nog<EPS0>(npx, npy, npz, eps2, w.tile[2 * k], w.tile[2 * k + 1], ax, ay, az);
 }
 
 // Stages one source per lane (a zero-mass source at the origin past the end) as 16 interleaved
@@ -1234,27 +1264,38 @@ __device__ void chunk_walk(const Ctx &x, NearWarp &w, const Lane &L, int2 *stack
         const int base = top - k;
         top = base;
         int c = 0, l0 = 0, l1 = -1;
-        unsigned A = 0, O = 0;
+        unsigned A = 0, O = 0, m = 0;
+        bool mixed = false;
+        DNode nd;
+        float4 thr = make_float4(0.f, 0.f, 0.f, 0.f);
         if (lane < k) {
             const int2 e = stack[base + lane];
             c = e.x;
-            const unsigned m = (unsigned) e.y;
-            const DNode nd = load_node(x.nodes, c);
-            const float4 thr = __ldg(x.nodes.thr + c);
+            m = (unsigned) e.y;
+            nd = load_node(x.nodes, c);
+            thr = __ldg(x.nodes.thr + c);
             l0 = nd.link0;
             l1 = nd.link1;
             const int cls = classify_group(nd, thr, lo, hi);
-            if (cls == kGroupAccept) {
-                A = m;
-            } else if (cls == kGroupOpen) {
-                O = m;
-            } else {
-                unsigned bits = 0;
-                for (int t = 0; t < L.T; ++t) {
-                    const float4 tp = w.tpos[t];
-                    const float pt[3] = {tp.x, tp.y, tp.z};
-                    if (sep_at_least(nd, pt, thr.x, thr.y)) bits |= 1u << t;
-                }
+            if (cls == kGroupAccept) A = m;
+            else if (cls == kGroupOpen) O = m;
+            else mixed = true;
+        }
+        // nodes left mixed: decided per target, one node at a time, every lane testing its own
+        // target (lane t < T holds target t)
+        for (unsigned mb = __ballot_sync(0xffffffffu, mixed); mb; mb &= mb - 1) {
+            const int src = __ffs(mb) - 1;
+            DNode q;
+            q.mn[0] = __shfl_sync(0xffffffffu, nd.mn[0], src);
+            q.mn[1] = __shfl_sync(0xffffffffu, nd.mn[1], src);
+            q.mn[2] = __shfl_sync(0xffffffffu, nd.mn[2], src);
+            q.mx[0] = __shfl_sync(0xffffffffu, nd.mx[0], src);
+            q.mx[1] = __shfl_sync(0xffffffffu, nd.mx[1], src);
+            q.mx[2] = __shfl_sync(0xffffffffu, nd.mx[2], src);
+            const float B = __shfl_sync(0xffffffffu, thr.x, src), S = __shfl_sync(0xffffffffu, thr.y, src);
+            const bool yes = lane < L.T && sep_at_least(q, p, B, S);
+            const unsigned bits = __ballot_sync(0xffffffffu, yes);
+            if (lane == src) {
                 A = bits & m;
                 O = m & ~A;
             }
