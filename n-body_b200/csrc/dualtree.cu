@@ -1008,32 +1008,6 @@ __device__ __forceinline__ void m2p_staged(const float4 *pc, float eps, const fl
     m2p_term(pc[0], pc[1], pc[2], pc[3], pc[4], eps, p, a);
 }
 
-// Gravity::particleParticle (Gravity.h:199-209) without G for two sources against one target, in
-// paired FP32 arithmetic (sm_100 FADD2/FFMA2/FMUL2: one instruction for both halves):
-// u = (x_a, x_b, y_a, y_b), v = (z_a, z_b, m_a, m_b), np = -p in both halves. Per half:
-// d = b - p, r2 = d.d + eps, a += d m / r2^(3/2). With eps > 0 a source at the target's own
-// position adds 0 * s = 0 and a padding source (zero mass at the origin) adds 0; with eps = 0 a
-// source at zero distance is skipped.
-template<bool EPS0>
-__device__ __forceinline__ void pair2_nog(float2 npx, float2 npy, float2 npz, float2 eps2, float4 u, float4 v,
-                                          float2 &ax, float2 &ay, float2 &az) {
-    const float2 dx = __fadd2_rn(make_float2(u.x, u.y), npx);
-    const float2 dy = __fadd2_rn(make_float2(u.z, u.w), npy);
-    const float2 dz = __fadd2_rn(make_float2(v.x, v.y), npz);
-    const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
-    float2 inv;
-    inv.x = rsqrt_hw(r2.x);
-    inv.y = rsqrt_hw(r2.y);
-    float2 s = __fmul2_rn(make_float2(v.z, v.w), __fmul2_rn(__fmul2_rn(inv, inv), inv));
-    if (EPS0) {
-        if (r2.x == 0.f) s.x = 0.f;
-        if (r2.y == 0.f) s.y = 0.f;
-    }
-    ax = __ffma2_rn(dx, s, ax);
-    ay = __ffma2_rn(dy, s, ay);
-    az = __ffma2_rn(dz, s, az);
-}
-
 // Pairs of the unit's targets with sources src(0..m) for lanes in `mine`. 32 sources at a time are
 // staged in shared memory as 16 interleaved pairs (sources 2j and 2j+1 in one 32-byte record, so
 // that each 16-byte load yields two register pairs); replica r takes pairs r, r + G, ...
@@ -1051,12 +1025,12 @@ __device__ __forceinline__ void tile_pairs(NearWarp &w, const Lane &L, int c, bo
         const float4 u1 = w.tile[2 * (k + G)], v1 = w.tile[2 * (k + G) + 1];
         const float4 u2 = w.tile[2 * (k + 2 * G)], v2 = w.tile[2 * (k + 2 * G) + 1];
         const float4 u3 = w.tile[2 * (k + 3 * G)], v3 = w.tile[2 * (k + 3 * G) + 1];
-        pair2_nog<EPS0>(npx, npy, npz, eps2, u0, v0, ax, ay, az);
-        pair2_nog<EPS0>(npx, npy, npz, eps2, u1, v1, ax, ay, az);
-        pair2_nog<EPS0>(npx, npy, npz, eps2, u2, v2, ax, ay, az);
-        pair2_nog<EPS0>(npx, npy, npz, eps2, u3, v3, ax, ay, az);
+        pair2_term<EPS0>(npx, npy, npz, eps2, u0, v0, ax, ay, az);
+        pair2_term<EPS0>(npx, npy, npz, eps2, u1, v1, ax, ay, az);
+        pair2_term<EPS0>(npx, npy, npz, eps2, u2, v2, ax, ay, az);
+        pair2_term<EPS0>(npx, npy, npz, eps2, u3, v3, ax, ay, az);
     }
-    for (; k < np; k += G) pair2_nog<EPS0>(npx, npy, npz, eps2, w.tile[2 * k], w.tile[2 * k + 1], ax, ay, az);
+    for (; k < np; k += G) pair2_term<EPS0>(npx, npy, npz, eps2, w.tile[2 * k], w.tile[2 * k + 1], ax, ay, az);
 }
 
 // Stages one source per lane (a zero-mass source at the origin past the end) as 16 interleaved

@@ -29,6 +29,32 @@ __device__ __forceinline__ float rsqrt_hw(float x) {
     return y;
 }
 
+// Gravity::particleParticle (Gravity.h:199-209) without G for one target and two sources at once,
+// in paired FP32 arithmetic (sm_100 FADD2 / FFMA2 / FMUL2: one instruction for both halves):
+// u = (x_a, x_b, y_a, y_b), v = (z_a, z_b, m_a, m_b), np = -p in both halves. Per half:
+// d = b - p, r2 = d.d + eps (z term first, as the scalar form), a += d m / r2^(3/2). With eps > 0 a
+// source at the target's own position adds 0 * s = 0, and so does a zero-mass padding source; with
+// eps = 0 a source at zero distance is skipped.
+template<bool EPS0>
+__device__ __forceinline__ void pair2_term(float2 npx, float2 npy, float2 npz, float2 eps2, float4 u, float4 v,
+                                           float2 &ax, float2 &ay, float2 &az) {
+    const float2 dx = __fadd2_rn(make_float2(u.x, u.y), npx);
+    const float2 dy = __fadd2_rn(make_float2(u.z, u.w), npy);
+    const float2 dz = __fadd2_rn(make_float2(v.x, v.y), npz);
+    const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, eps2)));
+    float2 inv;
+    inv.x = rsqrt_hw(r2.x);
+    inv.y = rsqrt_hw(r2.y);
+    float2 s = __fmul2_rn(make_float2(v.z, v.w), __fmul2_rn(__fmul2_rn(inv, inv), inv));
+    if (EPS0) {
+        if (r2.x == 0.f) s.x = 0.f;
+        if (r2.y == 0.f) s.y = 0.f;
+    }
+    ax = __ffma2_rn(dx, s, ax);
+    ay = __ffma2_rn(dy, s, ay);
+    az = __ffma2_rn(dz, s, az);
+}
+
 // glm::min / glm::max semantics: min(x, y) = (y < x) ? y : x, max(x, y) = (x < y) ? y : x
 __device__ __forceinline__ float gmin(float x, float y) { return (y < x) ? y : x; }
 __device__ __forceinline__ float gmax(float x, float y) { return (x < y) ? y : x; }

@@ -214,18 +214,21 @@ __device__ __forceinline__ void flush_pp(WarpSmem<PAY, PART> &S, int &npp, const
         const bool on = (S.pp_mask[j] >> lane) & 1u;
         int k = b;
         for (; k + 3 < e; k += 4) {
-            const float4 s0 = __ldg(bodies + k), s1 = __ldg(bodies + k + 1);
-            const float4 s2 = __ldg(bodies + k + 2), s3 = __ldg(bodies + k + 3);
-            if (on) {
-                pair_term<EPS0>(p, s0, eps, ax, ay, az);
-                pair_term<EPS0>(p, s1, eps, ax, ay, az);
-                pair_term<EPS0>(p, s2, eps, ax, ay, az);
-                pair_term<EPS0>(p, s3, eps, ax, ay, az);
-            }
+            float4 s0 = __ldg(bodies + k), s1 = __ldg(bodies + k + 1);
+            float4 s2 = __ldg(bodies + k + 2), s3 = __ldg(bodies + k + 3);
+            s0.w = on ? s0.w : 0.f;
+            s1.w = on ? s1.w : 0.f;
+            s2.w = on ? s2.w : 0.f;
+            s3.w = on ? s3.w : 0.f;
+            pair_term<EPS0>(p, s0, eps, ax, ay, az);
+            pair_term<EPS0>(p, s1, eps, ax, ay, az);
+            pair_term<EPS0>(p, s2, eps, ax, ay, az);
+            pair_term<EPS0>(p, s3, eps, ax, ay, az);
         }
         for (; k < e; ++k) {
-            const float4 s0 = __ldg(bodies + k);
-            if (on) pair_term<EPS0>(p, s0, eps, ax, ay, az);
+            float4 s0 = __ldg(bodies + k);
+            s0.w = on ? s0.w : 0.f;
+            pair_term<EPS0>(p, s0, eps, ax, ay, az);
         }
         if (on) cpp += (unsigned) (e - b);
     }
