@@ -1033,7 +1033,13 @@ __device__ __forceinline__ void tile_pairs(NearWarp &w, const Lane &L, int c, bo
     for (; k < np; k += G) pair2_term<EPS0>(npx, npy, npz, eps2, w.tile[2 * k], w.tile[2 * k + 1], ax, ay, az);
 }
 
-// Stages one source per lane (a zero-mass source at the origin past the end) as 16 interleaved
+// Padding of a partly filled tile: no mass, at 1e30 on every axis, where the squared distance from
+// any target with coordinates below 1e29 in magnitude overflows to infinity; its reciprocal root
+// and every factor of its term are then exactly zero (a source at the origin would give 0 * inf
+// for a target within about 1e-13 of the origin when the softening is zero).
+__device__ __constant__ const float4 kNullSource = {1e30f, 1e30f, 1e30f, 0.f};
+
+// Stages one source per lane (the null source past the end) as 16 interleaved
 // pairs: sources 2j and 2j+1 in one 32-byte record, so that each 16-byte load yields two register
 // pairs.
 __device__ __forceinline__ void stage_tile(NearWarp &w, float4 b) {
@@ -1056,7 +1062,7 @@ __device__ __forceinline__ void pair_tile(NearWarp &w, const Lane &L, int m, Src
     float2 ax = make_float2(0.f, 0.f), ay = ax, az = ax;
     for (int j0 = 0; j0 < m; j0 += 32) {
         const int c = min(32, m - j0);
-        stage_tile(w, lane < c ? src(j0 + lane) : make_float4(0.f, 0.f, 0.f, 0.f));
+        stage_tile(w, lane < c ? src(j0 + lane) : kNullSource);
         __syncwarp();
         tile_pairs<EPS0>(w, L, c, mine, npx, npy, npz, eps2, ax, ay, az);
         __syncwarp();
@@ -1079,7 +1085,7 @@ __device__ void run_tiles(const Ctx &x, NearWarp &w, const Lane &L, const int *w
     int r = 0, first = 0, len = 0, o = 0;  // next word, current run, offset in it
     for (;;) {
         int fill = 0;
-        float4 b = make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 b = kNullSource;
         while (fill < 32) {
             if (o == len) {  // the current run is used up: take the next valid one
                 if (r + 1 >= nwords) break;

@@ -33,8 +33,8 @@ __device__ __forceinline__ float rsqrt_hw(float x) {
 // in paired FP32 arithmetic (sm_100 FADD2 / FFMA2 / FMUL2: one instruction for both halves):
 // u = (x_a, x_b, y_a, y_b), v = (z_a, z_b, m_a, m_b), np = -p in both halves. Per half:
 // d = b - p, r2 = d.d + eps (z term first, as the scalar form), a += d m / r2^(3/2). With eps > 0 a
-// source at the target's own position adds 0 * s = 0, and so does a zero-mass padding source; with
-// eps = 0 a source at zero distance is skipped.
+// source at the target's own position adds 0 * s = 0; with eps = 0 a source at zero distance is
+// skipped. A massless padding source far away (r2 overflowing to infinity) adds exactly 0.
 template<bool EPS0>
 __device__ __forceinline__ void pair2_term(float2 npx, float2 npy, float2 npz, float2 eps2, float4 u, float4 v,
                                            float2 &ax, float2 &ay, float2 &az) {

@@ -61,7 +61,7 @@ template<int PAY, int PART>
 struct WarpSmem {
     float4 tpos[32];
     float4 full_pay[kFullSlab * PAY];  // payloads of group-wide accepted nodes
-    float4 part_pay[PART * PAY];       // payloads of partially accepted nodes
+    float4 part_pay[(PART + 1) * PAY]; // payloads of partially accepted nodes, then the null payload
     uint32_t part_mask[PART];          // their target masks
     int pp_begin[kList], pp_end[kList];
     uint32_t pp_mask[kList];
@@ -106,13 +106,16 @@ __device__ __forceinline__ float ref_dist2(float px, float py, float pz, float4 
     return fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz));
 }
 
+// on = false makes the term exactly zero (a select, not a branch, so that lanes whose target does
+// not take the term run the same instructions).
 template<bool EPS0>
-__device__ __forceinline__ void pair_term(float4 p, float4 b, float eps, float &ax, float &ay, float &az) {
+__device__ __forceinline__ void pair_term(float4 p, float4 b, float eps, float &ax, float &ay, float &az,
+                                          bool on = true) {
     const float rx = p.x - b.x, ry = p.y - b.y, rz = p.z - b.z;
     const float r2 = fmaf(rx, rx, fmaf(ry, ry, fmaf(rz, rz, eps)));
     if (EPS0 && r2 == 0.f) return;  // equal positions contribute nothing (Gravity.h:203)
     const float inv = rsqrt_hw(r2);
-    const float s = b.w * (inv * inv * inv);
+    const float s = on ? b.w * (inv * inv * inv) : 0.f;
     ax = fmaf(-rx, s, ax);
     ay = fmaf(-ry, s, ay);
     az = fmaf(-rz, s, az);
@@ -189,18 +192,17 @@ __device__ __forceinline__ void flush_part(WarpSmem<NodeLayout<ORDER>::PAY, PART
     if constexpr (PART > 32)
         b1 = npart > 32 ? transpose32(lane + 32 < npart ? S.part_mask[lane + 32] : 0u, lane) : 0u;
     cnp += (unsigned) (__popc(b0) + __popc(b1));
+    // a lane whose set is used up evaluates the null payload instead of branching around the term
     while (__any_sync(kFull, (b0 | b1) != 0u)) {
-        if (b0 | b1) {
-            int j;
-            if (b0) {
-                j = __ffs(b0) - 1;
-                b0 &= b0 - 1;
-            } else {
-                j = 31 + __ffs(b1);
-                b1 &= b1 - 1;
-            }
-            staged_term<ORDER, EPS0>(S.part_pay + j * PAY, p, eps, ax, ay, az);
+        int j = PART;
+        if (b0) {
+            j = __ffs(b0) - 1;
+            b0 &= b0 - 1;
+        } else if (b1) {
+            j = 31 + __ffs(b1);
+            b1 &= b1 - 1;
         }
+        staged_term<ORDER, EPS0>(S.part_pay + j * PAY, p, eps, ax, ay, az);
     }
     npart = 0;
     __syncwarp();
@@ -214,21 +216,16 @@ __device__ __forceinline__ void flush_pp(WarpSmem<PAY, PART> &S, int &npp, const
         const bool on = (S.pp_mask[j] >> lane) & 1u;
         int k = b;
         for (; k + 3 < e; k += 4) {
-            float4 s0 = __ldg(bodies + k), s1 = __ldg(bodies + k + 1);
-            float4 s2 = __ldg(bodies + k + 2), s3 = __ldg(bodies + k + 3);
-            s0.w = on ? s0.w : 0.f;
-            s1.w = on ? s1.w : 0.f;
-            s2.w = on ? s2.w : 0.f;
-            s3.w = on ? s3.w : 0.f;
-            pair_term<EPS0>(p, s0, eps, ax, ay, az);
-            pair_term<EPS0>(p, s1, eps, ax, ay, az);
-            pair_term<EPS0>(p, s2, eps, ax, ay, az);
-            pair_term<EPS0>(p, s3, eps, ax, ay, az);
+            const float4 s0 = __ldg(bodies + k), s1 = __ldg(bodies + k + 1);
+            const float4 s2 = __ldg(bodies + k + 2), s3 = __ldg(bodies + k + 3);
+            pair_term<EPS0>(p, s0, eps, ax, ay, az, on);
+            pair_term<EPS0>(p, s1, eps, ax, ay, az, on);
+            pair_term<EPS0>(p, s2, eps, ax, ay, az, on);
+            pair_term<EPS0>(p, s3, eps, ax, ay, az, on);
         }
         for (; k < e; ++k) {
-            float4 s0 = __ldg(bodies + k);
-            s0.w = on ? s0.w : 0.f;
-            pair_term<EPS0>(p, s0, eps, ax, ay, az);
+            const float4 s0 = __ldg(bodies + k);
+            pair_term<EPS0>(p, s0, eps, ax, ay, az, on);
         }
         if (on) cpp += (unsigned) (e - b);
     }
@@ -354,6 +351,11 @@ __global__ void __launch_bounds__(THREADS, kResidentThreads / THREADS) bh_kernel
             }
         }
         S.tpos[lane] = p;
+        // the null payload: no mass and no moments at 1e30 on every axis, where the squared
+        // distance from any target with coordinates below 1e29 in magnitude overflows to
+        // infinity, so that every factor of the term is exactly zero and it adds nothing
+        if (lane < PAY) S.part_pay[PART * PAY + lane] = lane == 0 ? make_float4(1e30f, 1e30f, 1e30f, 0.f)
+                                                                  : make_float4(0.f, 0.f, 0.f, 0.f);
         int top = 0, nfull = 0, npart = 0, npp = 0, nmixed = 0;
         if (num_nodes > 0 && root >= 0 && root < num_nodes) {
             if (lane == 0) stack[0] = make_int2(root, (int) full);

@@ -135,6 +135,16 @@ def test_dual_G_and_softening(nb, oracle):
     check_against_oracle(nb, oracle, pm, 64, 0.4, eps=1e-3, G=2.5)
 
 
+def test_dual_zero_softening_target_near_origin(nb, oracle):
+    """epsilon = 0 and a target 1e-14 from the origin: the padding of partly filled pair tiles adds
+    exactly zero (a massless source at the origin would give 0 * inf there)."""
+    pm, _ = nb.scenarios.uniform_ball(12000, seed=32)
+    pm = pm[np.linalg.norm(pm[:, :3].astype(np.float64), axis=1) > 0.05]
+    pm = np.ascontiguousarray(np.concatenate([pm, np.array([[1e-14, 0.0, 0.0, pm[0, 3]]], dtype=np.float32)]))
+    acc, _ = check_against_oracle(nb, oracle, pm, 64, 0.4, eps=0.0)
+    assert np.all(np.isfinite(acc))
+
+
 def test_dual_accuracy_vs_fp64(nb, oracle):
     """The dual-tree field against FP64 direct summation: RMS relative error well under 1e-3."""
     pm, _ = two_spheres(nb, 60000, seed=21)

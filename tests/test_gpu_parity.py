@@ -169,6 +169,25 @@ def test_zero_softening(nb, oracle):
             check_accelerations(oracle, s, pm, acc, order, 16, 0.5, 0.0, max_tol=1e-3)
 
 
+def near_origin_scene(nb, n, seed):
+    """A ball with no body within 0.05 of the origin plus one body 1e-14 from it."""
+    pm, _ = nb.scenarios.uniform_ball(n, seed=seed)
+    pm = pm[np.linalg.norm(pm[:, :3].astype(np.float64), axis=1) > 0.05]
+    extra = np.array([[1e-14, 0.0, 0.0, pm[0, 3]]], dtype=np.float32)
+    return np.ascontiguousarray(np.concatenate([pm, extra]))
+
+
+def test_zero_softening_target_near_origin(nb, oracle):
+    """epsilon = 0 and a target 1e-14 from the origin: padding and masked terms stay exactly zero
+    (no 0 * inf from a distance below 1e-13)."""
+    pm = near_origin_scene(nb, 4000, 31)
+    for order in (1, 2):
+        with make_solver(nb, pm, order=order, leaf=16, theta=0.5, eps=0.0) as s:
+            acc = s.update_accelerations()
+            assert np.all(np.isfinite(acc))
+            check_accelerations(oracle, s, pm, acc, order, 16, 0.5, 0.0, max_tol=1e-3)
+
+
 def test_gravitational_constant(nb, oracle):
     pm, _ = nb.scenarios.uniform_ball(2500, seed=29)
     with make_solver(nb, pm, order=2, leaf=16, theta=0.5, G=2.5) as s:
