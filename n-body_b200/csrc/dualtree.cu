@@ -586,20 +586,26 @@ __global__ void __launch_bounds__(kThreads, 4) dual_kernel(DualNodes nodes, cons
         const int nfar = s_scan.base[0], nleaf = s_scan.base[1], nnon = s_scan.base[2];
 
         // ---- far entries into the local field: M2L (lock-step) or P2L (passive tree) ----
-        float part[F];
+        if (type == kLockstep) {
+            float part[F];
 #pragma unroll
-        for (int a = 0; a < F; ++a) part[a] = 0.f;
-        for (int i = tid; i < nfar; i += kThreads) {
-            const int e = c0[i];
-            if (type == kLockstep) {
+            for (int a = 0; a < F; ++a) part[a] = 0.f;
+            for (int i = tid; i < nfar; i += kThreads) {
+                const int e = c0[i];
                 m2l(x, e, load_node(nodes, e), pc, part);
                 ++nnn;
-            } else {
-                p2l(x, __ldg(bodies + e), pc, part);
+            }
+            block_add_field(part, s_field, s_red);
+        } else {
+            float part[F];
+#pragma unroll
+            for (int a = 0; a < F; ++a) part[a] = 0.f;
+            for (int i = tid; i < nfar; i += kThreads) {
+                p2l(x, __ldg(bodies + c0[i]), pc, part);
                 ++npn;
             }
+            block_add_field(part, s_field, s_red);
         }
-        block_add_field(part, s_field, s_red);
 
         if (P.leaf()) {
             // ---- passive leaf: L2P of this task's field; the near field goes to the leaf's items ----
@@ -949,7 +955,7 @@ static_assert(kM2pFull >= 32 && kM2pPart >= 32 && kNearLeaves >= 32, "a round ad
 
 struct NearWarp {
     float4 m2p_full[kM2pFull * kM2pRec];  // node records approximated for every target
-    float4 m2p_part[kM2pPart * kM2pRec];  // node records approximated for some targets
+    float4 m2p_part[(kM2pPart + 1) * kM2pRec];  // node records approximated for some targets, then a null record
     unsigned part_mask[kM2pPart];         // their target masks
     float4 tile[32];      // staged source bodies (16 interleaved pairs), then the replicas' partial sums
     float4 tpos[32];      // the unit's targets (replica-0 lanes)
@@ -1167,14 +1173,21 @@ __device__ void flush_m2p_part(const Ctx &x, NearWarp &w, const Lane &L, int &np
     uint32_t bits = __shfl_sync(0xffffffffu, mine_t, L.t);
     if (!L.active) bits = 0u;
     if (L.counted) nnp += (unsigned long long) __popc(bits);
-    int idx = 0;
+    if (L.G > 1) {  // replica r takes every G-th entry of its target's set, starting at the r-th
+        uint32_t own = 0u;
+        int idx = 0;
+        for (uint32_t t = bits; t; t &= t - 1, ++idx)
+            if (idx % L.G == L.r) own |= t & (0u - t);
+        bits = own;
+    }
+    // a lane whose entries are used up evaluates the null record instead of branching
     while (__any_sync(0xffffffffu, bits != 0u)) {
+        int j = kM2pPart;
         if (bits) {
-            const int j = __ffs(bits) - 1;
+            j = __ffs(bits) - 1;
             bits &= bits - 1;
-            if (idx % L.G == L.r) m2p_staged(w.m2p_part + j * kM2pRec, x.eps, p, a);
-            ++idx;
         }
+        m2p_staged(w.m2p_part + j * kM2pRec, x.eps, p, a);
     }
     npart = 0;
     __syncwarp();
@@ -1385,6 +1398,11 @@ __global__ void __launch_bounds__(kNearThreads, 8) near_kernel(DualNodes nodes, 
             }
         }
         if (lane < L.T) w.tpos[lane] = q;
+        // the null M2P record: no mass and no moments at 1e18 on every axis; for targets with
+        // coordinates below 1e17 in magnitude every product of offsets in the term stays finite,
+        // so each one meets a zero moment or mass and the term adds exactly zero
+        if (lane < kM2pRec) w.m2p_part[kM2pPart * kM2pRec + lane] = lane == 0 ? make_float4(1e18f, 1e18f, 1e18f, 0.f)
+                                                                              : make_float4(0.f, 0.f, 0.f, 0.f);
         __syncwarp();
         float a[3] = {0.f, 0.f, 0.f};
         int guard = 0;
