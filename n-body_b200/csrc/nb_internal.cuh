@@ -34,11 +34,10 @@ __device__ __forceinline__ float rsqrt_hw(float x) {
 // u = (x_a, x_b, y_a, y_b), v = (z_a, z_b, m_a, m_b), np = -p in both halves. Per half:
 // d = b - p, r2 = d.d + eps (z term first, as the scalar form), a += d m / r2^(3/2). With eps > 0 a
 // source at the target's own position adds 0 * s = 0; with eps = 0 a source at zero distance is
-// skipped. A massless padding source far away (r2 overflowing to infinity) adds exactly 0, and
-// on = false selects a zero factor for both halves (no branch for lanes that skip the sources).
+// skipped. A massless padding source far away (r2 overflowing to infinity) adds exactly 0.
 template<bool EPS0>
 __device__ __forceinline__ void pair2_term(float2 npx, float2 npy, float2 npz, float2 eps2, float4 u, float4 v,
-                                           float2 &ax, float2 &ay, float2 &az, bool on = true) {
+                                           float2 &ax, float2 &ay, float2 &az) {
     const float2 dx = __fadd2_rn(make_float2(u.x, u.y), npx);
     const float2 dy = __fadd2_rn(make_float2(u.z, u.w), npy);
     const float2 dz = __fadd2_rn(make_float2(v.x, v.y), npz);
@@ -51,7 +50,6 @@ __device__ __forceinline__ void pair2_term(float2 npx, float2 npy, float2 npz, f
         if (r2.x == 0.f) s.x = 0.f;
         if (r2.y == 0.f) s.y = 0.f;
     }
-    if (!on) s = make_float2(0.f, 0.f);
     ax = __ffma2_rn(dx, s, ax);
     ay = __ffma2_rn(dy, s, ay);
     az = __ffma2_rn(dz, s, az);
