@@ -111,7 +111,10 @@ int nb_set_stream(nb_ctx *ctx, void *cuda_stream);
 void *nb_get_stream(const nb_ctx *ctx);
 
 /* Replace the body set (the Simulation's Position/Mass/Velocity components). velocity may be NULL
- * (zero velocities). n may be 0. */
+ * (zero velocities). n may be 0. Coordinates are expected well inside float range: the traversals
+ * pad partly filled work with massless records far away (1e30, and 1e18 in the dual tree's M2P),
+ * whose terms are exactly zero for targets with coordinates below 1e29 (1e17 for the dual tree)
+ * in magnitude. */
 int nb_set_bodies(nb_ctx *ctx, int64_t n, const float *pos_mass, const float *velocity);
 int nb_set_bodies_device(nb_ctx *ctx, int64_t n, const void *d_pos_mass, const void *d_velocity);
 int64_t nb_body_count(const nb_ctx *ctx);
